@@ -1,0 +1,42 @@
+"""bigint_b200 -- B200-native big-integer multiplication.
+
+Python mirror of the reference's multiply interface (Looading99/BigInt,
+``include/bigint/mul.h``) over the C-ABI in ``include/bigint_b200.h``:
+
+=====================  ==============================================  =========================
+this package           reference                                       C-ABI
+=====================  ==============================================  =========================
+``mul(A, B)``          ``bigint::mul::_mul`` (mul.h:208-220)           ``bgpu_mul_u64``
+``ntt_mul(A, B)``      ``bigint::mul::ntt::mul`` (ntt_multithread.cpp:444) ``bgpu_mul_u64`` + NTT
+``brute_mul(A, B)``    ``bigint::mul::brute::mul`` (mul.h:82-102)      ``bgpu_mul_u64`` + schoolbook
+``mul_digits(a, b,``   ``bigint::mul::mul_digits`` (mul.h:223-318)     ``bgpu_mul_digits``
+``  precision, pos)``
+``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
+=====================  ==============================================  =========================
+
+Operands are little-endian ``numpy.uint64`` limb arrays (or 28-bit
+``numpy.uint32`` Digits for ``mul_digits``).  Passing the same array object
+for both operands squares, as the reference detects squaring by address.
+All arithmetic runs in the CUDA library ``libbigint_b200.so``; there is no
+CPU fallback, and importing raises if the library is missing.
+"""
+from __future__ import annotations
+
+from ._lib import (  # noqa: F401
+    BGPU_METHOD_AUTO,
+    BGPU_METHOD_NTT,
+    BGPU_METHOD_SCHOOLBOOK,
+    BigIntGPUError,
+    Stats,
+    brute_mul,
+    device_status,
+    init,
+    last_launch_count,
+    lib,
+    library_path,
+    mul,
+    mul_device,
+    mul_digits,
+    ntt_mul,
+    shutdown,
+)

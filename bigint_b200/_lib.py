@@ -1,0 +1,221 @@
+"""ctypes binding of libbigint_b200.so (see include/bigint_b200.h)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+library_path = os.environ.get("BIGINT_B200_LIB", os.path.join(_HERE, "libbigint_b200.so"))
+
+BGPU_OK = 0
+BGPU_METHOD_AUTO = 0
+BGPU_METHOD_NTT = 1
+BGPU_METHOD_SCHOOLBOOK = 2
+
+ERRORS = {
+    -1: "BGPU_ERR_INVALID_ARG",
+    -2: "BGPU_ERR_NO_DEVICE",
+    -3: "BGPU_ERR_OOM",
+    -4: "BGPU_ERR_CAPACITY",
+    -5: "BGPU_ERR_OUT_CAPACITY",
+    -6: "BGPU_ERR_CUDA",
+    -7: "BGPU_ERR_DEVICE_TIMEOUT",
+    -8: "BGPU_ERR_NOT_INIT",
+}
+
+
+class BigIntGPUError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        name = ERRORS.get(code, str(code))
+        super().__init__(f"{what}: {name} ({lib.bgpu_strerror(code).decode()})")
+
+
+class _Stats(C.Structure):
+    _fields_ = [
+        ("method", C.c_int32),
+        ("log2_points", C.c_uint32),
+        ("max_round_err", C.c_double),
+        ("fell_back", C.c_int32),
+        ("device_ms", C.c_float),
+    ]
+
+
+@dataclass
+class Stats:
+    method: int
+    log2_points: int
+    max_round_err: float
+    fell_back: bool
+    device_ms: float
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(library_path):
+        raise ImportError(
+            f"bigint_b200: CUDA library not found at {library_path}; build it with "
+            "`python -m bigint_b200.build` (there is no CPU fallback)")
+    L = C.CDLL(library_path)
+    u64p, u32p, szp = C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_size_t)
+    L.bgpu_init.argtypes = [C.c_int]
+    L.bgpu_init.restype = C.c_int
+    L.bgpu_shutdown.argtypes = []
+    L.bgpu_shutdown.restype = C.c_int
+    L.bgpu_strerror.argtypes = [C.c_int]
+    L.bgpu_strerror.restype = C.c_char_p
+    L.bgpu_mul_u64.argtypes = [u64p, C.c_size_t, u64p, C.c_size_t, u64p, C.c_size_t, szp,
+                               C.c_uint32, C.POINTER(_Stats)]
+    L.bgpu_mul_u64.restype = C.c_int
+    L.bgpu_mul_digits.argtypes = [u32p, C.c_size_t, u32p, C.c_size_t, C.c_size_t,
+                                  C.POINTER(C.c_int64), u32p, C.c_size_t, szp, C.c_uint32,
+                                  C.POINTER(_Stats)]
+    L.bgpu_mul_digits.restype = C.c_int
+    L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.c_uint32, C.c_void_p]
+    L.bgpu_mul_u64_device.restype = C.c_int
+    L.bgpu_device_status.argtypes = [C.c_void_p]
+    L.bgpu_device_status.restype = C.c_int
+    L.bgpu_last_launch_count.argtypes = []
+    L.bgpu_last_launch_count.restype = C.c_uint32
+    return L
+
+
+lib = _load()
+_init_lock = threading.Lock()
+_initialized_device: int | None = None
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != BGPU_OK:
+        raise BigIntGPUError(rc, what)
+
+
+def init(device: int = 0) -> None:
+    """Select the CUDA device and build the twiddle tables (idempotent)."""
+    global _initialized_device
+    with _init_lock:
+        _check(lib.bgpu_init(int(device)), "bgpu_init")
+        _initialized_device = int(device)
+
+
+def shutdown() -> None:
+    global _initialized_device
+    with _init_lock:
+        lib.bgpu_shutdown()
+        _initialized_device = None
+
+
+def _ensure_init() -> None:
+    if _initialized_device is None:
+        init(int(os.environ.get("BIGINT_B200_DEVICE", "0")))
+
+
+def _as_limbs(x) -> np.ndarray:
+    a = np.asarray(x)
+    if a.dtype != np.uint64:
+        a = a.astype(np.uint64)
+    return np.ascontiguousarray(a)
+
+
+def _as_digits(x) -> np.ndarray:
+    a = np.asarray(x)
+    if a.dtype != np.uint32:
+        a = a.astype(np.uint32)
+    return np.ascontiguousarray(a)
+
+
+def _stats(s: _Stats) -> Stats:
+    return Stats(int(s.method), int(s.log2_points), float(s.max_round_err), bool(s.fell_back),
+                 float(s.device_ms))
+
+
+def _mul_u64(A, B, flags: int, stats: bool):
+    _ensure_init()
+    square = B is None or B is A
+    a = _as_limbs(A)
+    b = a if square else _as_limbs(B)
+    if a.size == 0 or b.size == 0:
+        raise BigIntGPUError(-1, "bgpu_mul_u64 (empty operand)")
+    out = np.empty(a.size + b.size, dtype=np.uint64)
+    n = C.c_size_t(0)
+    st = _Stats()
+    u64p = C.POINTER(C.c_uint64)
+    pa = a.ctypes.data_as(u64p)
+    pb = pa if square else b.ctypes.data_as(u64p)
+    rc = lib.bgpu_mul_u64(pa, a.size, pb, b.size, out.ctypes.data_as(u64p), out.size,
+                          C.byref(n), flags, C.byref(st))
+    _check(rc, "bgpu_mul_u64")
+    res = out[: n.value]
+    return (res, _stats(st)) if stats else res
+
+
+def mul(A, B=None, *, stats: bool = False):
+    """A*B for little-endian u64 limb arrays (``_mul``, mul.h:208-220).
+
+    ``mul(A)`` or ``mul(A, A)`` squares.  Returns the product without leading
+    zero limbs (an empty array for a zero operand)."""
+    return _mul_u64(A, B, BGPU_METHOD_AUTO, stats)
+
+
+def ntt_mul(A, B=None, *, stats: bool = False):
+    """A*B forced onto the three-prime NTT (``ntt::mul``, ntt_multithread.cpp:444)."""
+    return _mul_u64(A, B, BGPU_METHOD_NTT, stats)
+
+
+def brute_mul(A, B=None, *, stats: bool = False):
+    """A*B on the schoolbook kernel (``brute::mul``, mul.h:82-102); na+nb <= 256."""
+    return _mul_u64(A, B, BGPU_METHOD_SCHOOLBOOK, stats)
+
+
+def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = None, *,
+               method: int = BGPU_METHOD_AUTO, stats: bool = False):
+    """Product of 28-bit Digits with the reference's ``mul_digits`` semantics.
+
+    With ``point_pos`` given, returns ``(digits, new_point_pos)``."""
+    _ensure_init()
+    square = b is None or b is a
+    da = _as_digits(a)
+    db = da if square else _as_digits(b)
+    if da.size == 0 or db.size == 0:
+        raise BigIntGPUError(-1, "bgpu_mul_digits (empty operand)")
+    cap = da.size + db.size + 2
+    out = np.empty(cap, dtype=np.uint32)
+    n = C.c_size_t(0)
+    pp = C.c_int64(0 if point_pos is None else int(point_pos))
+    st = _Stats()
+    u32p = C.POINTER(C.c_uint32)
+    pa = da.ctypes.data_as(u32p)
+    pb = pa if square else db.ctypes.data_as(u32p)
+    rc = lib.bgpu_mul_digits(pa, da.size, pb, db.size, int(output_precision),
+                             C.byref(pp) if point_pos is not None else None,
+                             out.ctypes.data_as(u32p), cap, C.byref(n), method, C.byref(st))
+    _check(rc, "bgpu_mul_digits")
+    res = out[: n.value]
+    ret = (res, int(pp.value)) if point_pos is not None else res
+    if stats:
+        return ret, _stats(st)
+    return ret
+
+
+def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, stream: int = 0,
+               method: int = BGPU_METHOD_AUTO) -> None:
+    """Asynchronous product of device-resident limbs (``bgpu_mul_u64_device``).
+
+    ``out_ptr`` receives na+nb limbs.  Equal pointers and lengths square."""
+    _ensure_init()
+    rc = lib.bgpu_mul_u64_device(C.c_void_p(a_ptr), na, C.c_void_p(b_ptr), nb,
+                                 C.c_void_p(out_ptr), method, C.c_void_p(stream or None))
+    _check(rc, "bgpu_mul_u64_device")
+
+
+def device_status(stream: int = 0) -> None:
+    """Synchronize ``stream`` and raise if a device-side error was recorded."""
+    _check(lib.bgpu_device_status(C.c_void_p(stream or None)), "bgpu_device_status")
+
+
+def last_launch_count() -> int:
+    return int(lib.bgpu_last_launch_count())

@@ -1,0 +1,534 @@
+// Host engine and C-ABI of bigint_b200.
+//
+// Owns the device, the twiddle tables, a grow-only scratch arena and the
+// stream; maps the reference's multiply seams onto the kernel pipelines:
+//   bgpu_mul_u64     <- bigint::mul::_mul / ntt::mul   (include/bigint/mul.h:208-220,
+//                                                       src/mul/ntt_multithread.cpp:444-530)
+//   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/bigint_b200.h"
+#include "engine.h"
+
+namespace bgpu {
+namespace {
+
+constexpr uint32_t kPrimes[kNumPrimes] = {469762049u, 1811939329u, 2013265921u};
+constexpr uint32_t kGens[kNumPrimes] = {3u, 13u, 31u};
+
+uint64_t pow_mod(uint64_t b, uint64_t e, uint64_t p) {
+    uint64_t r = 1;
+    b %= p;
+    while (e) {
+        if (e & 1) r = r * b % p;
+        b = b * b % p;
+        e >>= 1;
+    }
+    return r;
+}
+
+uint32_t inv32(uint32_t p) {  // p^-1 mod 2^32, p odd
+    uint32_t x = 1;
+    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
+    return x;
+}
+
+struct MontPair {
+    uint32_t w, wp;
+};
+
+MontPair mont(uint64_t v, uint32_t p) {
+    MontPair m;
+    m.w = (uint32_t)(((v % p) << 32) % p);
+    m.wp = m.w * inv32(p);
+    return m;
+}
+
+struct Engine {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    NttConsts consts{};
+    void* d_tables = nullptr;
+    // scratch arena
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // small fixed state
+    uint32_t* d_err = nullptr;
+    unsigned long long* d_ticket = nullptr;
+    uint64_t ticket_base = 0, epoch = 0;
+    // device I/O buffers of the host API
+    void* d_io = nullptr;
+    size_t io_bytes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t last_launches = 0;
+};
+
+Engine g;
+std::mutex g_mu;
+
+int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return BGPU_OK;
+    if (e == cudaErrorMemoryAllocation) return BGPU_ERR_OOM;
+    return BGPU_ERR_CUDA;
+}
+
+void release_locked() {
+    if (g.device < 0) return;
+    cudaSetDevice(g.device);
+    if (g.stream) cudaStreamSynchronize(g.stream);
+    cudaFree(g.d_tables);
+    cudaFree(g.d_scratch);
+    cudaFree(g.d_err);
+    cudaFree(g.d_ticket);
+    cudaFree(g.d_io);
+    if (g.ev0) cudaEventDestroy(g.ev0);
+    if (g.ev1) cudaEventDestroy(g.ev1);
+    if (g.stream) cudaStreamDestroy(g.stream);
+    g = Engine{};
+}
+
+int build_tables_locked() {
+    const size_t stage_n = (size_t)1 << kMaxLogRow;
+    const size_t split_n = (size_t)1 << kTwSplit;
+    const size_t per_dir = stage_n + 2 * split_n;
+    std::vector<uint2> host(kNumPrimes * 2 * per_dir);
+    for (int q = 0; q < kNumPrimes; ++q) {
+        const uint32_t p = kPrimes[q];
+        for (int dir = 0; dir < 2; ++dir) {
+            uint2* base = host.data() + (q * 2 + dir) * per_dir;
+            // stage table: entry h + m = omega_{2h}^(+-m)
+            MontPair one = mont(1, p);
+            base[0] = make_uint2(one.w, one.wp);
+            for (size_t h = 1; h < stage_n; h <<= 1) {
+                uint64_t root = pow_mod(kGens[q], (p - 1) / (2 * h), p);
+                if (dir) root = pow_mod(root, p - 2, p);
+                uint64_t v = 1;
+                for (size_t m = 0; m < h; ++m) {
+                    MontPair mp = mont(v, p);
+                    base[h + m] = make_uint2(mp.w, mp.wp);
+                    v = v * root % p;
+                }
+            }
+            // split tables for omega_{2^26}^(+-e)
+            uint64_t r26 = pow_mod(kGens[q], (p - 1) >> kMaxLogN, p);
+            if (dir) r26 = pow_mod(r26, p - 2, p);
+            uint2* th = base + stage_n;
+            uint2* tl = th + split_n;
+            const uint64_t step_hi = pow_mod(r26, split_n, p);
+            uint64_t vh = 1, vl = 1;
+            for (size_t i = 0; i < split_n; ++i) {
+                MontPair mh = mont(vh, p), ml = mont(vl, p);
+                th[i] = make_uint2(mh.w, mh.wp);
+                tl[i] = make_uint2(ml.w, ml.wp);
+                vh = vh * step_hi % p;
+                vl = vl * r26 % p;
+            }
+        }
+    }
+    cudaError_t e = cudaMalloc(&g.d_tables, host.size() * sizeof(uint2));
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaMemcpy(g.d_tables, host.data(), host.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_status(e);
+    const uint2* dt = static_cast<const uint2*>(g.d_tables);
+    NttConsts& c = g.consts;
+    for (int q = 0; q < kNumPrimes; ++q) {
+        c.pr[q].p = kPrimes[q];
+        c.pr[q].pinv = inv32(kPrimes[q]);
+        MontPair one = mont(1, kPrimes[q]);
+        c.one_w[q] = one.w;
+        c.one_wp[q] = one.wp;
+        for (int dir = 0; dir < 2; ++dir) {
+            const uint2* base = dt + (q * 2 + dir) * per_dir;
+            c.stage[q][dir] = base;
+            c.th[q][dir] = base + stage_n;
+            c.tl[q][dir] = base + stage_n + split_n;
+        }
+    }
+    const uint32_t p0 = kPrimes[0], p1 = kPrimes[1], p2 = kPrimes[2];
+    MontPair k1 = mont(pow_mod(p0, p1 - 2, p1), p1);
+    MontPair k2 = mont(p0 % p2, p2);
+    MontPair k3 = mont(pow_mod((uint64_t)p0 * p1 % p2, p2 - 2, p2), p2);
+    c.k1 = k1.w, c.k1p = k1.wp;
+    c.k2 = k2.w, c.k2p = k2.wp;
+    c.k3 = k3.w, c.k3p = k3.wp;
+    c.m01 = (uint64_t)p0 * p1;
+    return BGPU_OK;
+}
+
+int init_locked(int device) {
+    if (g.device == device) return BGPU_OK;
+    release_locked();
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) return BGPU_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return BGPU_ERR_NO_DEVICE;
+    g.device = device;
+    int rc = build_tables_locked();
+    if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    if (rc == BGPU_OK) rc = cuda_status(cudaMalloc(&g.d_err, sizeof(uint32_t)));
+    if (rc == BGPU_OK) rc = cuda_status(cudaMemset(g.d_err, 0, sizeof(uint32_t)));
+    if (rc == BGPU_OK) rc = cuda_status(cudaMalloc(&g.d_ticket, sizeof(unsigned long long)));
+    if (rc == BGPU_OK) rc = cuda_status(cudaMemset(g.d_ticket, 0, sizeof(unsigned long long)));
+    if (rc == BGPU_OK) rc = cuda_status(cudaEventCreate(&g.ev0));
+    if (rc == BGPU_OK) rc = cuda_status(cudaEventCreate(&g.ev1));
+    if (rc != BGPU_OK) {
+        release_locked();
+        return rc == BGPU_ERR_CUDA ? BGPU_ERR_NO_DEVICE : rc;
+    }
+    return BGPU_OK;
+}
+
+int ensure(void** ptr, size_t* have, size_t need) {
+    if (*have >= need) return BGPU_OK;
+    if (*ptr) {
+        cudaStreamSynchronize(g.stream);
+        cudaFree(*ptr);
+        *ptr = nullptr;
+        *have = 0;
+    }
+    size_t sz = need + need / 4;
+    cudaError_t e = cudaMalloc(ptr, sz);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        return BGPU_ERR_OOM;
+    }
+    *have = sz;
+    return BGPU_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int ceil_log2(uint64_t x) {
+    int l = 0;
+    while (((uint64_t)1 << l) < x) ++l;
+    return l;
+}
+
+// Scratch for an NTT product of 2^log_n points.
+int prepare_scratch(int log_n, bool square, ProductScratch* s) {
+    const size_t nn = (size_t)1 << log_n;
+    const size_t y_bytes = align256((square ? 1 : 2) * (size_t)kNumPrimes * nn * 4);
+    const size_t ch_bytes = align256(nn / 2 * 8);
+    const size_t sp_bytes = align256(nn / 8 * 8);
+    const size_t fl_bytes = align256((size_t)carry_blocks((uint32_t)(nn / 8)) * 8);
+    int rc = ensure(&g.d_scratch, &g.scratch_bytes, y_bytes + ch_bytes + sp_bytes + fl_bytes);
+    if (rc != BGPU_OK) return rc;
+    char* b = static_cast<char*>(g.d_scratch);
+    s->y = reinterpret_cast<uint32_t*>(b);
+    s->chunks = reinterpret_cast<uint64_t*>(b + y_bytes);
+    s->spill = reinterpret_cast<uint64_t*>(b + y_bytes + ch_bytes);
+    s->flags = reinterpret_cast<uint64_t*>(b + y_bytes + ch_bytes + sp_bytes);
+    s->ticket = g.d_ticket;
+    s->err = g.d_err;
+    return BGPU_OK;
+}
+
+// Core: product of two device operands into a device output (async).
+// nd32 values are operand lengths in 32-bit digits.
+int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, void* out,
+                    int out_fmt, size_t out_cap, uint32_t flags, cudaStream_t st,
+                    bgpu_stats* stats) {
+    const uint32_t method = flags & BGPU_METHOD_MASK;
+    const uint64_t total32 = (uint64_t)a.nd32 + b.nd32;
+    const int log_n = ceil_log2(total32 - 1);
+    if (log_n > kMaxLogN || !shape_supported(log_n < 5 ? 5 : log_n, square))
+        return BGPU_ERR_CAPACITY;
+    const int ln = log_n < 5 ? 5 : log_n;
+    ProductScratch s{};
+    int rc = prepare_scratch(ln, square, &s);
+    if (rc != BGPU_OK) return rc;
+    CarryLaunch cl;
+    cl.ticket_base = g.ticket_base;
+    cl.epoch = ++g.epoch;
+    g.ticket_base += carry_blocks((uint32_t)(((size_t)1 << ln) / 8));
+    cudaError_t e = launch_ntt_product(g.consts, a, b, square, ln, s, out, out_fmt, out_cap, cl, st);
+    g.last_launches = 4;
+    if (stats) {
+        stats->method = BGPU_METHOD_NTT;
+        stats->log2_points = (uint32_t)ln;
+    }
+    (void)method;
+    return cuda_status(e);
+}
+
+bool use_schoolbook(uint32_t flags, size_t na, size_t nb) {
+    const uint32_t m = flags & BGPU_METHOD_MASK;
+    if (m == BGPU_METHOD_SCHOOLBOOK) return true;
+    if (m == BGPU_METHOD_NTT) return false;
+    return na + nb <= kSchoolbookMaxLimbs;
+}
+
+int check_device_error(int rc) {
+    if (rc != BGPU_OK) return rc;
+    uint32_t err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, g.d_err, sizeof(err), cudaMemcpyDeviceToHost, g.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (err) {
+        cudaMemsetAsync(g.d_err, 0, sizeof(uint32_t), g.stream);
+        cudaStreamSynchronize(g.stream);
+        return BGPU_ERR_DEVICE_TIMEOUT;
+    }
+    return BGPU_OK;
+}
+
+size_t strip64(const uint64_t* x, size_t n) {
+    while (n > 0 && x[n - 1] == 0) --n;
+    return n;
+}
+
+size_t strip32(const uint32_t* x, size_t n) {
+    while (n > 0 && x[n - 1] == 0) --n;
+    return n;
+}
+
+int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                   size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats) {
+    const bool square = (a == b && na == nb);
+    na = strip64(a, na);
+    nb = square ? na : strip64(b, nb);
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (na == 0 || nb == 0) {
+        *out_len = 0;
+        return BGPU_OK;
+    }
+    const size_t nout = na + nb;
+    if (nout > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    const size_t a_off = 0, b_off = align256(na * 8), o_off = b_off + align256(nb * 8);
+    int rc = ensure(&g.d_io, &g.io_bytes, o_off + align256(nout * 8));
+    if (rc != BGPU_OK) return rc;
+    char* io = static_cast<char*>(g.d_io);
+    uint64_t* da = reinterpret_cast<uint64_t*>(io + a_off);
+    uint64_t* db = square ? da : reinterpret_cast<uint64_t*>(io + b_off);
+    uint64_t* dout = reinterpret_cast<uint64_t*>(io + o_off);
+    cudaStream_t st = g.stream;
+    cudaError_t e = cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, b, nb * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (stats) cudaEventRecord(g.ev0, st);
+    if (use_schoolbook(flags, na, nb)) {
+        if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+        rc = cuda_status(launch_schoolbook(da, (uint32_t)na, db, (uint32_t)nb, dout, st));
+        g.last_launches = 1;
+        if (stats) stats->method = BGPU_METHOD_SCHOOLBOOK;
+    } else {
+        OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
+        OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
+        rc = multiply_device(oa, ob, square, dout, kFmtLimb64, nout, flags, st, stats);
+    }
+    if (rc != BGPU_OK) return rc;
+    if (stats) cudaEventRecord(g.ev1, st);
+    // Copy straight into the caller's buffer when it holds na+nb limbs.
+    std::vector<uint64_t> tmp;
+    uint64_t* dst = out;
+    if (out_cap < nout) {
+        tmp.resize(nout);
+        dst = tmp.data();
+    }
+    e = cudaMemcpyAsync(dst, dout, nout * 8, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    if (stats) cudaEventElapsedTime(&stats->device_ms, g.ev0, g.ev1);
+    const size_t n = strip64(dst, nout);
+    *out_len = n;
+    if (dst != out) {
+        if (n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+        memcpy(out, dst, n * 8);
+    }
+    return BGPU_OK;
+}
+
+int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb, size_t prec,
+                      int64_t* point_pos, uint32_t* out, size_t out_cap, size_t* out_len,
+                      uint32_t flags, bgpu_stats* stats) {
+    const bool square = (a == b && na == nb);
+    if (stats) memset(stats, 0, sizeof(*stats));
+    // Offsets exactly as mul_digits (include/bigint/mul.h:227-243).
+    size_t off_a = (prec == 0 || na <= prec) ? 0 : na - prec;
+    size_t off_b = (prec == 0 || nb <= prec) ? 0 : nb - prec;
+    size_t tz_a = 0, tz_b = 0;
+    while (off_a + tz_a < na && a[off_a + tz_a] == 0) ++tz_a;
+    if (off_a + tz_a == na) return BGPU_ERR_INVALID_ARG;
+    if (square) {
+        tz_b = tz_a;
+    } else {
+        while (off_b + tz_b < nb && b[off_b + tz_b] == 0) ++tz_b;
+        if (off_b + tz_b == nb) return BGPU_ERR_INVALID_ARG;
+    }
+    off_a += tz_a;
+    off_b += tz_b;
+    const uint32_t* pa = a + off_a;
+    const uint32_t* pb = b + off_b;
+    size_t la = strip32(pa, na - off_a), lb = square ? la : strip32(pb, nb - off_b);
+    for (size_t i = 0; i < la; ++i)
+        if (pa[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    if (!square)
+        for (size_t i = 0; i < lb; ++i)
+            if (pb[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    const size_t nres = la + lb + 1;  // 28-bit digits of the product, with margin
+    if (nres > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    const size_t la64 = (la * 28 + 63) / 64, lb64 = (lb * 28 + 63) / 64;
+    const size_t a_off = 0, b_off = align256(la * 4), o_off = b_off + align256(lb * 4);
+    const size_t l_off = o_off + align256(nres * 4);
+    const size_t need = l_off + align256((la64 + 1) * 8) + align256((lb64 + 1) * 8) +
+                        align256((la64 + lb64) * 8);
+    int rc = ensure(&g.d_io, &g.io_bytes, need);
+    if (rc != BGPU_OK) return rc;
+    char* io = static_cast<char*>(g.d_io);
+    uint32_t* da = reinterpret_cast<uint32_t*>(io + a_off);
+    uint32_t* db = square ? da : reinterpret_cast<uint32_t*>(io + b_off);
+    uint32_t* dres = reinterpret_cast<uint32_t*>(io + o_off);
+    cudaStream_t st = g.stream;
+    cudaError_t e = cudaMemcpyAsync(da, pa, la * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, pb, lb * 4, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (stats) cudaEventRecord(g.ev0, st);
+    if (use_schoolbook(flags, la64, lb64)) {
+        if (la64 + lb64 > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+        uint64_t* la_d = reinterpret_cast<uint64_t*>(io + l_off);
+        uint64_t* lb_d = square ? la_d : la_d + align256((la64 + 1) * 8) / 8;
+        uint64_t* lo_d = reinterpret_cast<uint64_t*>(io + l_off + align256((la64 + 1) * 8) +
+                                                     align256((lb64 + 1) * 8));
+        e = launch_digits28_to_limbs(da, (uint32_t)la, la_d, (uint32_t)la64, st);
+        if (e == cudaSuccess && !square)
+            e = launch_digits28_to_limbs(db, (uint32_t)lb, lb_d, (uint32_t)lb64, st);
+        if (e == cudaSuccess)
+            e = launch_schoolbook(la_d, (uint32_t)la64, lb_d, (uint32_t)lb64, lo_d, st);
+        if (e == cudaSuccess)
+            e = launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st);
+        rc = cuda_status(e);
+        g.last_launches = square ? 3 : 4;
+        if (stats) stats->method = BGPU_METHOD_SCHOOLBOOK;
+    } else {
+        OperandDesc oa{da, (uint32_t)la, (uint32_t)((la * 28 + 31) / 32), kFmtDigit28};
+        OperandDesc ob{db, (uint32_t)lb, (uint32_t)((lb * 28 + 31) / 32), kFmtDigit28};
+        rc = multiply_device(oa, ob, square, dres, kFmtDigit28, nres, flags, st, stats);
+    }
+    if (rc != BGPU_OK) return rc;
+    if (stats) cudaEventRecord(g.ev1, st);
+    // Result digits land in the caller's buffer when it is large enough.
+    const size_t z = prec ? 0 : tz_a + tz_b;
+    std::vector<uint32_t> tmp;
+    uint32_t* dst = (out_cap >= z + nres) ? out + z : nullptr;
+    if (!dst) {
+        tmp.resize(nres);
+        dst = tmp.data();
+    }
+    e = cudaMemcpyAsync(dst, dres, nres * 4, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    if (stats) cudaEventElapsedTime(&stats->device_ms, g.ev0, g.ev1);
+    size_t n = strip32(dst, nres);
+    if (prec) {
+        // Trim to the top digits and shift the point (include/bigint/mul.h:302-312).
+        size_t off_r = n <= prec ? 0 : n - prec;
+        while (dst[off_r] == 0) ++off_r;
+        const size_t keep = n - off_r;
+        if (point_pos) *point_pos -= (int64_t)(off_a + off_b + off_r);
+        *out_len = keep;
+        if (keep > out_cap) return BGPU_ERR_OUT_CAPACITY;
+        memmove(out, dst + off_r, keep * 4);
+    } else {
+        *out_len = z + n;
+        if (z + n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+        if (dst != out + z) memcpy(out + z, dst, n * 4);
+        memset(out, 0, z * 4);
+    }
+    return BGPU_OK;
+}
+
+}  // namespace
+}  // namespace bgpu
+
+using namespace bgpu;
+
+extern "C" {
+
+int bgpu_init(int device) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return init_locked(device);
+}
+
+int bgpu_shutdown(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    release_locked();
+    return BGPU_OK;
+}
+
+const char* bgpu_strerror(int code) {
+    switch (code) {
+        case BGPU_OK: return "ok";
+        case BGPU_ERR_INVALID_ARG: return "invalid argument";
+        case BGPU_ERR_NO_DEVICE: return "no usable CUDA device";
+        case BGPU_ERR_OOM: return "out of memory";
+        case BGPU_ERR_CAPACITY: return "product exceeds the largest supported transform";
+        case BGPU_ERR_OUT_CAPACITY: return "output buffer too small";
+        case BGPU_ERR_CUDA: return "CUDA error";
+        case BGPU_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case BGPU_ERR_NOT_INIT: return "engine not initialized (call bgpu_init)";
+        default: return "unknown status";
+    }
+}
+
+int bgpu_mul_u64(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                 size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats) {
+    if (!a || !b || !out_len || (!out && out_cap) || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
+    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return mul_u64_locked(a, na, b, nb, out, out_cap, out_len, flags, stats);
+}
+
+int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
+                    size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
+                    size_t* out_len, uint32_t flags, bgpu_stats* stats) {
+    if (!a || !b || !out_len || (!out && out_cap) || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
+    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return mul_digits_locked(a, na, b, nb, output_precision, point_pos, out, out_cap, out_len,
+                             flags, stats);
+}
+
+int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
+                        uint64_t* d_out, uint32_t flags, void* stream) {
+    if (!d_a || !d_b || !d_out || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
+    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
+    const bool square = (d_a == d_b && na == nb);
+    if (use_schoolbook(flags, na, nb)) {
+        if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+        g.last_launches = 1;
+        return cuda_status(launch_schoolbook(d_a, (uint32_t)na, d_b, (uint32_t)nb, d_out, st));
+    }
+    if (na + nb > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    OperandDesc oa{d_a, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
+    OperandDesc ob{d_b, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
+    return multiply_device(oa, ob, square, d_out, kFmtLimb64, na + nb, flags, st, nullptr);
+}
+
+int bgpu_device_status(void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    return check_device_error(BGPU_OK);
+}
+
+uint32_t bgpu_last_launch_count(void) { return g.last_launches; }
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// Internal interfaces between the host engine and the CUDA kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "arith.cuh"
+
+namespace bgpu {
+
+// Input/output digit formats on the device.
+enum DigitFormat : int {
+    kFmtLimb64 = 0,  // little-endian uint64_t limbs (the reference's _mul / ntt::mul seam)
+    kFmtDigit28 = 1, // little-endian uint32_t digits of 28 bits (the reference's Digits)
+};
+
+// Constants shared by all transform kernels (passed by value as a kernel parameter).
+struct NttConsts {
+    PrimeInfo pr[kNumPrimes];
+    uint32_t one_w[kNumPrimes], one_wp[kNumPrimes];  // Montgomery form of 1 (reduces any u32 mod p)
+    const uint2* stage[kNumPrimes][2];  // [prime][dir]: entry h+m = omega_{2h}^{+-m}, h < 2^15
+    const uint2* th[kNumPrimes][2];     // omega_{2^26}^{+-(i << 13)}, i < 2^13
+    const uint2* tl[kNumPrimes][2];     // omega_{2^26}^{+-i}, i < 2^13
+    // Garner CRT for p0 < p1 < p2 (Montgomery constants with their w').
+    uint32_t k1, k1p;  // p0^-1 mod p1
+    uint32_t k2, k2p;  // p0 mod p2
+    uint32_t k3, k3p;  // (p0 p1)^-1 mod p2
+    uint64_t m01;      // p0 * p1
+};
+
+// One operand of a transform: a device pointer in `fmt` with `nsrc` source
+// elements; `nd32` is its length in 32-bit digits.
+struct OperandDesc {
+    const void* ptr;
+    uint32_t nsrc;
+    uint32_t nd32;
+    int fmt;
+};
+
+// Shape of a two-pass transform of N = N1 * N2 points.
+struct TransformShape {
+    int log_n;   // log2 N
+    int log_n1;  // row length (middle pass)
+    int log_n2;  // column length (outer passes)
+};
+
+TransformShape choose_shape(int log_n);
+bool shape_supported(int log_n, bool square);
+size_t smem_fwd_cols(int log_n2);
+size_t smem_mid_rows(int log_n1, bool square);
+size_t smem_inv_cols(int log_n2);
+
+// Per-call scratch for one product (device pointers).
+struct ProductScratch {
+    uint32_t* y;          // (square ? 1 : 2) * 3 * N residues
+    uint64_t* chunks;     // N/2 limbs: 8-digit chunk sums before the carry scan
+    uint64_t* spill;      // N/8 spills (chunk overflow above 256 bits)
+    uint64_t* flags;      // carry-scan block status words
+    unsigned long long* ticket;  // carry-scan block ticket counter
+    uint32_t* err;        // sticky device error word
+};
+
+struct CarryLaunch {
+    uint64_t ticket_base;
+    uint64_t epoch;
+};
+
+// Launch the full NTT product pipeline (4 kernels) on `stream`.
+// out: device buffer in `out_fmt` with `out_cap` elements.
+cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
+                               bool square, int log_n, const ProductScratch& s, void* out,
+                               int out_fmt, size_t out_cap, const CarryLaunch& cl,
+                               cudaStream_t stream);
+
+uint32_t carry_blocks(uint32_t nchunks);
+
+// Schoolbook product for small operands (one CTA); out has na+nb limbs.
+cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
+                              uint64_t* out, cudaStream_t stream);
+constexpr uint32_t kSchoolbookMaxLimbs = 256;  // na + nb
+
+// Digit-format conversion kernels (used around the schoolbook path).
+cudaError_t launch_digits28_to_limbs(const uint32_t* d, uint32_t nd, uint64_t* limbs,
+                                     uint32_t nlimbs, cudaStream_t stream);
+cudaError_t launch_limbs_to_digits28(const uint64_t* limbs, uint32_t nlimbs, uint32_t* d,
+                                     uint32_t nd, cudaStream_t stream);
+
+}  // namespace bgpu

@@ -1,0 +1,831 @@
+// Three-prime NTT product pipeline for sm_100a.
+//
+// A product of N = N1 * N2 points (point n = n1 + N1*n2, 32-bit digits) is
+// four kernel launches:
+//   1. k_fwd_cols   per (8-column tile, prime, operand): load digits straight
+//                   from the caller's limbs/Digits, reduce mod p, length-N2
+//                   DIF over n2 (natural -> bit-reversed k2), multiply by
+//                   omega_N^(n1*k2), store Y[slot][n1].
+//   2. k_mid_rows   per (row slot, prime): length-N1 DIF of A's and B's row,
+//                   pointwise product (scaled by N^-1), length-N1 DIT back to
+//                   natural n1, multiply by omega_N^-(n1*k2), store in place.
+//   3. k_inv_cols   per 8-column tile: for each prime, length-N2 DIT over the
+//                   bit-reversed slots -> natural n2; then Garner CRT per point
+//                   and the sum of each chunk of 8 consecutive coefficients
+//                   (an exact 256-bit chunk value plus a < 2^58 spill).
+//   4. k_carry      one chunk per thread: chunk + previous spill, carries
+//                   resolved by a decoupled look-back scan over blocks, final
+//                   limbs or 28-bit digits written in natural order.
+// The reference runs the same transform as log2 N barrier-separated radix-2
+// sweeps plus a serial carry (src/mul/ntt_multithread.cpp:333-379, 418-442);
+// here every pass keeps a whole row or column tile in shared memory and runs
+// radix-8/16 rounds in registers, so each product makes three sweeps over the
+// residues in global memory.
+#include <cuda/atomic>
+
+#include "engine.h"
+
+namespace bgpu {
+
+constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
+
+// Round split of a length-2^L transform into radix-2^r rounds (r <= 4),
+// top bits first (DIF order).
+template <int L>
+struct Plan {
+    static constexpr int nr = (L + 3) / 4;
+    __host__ __device__ static constexpr int r(int k) { return L / nr + (k < L % nr ? 1 : 0); }
+    __host__ __device__ static constexpr int hi(int k) {
+        int h = L - 1;
+        for (int i = 0; i < k; ++i) h -= r(i);
+        return h;
+    }
+    __host__ __device__ static constexpr int lo(int k) { return hi(k) - r(k) + 1; }
+};
+
+// ---- register-resident butterflies ------------------------------------------
+
+// DIF stages for pair bits HI..LO on the 2^R elements base + (j << LO).
+// Element pair (i, i+h): (a, b) -> (a+b, (a-b) * omega_{2h}^(i mod h)).
+template <int R, int HI, int LO>
+__device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_low,
+                                         const uint2* __restrict__ tw, uint32_t p) {
+#pragma unroll
+    for (int t = 0; t < R; ++t) {
+        const uint32_t h = 1u << (HI - t);
+        const int dist = 1 << (R - 1 - t);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+            if (j & dist) continue;
+            const uint32_t a = x[j], b = x[j + dist];
+            x[j] = mod_add(a, b, p);
+            const uint32_t d = mod_sub(a, b, p);
+            if (LO == 0 && (j & (dist - 1)) == 0) {
+                x[j + dist] = d;  // twiddle omega^0 (base_low is 0 when LO == 0)
+            } else {
+                const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
+                const uint2 w = __ldg(tw + h + m);
+                x[j + dist] = mont_mul_pre(d, w.x, w.y, p);
+            }
+        }
+    }
+}
+
+// DIT stages for pair bits LO..HI (inverse table):
+// (a, b) -> (a + b*w, a - b*w), w = omega_{2h}^-(i mod h).
+template <int R, int HI, int LO>
+__device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_low,
+                                         const uint2* __restrict__ tw, uint32_t p) {
+#pragma unroll
+    for (int t = R - 1; t >= 0; --t) {
+        const uint32_t h = 1u << (HI - t);
+        const int dist = 1 << (R - 1 - t);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+            if (j & dist) continue;
+            uint32_t b = x[j + dist];
+            if (!(LO == 0 && (j & (dist - 1)) == 0)) {
+                const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
+                const uint2 w = __ldg(tw + h + m);
+                b = mont_mul_pre(b, w.x, w.y, p);
+            }
+            const uint32_t a = x[j];
+            x[j] = mod_add(a, b, p);
+            x[j + dist] = mod_sub(a, b, p);
+        }
+    }
+}
+
+// Group g of round K on a [2^L][C] tile: column and base element index.
+template <int L, int C, int K>
+struct Group {
+    static constexpr int R = Plan<L>::r(K), HI = Plan<L>::hi(K), LO = Plan<L>::lo(K);
+    static constexpr int G = (1 << (L - R)) * C;
+    int col;
+    uint32_t base, base_low;
+    __device__ __forceinline__ explicit Group(int g) {
+        col = g % C;
+        const uint32_t q = (uint32_t)(g / C);
+        base_low = q & ((1u << LO) - 1u);
+        base = ((q >> LO) << (HI + 1)) | base_low;
+    }
+    __device__ __forceinline__ uint32_t idx(int j) const { return base + ((uint32_t)j << LO); }
+};
+
+// One smem round (load -> butterflies -> store back); no sync inside.
+template <int L, int C, int T, int K, bool INV>
+__device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict__ tw,
+                                           uint32_t p) {
+    using Gr = Group<L, C, K>;
+    constexpr int R = Gr::R;
+#pragma unroll 1
+    for (int g = threadIdx.x; g < Gr::G; g += T) {
+        const Gr gr(g);
+        uint32_t x[1 << R];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.idx(j) * C + gr.col];
+        if constexpr (INV)
+            dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+        else
+            dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) sm[gr.idx(j) * C + gr.col] = x[j];
+    }
+}
+
+// DIF rounds K0..K1 (inclusive) in smem, each followed by a block barrier.
+template <int L, int C, int T, int K, int KEND>
+__device__ __forceinline__ void dif_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
+    if constexpr (K <= KEND) {
+        smem_round<L, C, T, K, false>(sm, tw, p);
+        __syncthreads();
+        dif_rounds<L, C, T, K + 1, KEND>(sm, tw, p);
+    }
+}
+
+// DIT rounds K down to KEND (inclusive) in smem, each followed by a barrier.
+template <int L, int C, int T, int K, int KEND>
+__device__ __forceinline__ void dit_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
+    if constexpr (K >= KEND) {
+        smem_round<L, C, T, K, true>(sm, tw, p);
+        __syncthreads();
+        dit_rounds<L, C, T, K - 1, KEND>(sm, tw, p);
+    }
+}
+
+// omega_N^(+-e) in Montgomery form from the two split tables (N = 2^log_n).
+__device__ __forceinline__ uint32_t inter_twiddle(const NttConsts& c, int q, int dir, uint32_t e,
+                                                  int log_n, uint32_t p, uint32_t pinv) {
+    const uint32_t e26 = e << (kMaxLogN - log_n);
+    const uint32_t hi = __ldg(&c.th[q][dir][e26 >> kTwSplit].x);
+    const uint2 lo = __ldg(&c.tl[q][dir][e26 & ((1u << kTwSplit) - 1u)]);
+    return mont_mul_pre(hi, lo.x, lo.y, p);
+    (void)pinv;
+}
+
+__device__ __forceinline__ uint32_t bitrev(uint32_t v, int bits) {
+    return bits == 0 ? 0u : (__brev(v) >> (32 - bits));
+}
+
+// 32-bit digit n of an operand (0 beyond its length).
+__device__ __forceinline__ uint32_t load_digit32(const OperandDesc& in, uint32_t n) {
+    if (n >= in.nd32) return 0u;
+    if (in.fmt == kFmtLimb64) return __ldg(static_cast<const uint32_t*>(in.ptr) + n);
+    const uint32_t* d = static_cast<const uint32_t*>(in.ptr);
+    const uint32_t bit = n * 32u;
+    const uint32_t i0 = bit / 28u, sh = bit - i0 * 28u;  // sh in {0,4,...,24}
+    uint32_t v = __ldg(d + i0) >> sh;
+    if (i0 + 1 < in.nsrc) v |= __ldg(d + i0 + 1) << (28u - sh);
+    return v;
+}
+
+// ---- kernel 1: forward column pass ------------------------------------------
+
+struct FwdColsArgs {
+    OperandDesc op[2];
+    uint32_t* y;  // [op][prime][N]
+    int log_n, log_n1;
+};
+
+template <int L2, int T>
+__global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a, const NttConsts c) {
+    extern __shared__ __align__(16) uint32_t sm[];  // [2^L2][kCols]
+    using P2 = Plan<L2>;
+    constexpr int NR = P2::nr;
+    const int q = blockIdx.y, opi = blockIdx.z;
+    const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
+    const uint2* tw = c.stage[q][0];
+    const OperandDesc in = a.op[opi];
+    const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
+    const size_t nn = (size_t)1 << a.log_n;
+    uint32_t* y = a.y + ((size_t)opi * kNumPrimes + q) * nn;
+    const uint32_t one_w = c.one_w[q], one_wp = c.one_wp[q];
+
+    // Round 0: rows n2 = base + (j << LO) read from the caller's digits.
+    {
+        using Gr = Group<L2, kCols, 0>;
+        constexpr int R = Gr::R;
+#pragma unroll 1
+        for (int g = threadIdx.x; g < Gr::G; g += T) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
+            uint32_t any = 0;
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) {
+                const uint32_t n = c0 + gr.col + n1_len * gr.idx(j);
+                uint32_t v = load_digit32(in, n);
+                any |= v;
+                x[j] = mont_mul_pre(v, one_w, one_wp, p);
+            }
+            if (any) dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            if constexpr (NR == 1) {
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) {
+                    const uint32_t slot = gr.idx(j), n1 = c0 + gr.col;
+                    const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
+                    const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p, pinv);
+                    y[(size_t)slot * n1_len + n1] = mont_mul(x[j], w, p, pinv);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) sm[gr.idx(j) * kCols + gr.col] = x[j];
+            }
+        }
+    }
+    if constexpr (NR > 1) {
+        __syncthreads();
+        dif_rounds<L2, kCols, T, 1, NR - 2>(sm, tw, p);
+        // Last round: butterflies, inter-pass twiddle, store to global.
+        using Gr = Group<L2, kCols, NR - 1>;
+        constexpr int R = Gr::R;
+#pragma unroll 1
+        for (int g = threadIdx.x; g < Gr::G; g += T) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.idx(j) * kCols + gr.col];
+            dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            const uint32_t n1 = c0 + gr.col;
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) {
+                const uint32_t slot = gr.idx(j);
+                const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
+                const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p, pinv);
+                y[(size_t)slot * n1_len + n1] = mont_mul(x[j], w, p, pinv);
+            }
+        }
+    }
+}
+
+// ---- kernel 2: middle row pass ----------------------------------------------
+
+struct MidRowsArgs {
+    uint32_t* ya;        // [prime][N], result written in place
+    const uint32_t* yb;  // [prime][N] or null (square)
+    int log_n, log_n2;
+    uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
+};
+
+// Last DIF round of B (or A when squaring) fused with the pointwise product
+// and the first DIT round; with a single round also the inverse twiddle.
+template <int L1, int T, bool SQR, bool SINGLE>
+__device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& c, uint32_t* sa,
+                                         uint32_t* sb, const uint32_t* row_a, const uint32_t* row_b,
+                                         uint32_t* row_out, int q, uint32_t k2) {
+    using P1 = Plan<L1>;
+    constexpr int K = P1::nr - 1;
+    using Gr = Group<L1, 1, K>;
+    constexpr int R = Gr::R;
+    const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
+    const uint2* twf = c.stage[q][0];
+    const uint2* twi = c.stage[q][1];
+    const uint32_t sw = a.scale_w[q], swp = a.scale_wp[q];
+    const uint32_t* src = SQR ? sa : sb;
+#pragma unroll 1
+    for (int g = threadIdx.x; g < Gr::G; g += T) {
+        const Gr gr(g);
+        uint32_t x[1 << R];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+            if constexpr (SINGLE)
+                x[j] = (SQR ? row_a : row_b)[gr.idx(j)];
+            else
+                x[j] = src[gr.idx(j)];
+        }
+        dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+            const uint32_t other = SQR ? x[j] : sa[gr.idx(j)];
+            x[j] = mont_mul_pre(mont_mul(x[j], other, p, pinv), sw, swp, p);
+        }
+        dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+        if constexpr (SINGLE) {
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) {
+                const uint32_t n1 = gr.idx(j);
+                const uint32_t e = (n1 * k2) & ((1u << a.log_n) - 1u);
+                const uint32_t w = inter_twiddle(c, q, 1, e, a.log_n, p, pinv);
+                row_out[n1] = mont_mul(x[j], w, p, pinv);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) sa[gr.idx(j)] = x[j];
+        }
+    }
+}
+
+// DIF of one row: round 0 from global into smem, then rounds 1..nr-2 (the
+// last round is done by mid_turn).
+template <int L1, int T>
+__device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, const uint2* twf,
+                                            uint32_t p) {
+    using P1 = Plan<L1>;
+    using Gr = Group<L1, 1, 0>;
+    constexpr int R = Gr::R;
+#pragma unroll 1
+    for (int g = threadIdx.x; g < Gr::G; g += T) {
+        const Gr gr(g);
+        uint32_t x[1 << R];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) x[j] = row[gr.idx(j)];
+        dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) s[gr.idx(j)] = x[j];
+    }
+    __syncthreads();
+    dif_rounds<L1, 1, T, 1, P1::nr - 2>(s, twf, p);
+}
+
+template <int L1, int T, bool SQR>
+__global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a, const NttConsts c) {
+    extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1])
+    using P1 = Plan<L1>;
+    constexpr int NR = P1::nr;
+    uint32_t* sa = sm;
+    uint32_t* sb = sm + (1u << L1);
+    const int q = blockIdx.y;
+    const uint32_t slot = blockIdx.x;
+    const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
+    const uint2* twf = c.stage[q][0];
+    const uint2* twi = c.stage[q][1];
+    const size_t nn = (size_t)1 << a.log_n;
+    uint32_t* row_a = a.ya + q * nn + (size_t)slot * (1u << L1);
+    const uint32_t* row_b = SQR ? nullptr : a.yb + q * nn + (size_t)slot * (1u << L1);
+    const uint32_t k2 = bitrev(slot, a.log_n2);
+
+    if constexpr (NR == 1) {
+        if constexpr (!SQR) {
+            // A's single DIF round into smem first.
+            using Gr = Group<L1, 1, 0>;
+            constexpr int R = Gr::R;
+#pragma unroll 1
+            for (int g = threadIdx.x; g < Gr::G; g += T) {
+                const Gr gr(g);
+                uint32_t x[1 << R];
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) x[j] = row_a[gr.idx(j)];
+                dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) sa[gr.idx(j)] = x[j];
+            }
+            __syncthreads();
+        }
+        mid_turn<L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+    } else {
+        mid_dif_row<L1, T>(row_a, sa, twf, p);
+        if constexpr (!SQR) {
+            // A's last DIF round in place, then B's rounds.
+            smem_round<L1, 1, T, NR - 1, false>(sa, twf, p);
+            mid_dif_row<L1, T>(row_b, sb, twf, p);
+        }
+        mid_turn<L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+        __syncthreads();
+        dit_rounds<L1, 1, T, NR - 2, 1>(sa, twi, p);
+        // Round 0 (top bits): DIT, inverse twiddle, store to global.
+        using Gr = Group<L1, 1, 0>;
+        constexpr int R = Gr::R;
+#pragma unroll 1
+        for (int g = threadIdx.x; g < Gr::G; g += T) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) x[j] = sa[gr.idx(j)];
+            dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) {
+                const uint32_t n1 = gr.idx(j);
+                const uint32_t e = (n1 * k2) & (uint32_t)(nn - 1);
+                const uint32_t w = inter_twiddle(c, q, 1, e, a.log_n, p, pinv);
+                row_a[n1] = mont_mul(x[j], w, p, pinv);
+            }
+        }
+    }
+}
+
+// ---- kernel 3: inverse column pass + CRT + chunk sums -------------------------
+
+struct InvColsArgs {
+    const uint32_t* z;  // [prime][N]
+    uint64_t* chunks;   // 4 limbs per chunk
+    uint64_t* spill;    // per chunk
+    int log_n, log_n1;
+};
+
+// Garner: residues (r0,r1,r2) -> the coefficient as 96 bits (< 2^89).
+__device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r1, uint32_t r2,
+                                     uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+    const uint32_t p1 = c.pr[1].p, p2 = c.pr[2].p, p0 = c.pr[0].p;
+    const uint32_t t1 = mont_mul_pre(mod_sub(r1, r0, p1), c.k1, c.k1p, p1);   // (r1-r0)/p0 mod p1
+    const uint32_t d2 = mod_sub(r2, r0, p2);
+    const uint32_t e2 = mont_mul_pre(t1, c.k2, c.k2p, p2);                    // p0*t1 mod p2
+    const uint32_t t2 = mont_mul_pre(mod_sub(d2, e2, p2), c.k3, c.k3p, p2);   // /(p0 p1) mod p2
+    // v = r0 + p0*t1 + p0*p1*t2
+    const uint64_t a = (uint64_t)p0 * t1 + r0;
+    const uint64_t blo = c.m01 * (uint64_t)t2;
+    const uint64_t bhi = __umul64hi(c.m01, (uint64_t)t2);
+    const uint64_t lo = a + blo;
+    const uint64_t hi = bhi + (lo < a ? 1u : 0u);
+    w0 = (uint32_t)lo;
+    w1 = (uint32_t)(lo >> 32);
+    w2 = (uint32_t)hi;
+}
+
+template <int L2, int T>
+__global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a, const NttConsts c) {
+    extern __shared__ __align__(16) uint32_t sm[];  // 3 x [2^L2][kCols]
+    using P2 = Plan<L2>;
+    constexpr int NR = P2::nr;
+    constexpr int TILE = kCols << L2;
+    const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
+    const size_t nn = (size_t)1 << a.log_n;
+
+#pragma unroll 1
+    for (int q = 0; q < kNumPrimes; ++q) {
+        uint32_t* s = sm + q * TILE;
+        const uint32_t p = c.pr[q].p;
+        const uint2* twi = c.stage[q][1];
+        const uint32_t* z = a.z + q * nn;
+        // Round NR-1 (lowest bits): load slots from global.
+        {
+            using Gr = Group<L2, kCols, NR - 1>;
+            constexpr int R = Gr::R;
+#pragma unroll 1
+            for (int g = threadIdx.x; g < Gr::G; g += T) {
+                const Gr gr(g);
+                uint32_t x[1 << R];
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j)
+                    x[j] = z[(size_t)gr.idx(j) * n1_len + c0 + gr.col];
+                dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) s[gr.idx(j) * kCols + gr.col] = x[j];
+            }
+        }
+        __syncthreads();
+        dit_rounds<L2, kCols, T, NR - 2, 0>(s, twi, p);
+    }
+
+    // CRT and chunk sums: row n2 of the tile is chunk (c0 + N1*n2)/8.
+#pragma unroll 1
+    for (uint32_t n2 = threadIdx.x; n2 < (1u << L2); n2 += T) {
+        uint32_t w0[kCols], w1[kCols], w2[kCols];
+        const uint4* s0 = reinterpret_cast<const uint4*>(sm + n2 * kCols);
+        const uint4* s1 = reinterpret_cast<const uint4*>(sm + TILE + n2 * kCols);
+        const uint4* s2 = reinterpret_cast<const uint4*>(sm + 2 * TILE + n2 * kCols);
+        uint32_t r0[kCols], r1[kCols], r2[kCols];
+#pragma unroll
+        for (int h = 0; h < kCols / 4; ++h) {
+            uint4 u = s0[h], v = s1[h], t = s2[h];
+            r0[4 * h] = u.x, r0[4 * h + 1] = u.y, r0[4 * h + 2] = u.z, r0[4 * h + 3] = u.w;
+            r1[4 * h] = v.x, r1[4 * h + 1] = v.y, r1[4 * h + 2] = v.z, r1[4 * h + 3] = v.w;
+            r2[4 * h] = t.x, r2[4 * h + 1] = t.y, r2[4 * h + 2] = t.z, r2[4 * h + 3] = t.w;
+        }
+#pragma unroll
+        for (int i = 0; i < kCols; ++i) crt3(c, r0[i], r1[i], r2[i], w0[i], w1[i], w2[i]);
+        // digit k = w0[k] + w1[k-1] + w2[k-2] + carry, k = 0..9
+        uint32_t d[kCols + 2];
+        uint64_t carry = 0;
+#pragma unroll
+        for (int k = 0; k < kCols + 2; ++k) {
+            uint64_t s = carry;
+            if (k < kCols) s += w0[k];
+            if (k >= 1 && k - 1 < kCols) s += w1[k - 1];
+            if (k >= 2 && k - 2 < kCols) s += w2[k - 2];
+            d[k] = (uint32_t)s;
+            carry = s >> 32;
+        }
+        const size_t chunk = (size_t)(c0 / kCols) + (size_t)(n1_len / kCols) * n2;
+        ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.chunks + chunk * 4);
+        dst[0] = make_ulonglong2(d[0] | ((uint64_t)d[1] << 32), d[2] | ((uint64_t)d[3] << 32));
+        dst[1] = make_ulonglong2(d[4] | ((uint64_t)d[5] << 32), d[6] | ((uint64_t)d[7] << 32));
+        a.spill[chunk] = d[8] | ((uint64_t)d[9] << 32);
+    }
+}
+
+// ---- kernel 4: carry scan with decoupled look-back ----------------------------
+
+constexpr int kCarryThreads = 256;
+constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait, then error exit
+
+struct CarryArgs {
+    const uint64_t* chunks;
+    const uint64_t* spill;
+    uint32_t nchunks;  // real chunks; chunk nchunks is a virtual all-zero chunk
+    void* out;
+    int out_fmt;
+    size_t out_cap;
+    uint64_t* flags;
+    unsigned long long* ticket;
+    uint64_t ticket_base;
+    uint64_t epoch;
+    uint32_t* err;
+};
+
+// Flag word: [63:4] epoch, [3:2] status (1 aggregate, 2 inclusive), [1] G/carry, [0] P.
+__device__ __forceinline__ uint64_t make_flag(uint64_t epoch, uint32_t status, uint32_t g,
+                                              uint32_t pbit) {
+    return (epoch << 4) | ((uint64_t)status << 2) | ((uint64_t)g << 1) | pbit;
+}
+
+__global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
+    __shared__ uint32_t s_bid, s_cin;
+    __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
+    if (threadIdx.x == 0) s_bid = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticket_base);
+    __syncthreads();
+    const uint32_t bid = s_bid;
+    const uint32_t j = bid * kCarryThreads + threadIdx.x;
+    const uint32_t ntot = a.nchunks + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    uint64_t S[4] = {0, 0, 0, 0};
+    uint32_t G = 0, P = 0;
+    uint64_t next_lo = 0, my_spill = 0;
+    if (j < ntot) {
+        if (j < a.nchunks) {
+            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(a.chunks + (size_t)j * 4);
+            ulonglong2 u = src[0], v = src[1];
+            S[0] = u.x, S[1] = u.y, S[2] = v.x, S[3] = v.y;
+            my_spill = a.spill[j];
+            if (j + 1 < a.nchunks) next_lo = a.chunks[(size_t)(j + 1) * 4];
+        }
+        const uint64_t s = j > 0 ? a.spill[j - 1] : 0;
+        uint64_t t = S[0] + s;
+        uint32_t cy = t < s;
+        S[0] = t;
+#pragma unroll
+        for (int k = 1; k < 4; ++k) {
+            t = S[k] + cy;
+            cy = cy & (t == 0);
+            S[k] = t;
+        }
+        G = cy;
+        P = (!cy) && ((S[0] & S[1] & S[2] & S[3]) == ~0ull);
+    }
+    const uint32_t gm = __ballot_sync(0xffffffffu, G);
+    const uint32_t pm = __ballot_sync(0xffffffffu, P);
+    const uint32_t bm = gm | pm;
+    if (lane == 0) {
+        s_wg[warp] = (uint32_t)((((uint64_t)gm + bm) >> 32) & 1u);
+        s_wp[warp] = (pm == 0xffffffffu);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t bG = 0, bP = 1;
+        for (int w = 0; w < kCarryThreads / 32; ++w) {
+            bG = s_wg[w] | (s_wp[w] & bG);
+            bP = bP & s_wp[w];
+        }
+        uint32_t cin = 0;
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> self(
+            *reinterpret_cast<unsigned long long*>(a.flags + bid));
+        if (bid == 0) {
+            self.store(make_flag(a.epoch, 2, bG, 0), cuda::memory_order_release);
+        } else {
+            self.store(make_flag(a.epoch, 1, bG, bP), cuda::memory_order_release);
+            int k = (int)bid - 1;
+            uint32_t spins = 0;
+            while (true) {
+                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pred(
+                    *reinterpret_cast<unsigned long long*>(a.flags + k));
+                const uint64_t f = pred.load(cuda::memory_order_acquire);
+                if ((f >> 4) != a.epoch) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(a.err, 1u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                const uint32_t st = (uint32_t)(f >> 2) & 3u, fg = (uint32_t)(f >> 1) & 1u,
+                               fp = (uint32_t)f & 1u;
+                if (st == 2) {
+                    cin = fg;
+                    break;
+                }
+                if (fg) {
+                    cin = 1;
+                    break;
+                }
+                if (!fp) {
+                    cin = 0;
+                    break;
+                }
+                --k;  // predecessor propagates: look further back (block 0 is inclusive)
+            }
+            self.store(make_flag(a.epoch, 2, bG | (bP & cin), 0), cuda::memory_order_release);
+        }
+        s_cin = cin;
+    }
+    __syncthreads();
+    uint32_t cw = s_cin;
+    for (int w = 0; w < warp; ++w) cw = s_wg[w] | (s_wp[w] & cw);
+    const uint64_t sum = (uint64_t)gm + bm + cw;
+    const uint32_t carries = (uint32_t)sum ^ gm ^ bm;
+    const uint32_t cin = (carries >> lane) & 1u;
+    if (j >= ntot) return;
+    uint32_t cy = cin;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint64_t t = S[k] + cy;
+        cy = cy & (t == 0);
+        S[k] = t;
+    }
+    if (a.out_fmt == kFmtLimb64) {
+        uint64_t* o = static_cast<uint64_t*>(a.out);
+        const size_t base = (size_t)j * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (base + k < a.out_cap) o[base + k] = S[k];
+    } else {
+        // Final low limb of chunk j+1: its raw limb + this chunk's spill + carry out.
+        const uint32_t cout = G | (P & cin);
+        const uint64_t nl = next_lo + my_spill + cout;
+        uint32_t* o = static_cast<uint32_t*>(a.out);
+        const uint64_t bit0 = (uint64_t)j * 256;
+        const uint64_t k0 = (bit0 + 27) / 28, k1 = (bit0 + 256 + 27) / 28;
+        for (uint64_t k = k0; k < k1 && k < a.out_cap; ++k) {
+            const uint32_t off = (uint32_t)(k * 28 - bit0);  // < 256
+            const uint32_t w = off >> 6, sh = off & 63;
+            const uint64_t lo = S[w];
+            const uint64_t hi = (w + 1 < 4) ? S[w + 1] : nl;
+            uint64_t v = lo >> sh;
+            if (sh > 36) v |= hi << (64 - sh);
+            o[k] = (uint32_t)v & ((1u << 28) - 1u);
+        }
+    }
+}
+
+// ---- host launchers -------------------------------------------------------------
+
+TransformShape choose_shape(int log_n) {
+    TransformShape s;
+    s.log_n = log_n;
+    int l2 = (log_n - 1) / 2;
+    if (l2 > 11) l2 = 11;
+    if (l2 < 2) l2 = 2;
+    s.log_n2 = l2;
+    s.log_n1 = log_n - l2;
+    return s;
+}
+
+bool shape_supported(int log_n, bool square) {
+    if (log_n < 5 || log_n > kMaxLogN) return false;
+    TransformShape s = choose_shape(log_n);
+    if (s.log_n1 < 3) return false;
+    if (s.log_n1 > 15) return false;
+    if (s.log_n1 == 15 && !square) return false;
+    return true;
+}
+
+size_t smem_fwd_cols(int l2) { return (size_t)kCols * 4 << l2; }
+size_t smem_mid_rows(int l1, bool square) { return (square ? 1 : 2) * ((size_t)4 << l1); }
+size_t smem_inv_cols(int l2) { return (size_t)kNumPrimes * kCols * 4 << l2; }
+
+static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1 << (l1 - 4)) : 32); }
+
+template <int L2>
+static cudaError_t launch_outer(const NttConsts& c, const FwdColsArgs* f, const InvColsArgs* inv,
+                                int nops, uint32_t tiles, cudaStream_t st) {
+    constexpr int T = 256;
+    if (f) {
+        auto k = k_fwd_cols<L2, T>;
+        size_t sm = smem_fwd_cols(L2);
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<dim3(tiles, kNumPrimes, nops), T, sm, st>>>(*f, c);
+    } else {
+        auto k = k_inv_cols<L2, T>;
+        size_t sm = smem_inv_cols(L2);
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<dim3(tiles), T, sm, st>>>(*inv, c);
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t dispatch_outer(int l2, const NttConsts& c, const FwdColsArgs* f,
+                                  const InvColsArgs* inv, int nops, uint32_t tiles,
+                                  cudaStream_t st) {
+    switch (l2) {
+        case 2: return launch_outer<2>(c, f, inv, nops, tiles, st);
+        case 3: return launch_outer<3>(c, f, inv, nops, tiles, st);
+        case 4: return launch_outer<4>(c, f, inv, nops, tiles, st);
+        case 5: return launch_outer<5>(c, f, inv, nops, tiles, st);
+        case 6: return launch_outer<6>(c, f, inv, nops, tiles, st);
+        case 7: return launch_outer<7>(c, f, inv, nops, tiles, st);
+        case 8: return launch_outer<8>(c, f, inv, nops, tiles, st);
+        case 9: return launch_outer<9>(c, f, inv, nops, tiles, st);
+        case 10: return launch_outer<10>(c, f, inv, nops, tiles, st);
+        case 11: return launch_outer<11>(c, f, inv, nops, tiles, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int L1>
+static cudaError_t launch_mid(const NttConsts& c, const MidRowsArgs& m, bool square, uint32_t rows,
+                              cudaStream_t st) {
+    constexpr int T = mid_threads(L1);
+    size_t sm = smem_mid_rows(L1, square);
+    if (square) {
+        auto k = k_mid_rows<L1, T, true>;
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m, c);
+    } else {
+        if constexpr (L1 <= 14) {
+            auto k = k_mid_rows<L1, T, false>;
+            if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m, c);
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t dispatch_mid(int l1, const NttConsts& c, const MidRowsArgs& m, bool square,
+                                uint32_t rows, cudaStream_t st) {
+    switch (l1) {
+        case 3: return launch_mid<3>(c, m, square, rows, st);
+        case 4: return launch_mid<4>(c, m, square, rows, st);
+        case 5: return launch_mid<5>(c, m, square, rows, st);
+        case 6: return launch_mid<6>(c, m, square, rows, st);
+        case 7: return launch_mid<7>(c, m, square, rows, st);
+        case 8: return launch_mid<8>(c, m, square, rows, st);
+        case 9: return launch_mid<9>(c, m, square, rows, st);
+        case 10: return launch_mid<10>(c, m, square, rows, st);
+        case 11: return launch_mid<11>(c, m, square, rows, st);
+        case 12: return launch_mid<12>(c, m, square, rows, st);
+        case 13: return launch_mid<13>(c, m, square, rows, st);
+        case 14: return launch_mid<14>(c, m, square, rows, st);
+        case 15: return launch_mid<15>(c, m, square, rows, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+uint32_t carry_blocks(uint32_t nchunks) {
+    return (nchunks + 1 + kCarryThreads - 1) / kCarryThreads;
+}
+
+static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
+
+cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
+                               bool square, int log_n, const ProductScratch& s, void* out,
+                               int out_fmt, size_t out_cap, const CarryLaunch& cl,
+                               cudaStream_t st) {
+    if (!shape_supported(log_n, square)) return cudaErrorInvalidValue;
+    const TransformShape sh = choose_shape(log_n);
+    const size_t nn = (size_t)1 << log_n;
+    const uint32_t tiles = (1u << sh.log_n1) / kCols;
+
+    FwdColsArgs f{};
+    f.op[0] = a;
+    f.op[1] = square ? a : b;
+    f.y = s.y;
+    f.log_n = log_n;
+    f.log_n1 = sh.log_n1;
+    cudaError_t e = dispatch_outer(sh.log_n2, c, &f, nullptr, square ? 1 : 2, tiles, st);
+    if (e != cudaSuccess) return e;
+
+    MidRowsArgs m{};
+    m.ya = s.y;
+    m.yb = square ? nullptr : s.y + kNumPrimes * nn;
+    m.log_n = log_n;
+    m.log_n2 = sh.log_n2;
+    for (int q = 0; q < kNumPrimes; ++q) {
+        const uint32_t p = c.pr[q].p;
+        // The pointwise Montgomery product leaves a factor 2^-32; the scale
+        // N^-1 * 2^32 (mod p) cancels it and applies the inverse's 1/N.
+        uint64_t ninv = 1, base = (p + 1) / 2;  // 2^-1 mod p
+        for (int i = 0; i < log_n; ++i) ninv = ninv * base % p;
+        const uint64_t r = ((uint64_t)1 << 32) % p;
+        const uint64_t v = ninv * r % p;
+        m.scale_w[q] = mont_of(v, p);
+        m.scale_wp[q] = m.scale_w[q] * c.pr[q].pinv;
+    }
+    e = dispatch_mid(sh.log_n1, c, m, square, 1u << sh.log_n2, st);
+    if (e != cudaSuccess) return e;
+
+    InvColsArgs iv{};
+    iv.z = s.y;
+    iv.chunks = s.chunks;
+    iv.spill = s.spill;
+    iv.log_n = log_n;
+    iv.log_n1 = sh.log_n1;
+    e = dispatch_outer(sh.log_n2, c, nullptr, &iv, 0, tiles, st);
+    if (e != cudaSuccess) return e;
+
+    CarryArgs ca{};
+    ca.chunks = s.chunks;
+    ca.spill = s.spill;
+    ca.nchunks = (uint32_t)(nn / kCols);
+    ca.out = out;
+    ca.out_fmt = out_fmt;
+    ca.out_cap = out_cap;
+    ca.flags = s.flags;
+    ca.ticket = s.ticket;
+    ca.ticket_base = cl.ticket_base;
+    ca.epoch = cl.epoch;
+    ca.err = s.err;
+    k_carry<<<carry_blocks(ca.nchunks), kCarryThreads, 0, st>>>(ca);
+    return cudaGetLastError();
+}
+
+}  // namespace bgpu

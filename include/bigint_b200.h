@@ -1,0 +1,103 @@
+/* bigint_b200 -- C-ABI of the B200 big-integer multiply engine.
+ *
+ * Drop-in boundary for the multiply path of Looading99/BigInt.  Each entry
+ * point states the reference interface it replaces (paths inside that
+ * project).  All functions are plain C: host pointers and sizes in, status
+ * code out; they never throw.  Device-pointer variants take a CUDA stream as
+ * `void*`.  Unless noted, calls are serialized by an internal mutex, like the
+ * reference's pool (src/mul/ntt_multithread.cpp:259-260).
+ *
+ * Conventions shared with the reference:
+ *  - u64 limbs and 28-bit Digits are little-endian.
+ *  - squaring is signalled by passing the SAME pointer (and length) for both
+ *    operands, as the reference detects it by address
+ *    (include/bigint/mul.h:225, src/mul/ntt_multithread.cpp:445).
+ *  - results carry no leading zero limbs/digits.
+ */
+#ifndef BIGINT_B200_H
+#define BIGINT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (0 = success). */
+#define BGPU_OK 0
+#define BGPU_ERR_INVALID_ARG -1   /* null pointer, zero length, digit >= 2^28 ... */
+#define BGPU_ERR_NO_DEVICE -2     /* no CUDA device / CUDA runtime error at init */
+#define BGPU_ERR_OOM -3           /* device or pinned-host allocation failed */
+#define BGPU_ERR_CAPACITY -4      /* product beyond the largest supported transform */
+#define BGPU_ERR_OUT_CAPACITY -5  /* caller's output buffer too small; *out_len = needed */
+#define BGPU_ERR_CUDA -6          /* CUDA error during the multiply */
+#define BGPU_ERR_DEVICE_TIMEOUT -7/* a bounded device-side wait gave up (carry look-back) */
+#define BGPU_ERR_NOT_INIT -8      /* bgpu_init() not called / failed */
+
+/* Method selection (flags & BGPU_METHOD_MASK). */
+#define BGPU_METHOD_AUTO 0u
+#define BGPU_METHOD_NTT 1u        /* three-prime NTT (the plain method) */
+#define BGPU_METHOD_SCHOOLBOOK 2u /* O(n*m) kernel; na + nb <= BGPU_SCHOOLBOOK_MAX_LIMBS */
+#define BGPU_METHOD_MASK 0xFu
+
+#define BGPU_SCHOOLBOOK_MAX_LIMBS 256u
+#define BGPU_MAX_LOG2_POINTS 26u  /* transform points are 32-bit digits */
+
+typedef struct bgpu_stats {
+    int32_t method;          /* BGPU_METHOD_* actually used */
+    uint32_t log2_points;    /* transform length (0 for schoolbook) */
+    double max_round_err;    /* floating-point forms: max |x - round(x)|; 0 otherwise */
+    int32_t fell_back;       /* floating-point forms: recomputed on the NTT */
+    float device_ms;         /* device time of the multiply kernels */
+} bgpu_stats;
+
+/* Select the CUDA device and build the twiddle tables.  Idempotent; a second
+ * call with another device re-initializes.  Replaces the reference's
+ * init_thread_pool (include/bigint/bigint.h:35-38) as the engine set-up. */
+int bgpu_init(int device);
+
+/* Release device tables, scratch and streams. */
+int bgpu_shutdown(void);
+
+/* Human-readable text for a status code. */
+const char* bgpu_strerror(int code);
+
+/* Product of u64-limb integers: the `_mul` seam (include/bigint/mul.h:208-220)
+ * and ntt::mul (src/mul/ntt_multithread.cpp:444-530).  Writes the product
+ * without leading zeros into out[0..*out_len).  A zero operand gives
+ * *out_len == 0 (brute::mul's result, include/bigint/mul.h:82-102). */
+int bgpu_mul_u64(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                 size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats);
+
+/* Product of 28-bit Digits: the mul_digits seam (include/bigint/mul.h:223-318),
+ * called from BigInt::operator* (include/bigint/bigint.h:289) and
+ * BigFloat::mul (include/bigint/bigint.h:576).  Same output_precision /
+ * point_pos semantics as the reference: with output_precision > 0 only the
+ * top digits of each operand are used, the result is cut to about that many
+ * digits and *point_pos is decreased by the digits dropped; with 0 the exact
+ * product is returned (low zero digits re-inserted).  point_pos may be NULL.
+ * Precondition as in the reference: neither operand is all zero
+ * (BGPU_ERR_INVALID_ARG instead of undefined behaviour). */
+int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
+                    size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
+                    size_t* out_len, uint32_t flags, bgpu_stats* stats);
+
+/* Device-resident product (no host copies, asynchronous on `stream`):
+ * d_out receives exactly na + nb limbs (zero padded).  d_a == d_b with
+ * na == nb squares.  Errors found on the device are sticky and reported by
+ * bgpu_device_status.  Not reentrant: one call in flight per process. */
+int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
+                        uint64_t* d_out, uint32_t flags, void* stream);
+
+/* Synchronize `stream` and return (and clear) the sticky device status. */
+int bgpu_device_status(void* stream);
+
+/* Number of kernel launches the last multiply issued (for bench accounting). */
+uint32_t bgpu_last_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BIGINT_B200_H */

@@ -1,0 +1,87 @@
+"""Build recipe for the CPU oracle (test infrastructure only).
+
+Two shared libraries come out of here:
+
+* ``oracle/liboracle.so`` -- the plain-C restatement in ``bigint_oracle.c``.
+* ``oracle/_ref/libbigint_ref.so`` -- the UNMODIFIED reference multiply path,
+  compiled directly from its own sources where they lie (``src/mul/*.cpp``,
+  ``src/bigint.cpp``) plus ``ref_shim.cpp``.  The reference targets MinGW; the
+  force-included ``ref_compat.h`` supplies the overloads four of its call sites
+  need on Linux (no source is copied or edited).  ``-flto`` from the
+  reference's CMake release flags is left out: the LTO plugin cannot run here.
+
+Usage: ``python oracle/build.py [port|ref|all]`` (default ``all``).  The
+reference tree is only needed for ``ref``; when it is absent that step is
+skipped and an existing ``oracle/_ref`` build is kept.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.environ.get("BIGINT_REF_ROOT", "/root/reference")
+REF_SOURCES = [
+    "src/mul/ntt_multithread.cpp",
+    "src/mul/fft.cpp",
+    "src/mul/ssa.cpp",
+    "src/bigint.cpp",
+]
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+REF_SO = os.path.join(REF_DIR, "libbigint_ref.so")
+
+
+def _run(cmd: list[str]) -> None:
+    subprocess.run(cmd, check=True)
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_port(force: bool = False) -> str:
+    src = os.path.join(HERE, "bigint_oracle.c")
+    hdr = os.path.join(HERE, "bigint_oracle.h")
+    if force or _stale(PORT_SO, [src, hdr, __file__]):
+        _run(["gcc", "-O2", "-std=c11", "-Wall", "-Wextra", "-fPIC", "-shared", src, "-o", PORT_SO])
+    return PORT_SO
+
+
+def build_ref(force: bool = False) -> str | None:
+    if not os.path.isdir(os.path.join(REF_ROOT, "src")):
+        return REF_SO if os.path.exists(REF_SO) else None
+    os.makedirs(REF_DIR, exist_ok=True)
+    shim = os.path.join(HERE, "ref_shim.cpp")
+    compat = os.path.join(HERE, "ref_compat.h")
+    srcs = [os.path.join(REF_ROOT, s) for s in REF_SOURCES]
+    if not (force or _stale(REF_SO, srcs + [shim, compat, __file__])):
+        return REF_SO
+    flags = ["-std=c++20", "-O3", "-DNDEBUG", "-mavx", "-mavx2", "-mfma", "-fPIC", "-pthread",
+             "-include", compat, "-I", os.path.join(REF_ROOT, "include")]
+    objs = []
+    for s in srcs + [shim]:
+        o = os.path.join(REF_DIR, os.path.basename(s).replace(".cpp", ".o"))
+        _run(["g++", *flags, "-c", s, "-o", o])
+        objs.append(o)
+    _run(["g++", "-shared", "-pthread", *objs, "-o", REF_SO])
+    for o in objs:
+        os.remove(o)
+    return REF_SO
+
+
+def main(argv: list[str]) -> int:
+    what = argv[1] if len(argv) > 1 else "all"
+    if what in ("port", "all"):
+        print("oracle port:", build_port())
+    if what in ("ref", "all"):
+        print("oracle reference:", build_ref())
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv))

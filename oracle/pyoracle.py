@@ -1,0 +1,207 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+``Port`` wraps ``oracle/liboracle.so`` (the C restatement); ``Reference``
+wraps ``oracle/_ref/libbigint_ref.so`` (the unmodified reference compiled by
+``oracle/build.py``).  Only the tests, ``__graft_entry__.smoke()`` and the
+bench's CPU legs import this module; it is the checker, never the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libbigint_ref.so")
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_szp = C.POINTER(C.c_size_t)
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(_u64p)
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(_u32p)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _limbs(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint64))
+
+
+def _digits(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.uint32))
+
+
+class _Lib:
+    def __init__(self, path: str):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library not built: {path} (run python oracle/build.py)")
+        self.path = path
+        self.lib = C.CDLL(path)
+
+    def _mul64(self, fn, a, b, *extra, same: bool = False) -> np.ndarray:
+        a = _limbs(a)
+        b = a if same else _limbs(b)
+        cap = a.size + b.size + 2
+        out = np.zeros(max(cap, 1), dtype=np.uint64)
+        n = C.c_size_t(0)
+        pa = _p64(a) if a.size else _p64(np.zeros(1, np.uint64))
+        pb = pa if same else (_p64(b) if b.size else _p64(np.zeros(1, np.uint64)))
+        rc = fn(pa, a.size, pb, b.size, *extra, _p64(out), cap, C.byref(n))
+        if rc != 0:
+            raise OracleError(f"{fn.__name__} returned {rc}")
+        return out[: n.value].copy()
+
+
+class Port(_Lib):
+    """The plain-C restatement (oracle/bigint_oracle.c)."""
+
+    def __init__(self, path: str = PORT_SO):
+        super().__init__(path)
+        L = self.lib
+        for name in ("orc_ntt_mul", "orc_brute_mul", "orc_mul"):
+            f = getattr(L, name)
+            f.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, _u64p, C.c_size_t, _szp]
+            f.restype = C.c_int
+        L.orc_mul_digits.argtypes = [_u32p, C.c_size_t, _u32p, C.c_size_t, C.c_int, C.c_size_t,
+                                     C.POINTER(C.c_int64), _u32p, C.c_size_t, _szp]
+        L.orc_mul_digits.restype = C.c_int
+        L.orc_mod_m61.argtypes = [_u64p, C.c_size_t]
+        L.orc_mod_m61.restype = C.c_uint64
+        L.orc_product_tree.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, _szp]
+        L.orc_product_tree.restype = C.c_int
+
+    def ntt_mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.orc_ntt_mul, a, b, same=b is None)
+
+    def brute_mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.orc_brute_mul, a, b, same=b is None)
+
+    def mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.orc_mul, a, b, same=b is None)
+
+    def mul_digits(self, a, b=None, output_precision: int = 0, point_pos: int | None = None):
+        return _mul_digits(self.lib.orc_mul_digits, a, b, output_precision, point_pos)
+
+    def mod_m61(self, x) -> int:
+        x = _limbs(x)
+        if x.size == 0:
+            return 0
+        return int(self.lib.orc_mod_m61(_p64(x), x.size))
+
+    def product_tree(self, leaves) -> np.ndarray:
+        leaves = _limbs(leaves)
+        cap = leaves.size + 2
+        out = np.zeros(cap, dtype=np.uint64)
+        n = C.c_size_t(0)
+        rc = self.lib.orc_product_tree(_p64(leaves), leaves.size, _p64(out), cap, C.byref(n))
+        if rc != 0:
+            raise OracleError(f"orc_product_tree returned {rc}")
+        return out[: n.value].copy()
+
+
+def _mul_digits(fn, a, b, output_precision, point_pos):
+    a = _digits(a)
+    same = b is None
+    b = a if same else _digits(b)
+    cap = a.size + b.size + 4
+    out = np.zeros(cap, dtype=np.uint32)
+    n = C.c_size_t(0)
+    pp = C.c_int64(point_pos if point_pos is not None else 0)
+    rc = fn(_p32(a), a.size, _p32(b), b.size, int(same), int(output_precision),
+            C.byref(pp) if point_pos is not None else None, _p32(out), cap, C.byref(n))
+    if rc != 0:
+        raise OracleError(f"mul_digits returned {rc}")
+    res = out[: n.value].copy()
+    if point_pos is not None:
+        return res, int(pp.value)
+    return res
+
+
+class Reference(_Lib):
+    """The unmodified reference path (oracle/_ref/libbigint_ref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        super().__init__(path)
+        L = self.lib
+        for name in ("ref_ntt_mul", "ref_ssa_mul", "ref_brute_mul", "ref_mul"):
+            f = getattr(L, name)
+            f.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, _u64p, C.c_size_t, _szp]
+            f.restype = C.c_int
+        L.ref_fft_mul.argtypes = [_u64p, C.c_size_t, _u64p, C.c_size_t, C.c_int, _u64p,
+                                  C.c_size_t, _szp]
+        L.ref_fft_mul.restype = C.c_int
+        L.ref_mul_digits.argtypes = [_u32p, C.c_size_t, _u32p, C.c_size_t, C.c_int, C.c_size_t,
+                                     C.POINTER(C.c_int64), _u32p, C.c_size_t, _szp]
+        L.ref_mul_digits.restype = C.c_int
+        L.ref_product_tree.argtypes = [_u64p, C.c_size_t, _u32p, C.c_size_t, _szp]
+        L.ref_product_tree.restype = C.c_int
+        L.ref_init_thread_pool.argtypes = [C.c_uint32]
+        L.ref_init_thread_pool.restype = None
+
+    def init_thread_pool(self, n: int) -> None:
+        """First call wins (ntt_multithread.cpp:287-290); 0/1 disables threads."""
+        self.lib.ref_init_thread_pool(int(n))
+
+    def ntt_mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.ref_ntt_mul, a, b, same=b is None)
+
+    def ssa_mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.ref_ssa_mul, a, b, same=b is None)
+
+    def brute_mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.ref_brute_mul, a, b, same=b is None)
+
+    def mul(self, a, b=None) -> np.ndarray:
+        return self._mul64(self.lib.ref_mul, a, b, same=b is None)
+
+    def fft_mul(self, a, b=None, digit_bits: int = 0) -> np.ndarray:
+        return self._mul64(self.lib.ref_fft_mul, a, b, int(digit_bits), same=b is None)
+
+    def mul_digits(self, a, b=None, output_precision: int = 0, point_pos: int | None = None):
+        return _mul_digits(self.lib.ref_mul_digits, a, b, output_precision, point_pos)
+
+    def product_tree_digits(self, leaves) -> np.ndarray:
+        leaves = _limbs(leaves)
+        cap = (leaves.size * 64) // 28 + 8
+        out = np.zeros(cap, dtype=np.uint32)
+        n = C.c_size_t(0)
+        rc = self.lib.ref_product_tree(_p64(leaves), leaves.size, _p32(out), cap, C.byref(n))
+        if rc != 0:
+            raise OracleError(f"ref_product_tree returned {rc}")
+        return out[: n.value].copy()
+
+
+def have_reference() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def digits28_to_limbs(d) -> np.ndarray:
+    """Pack little-endian 28-bit digits into u64 limbs (leading zeros stripped)."""
+    d = _digits(d)
+    v = 0
+    for i in range(d.size - 1, -1, -1):
+        v = (v << 28) | int(d[i])
+    return int_to_limbs(v)
+
+
+def int_to_limbs(v: int) -> np.ndarray:
+    out = []
+    while v:
+        out.append(v & 0xFFFFFFFFFFFFFFFF)
+        v >>= 64
+    return np.array(out, dtype=np.uint64)
+
+
+def limbs_to_int(x) -> int:
+    x = _limbs(x)
+    return int.from_bytes(x.astype("<u8").tobytes(), "little")

@@ -1,0 +1,124 @@
+// C-ABI shim over the UNMODIFIED reference multiply path (Looading99/BigInt),
+// compiled together with the reference's own sources into
+// oracle/_ref/libbigint_ref.so by oracle/build_ref.sh.  It is test
+// infrastructure: the parity tests, the golden-vector generator and the
+// bench's CPU reference arm load it; the product never does.
+//
+// Every function forwards to one reference entry point:
+//   ref_ntt_mul     -> bigint::mul::ntt::mul      src/mul/ntt_multithread.cpp:444
+//   ref_fft_mul     -> bigint::mul::fft::mul      src/mul/fft.cpp:281
+//   ref_ssa_mul     -> bigint::mul::ssa::mul      src/mul/ssa.cpp:383
+//   ref_brute_mul   -> bigint::mul::brute::mul    include/bigint/mul.h:82
+//   ref_mul         -> bigint::mul::_mul          include/bigint/mul.h:208
+//   ref_mul_digits  -> bigint::mul::mul_digits    include/bigint/mul.h:223
+//   ref_product_tree-> BigInt::operator* (bigint.h:284) over a pairwise tree
+//   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
+// Results are copied into caller buffers; return 0 on success, -1 when the
+// caller's buffer is too small (out_len then holds the needed size).
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <span>
+#include <vector>
+
+#include "bigint/bigint.h"
+#include "bigint/mul.h"
+
+namespace {
+
+int copy_out64(const std::vector<uint64_t>& r, uint64_t* out, size_t cap, size_t* out_len) {
+    *out_len = r.size();
+    if (r.size() > cap) return -1;
+    if (!r.empty()) std::memcpy(out, r.data(), r.size() * sizeof(uint64_t));
+    return 0;
+}
+
+int copy_out32(const std::vector<uint32_t>& r, uint32_t* out, size_t cap, size_t* out_len) {
+    *out_len = r.size();
+    if (r.size() > cap) return -1;
+    if (!r.empty()) std::memcpy(out, r.data(), r.size() * sizeof(uint32_t));
+    return 0;
+}
+
+// The reference detects squaring by pointer identity (ntt_multithread.cpp:445,
+// fft.cpp:283, mul.h:225); passing the same pointer for a and b reproduces it.
+std::span<const uint64_t> span_b(const uint64_t* a, size_t na, const uint64_t* b, size_t nb) {
+    if (a == b && na == nb) return std::span<const uint64_t>(a, na);
+    return std::span<const uint64_t>(b, nb);
+}
+
+}  // namespace
+
+extern "C" {
+
+void ref_init_thread_pool(uint32_t n) { bigint::init_thread_pool(n); }
+
+int ref_ntt_mul(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                size_t cap, size_t* out_len) {
+    auto r = bigint::mul::ntt::mul(std::span<const uint64_t>(a, na), span_b(a, na, b, nb));
+    return copy_out64(r, out, cap, out_len);
+}
+
+int ref_fft_mul(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, int digit_bits,
+                uint64_t* out, size_t cap, size_t* out_len) {
+    auto r = bigint::mul::fft::mul(std::span<const uint64_t>(a, na), span_b(a, na, b, nb),
+                                   digit_bits);
+    return copy_out64(r, out, cap, out_len);
+}
+
+int ref_ssa_mul(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                size_t cap, size_t* out_len) {
+    auto r = bigint::mul::ssa::mul(std::span<const uint64_t>(a, na), span_b(a, na, b, nb));
+    return copy_out64(r, out, cap, out_len);
+}
+
+int ref_brute_mul(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                  size_t cap, size_t* out_len) {
+    auto r = bigint::mul::brute::mul(std::span<const uint64_t>(a, na), span_b(a, na, b, nb));
+    return copy_out64(r, out, cap, out_len);
+}
+
+int ref_mul(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+            size_t cap, size_t* out_len) {
+    auto r = bigint::mul::_mul(std::span<const uint64_t>(a, na), span_b(a, na, b, nb));
+    return copy_out64(r, out, cap, out_len);
+}
+
+// mul_digits takes `const Digits&`; squaring is `&a == &b`, so `same` != 0
+// passes one vector twice.  point_pos may be null (the reference allows it).
+int ref_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb, int same,
+                   size_t output_precision, int64_t* point_pos, uint32_t* out, size_t cap,
+                   size_t* out_len) {
+    bigint::Digits da(a, a + na);
+    if (same) {
+        auto r = bigint::mul::mul_digits(da, da, output_precision, point_pos);
+        return copy_out32(r, out, cap, out_len);
+    }
+    bigint::Digits db(b, b + nb);
+    auto r = bigint::mul::mul_digits(da, db, output_precision, point_pos);
+    return copy_out32(r, out, cap, out_len);
+}
+
+// Binary-splitting style product tree: leaves are u64 values; each level
+// multiplies neighbours pairwise with BigInt::operator* (odd tail carried up).
+// The product is returned as reference 28-bit Digits.
+int ref_product_tree(const uint64_t* leaves, size_t n, uint32_t* out, size_t cap,
+                     size_t* out_len) {
+    std::vector<bigint::BigInt> level;
+    level.reserve(n);
+    for (size_t i = 0; i < n; ++i) level.emplace_back(leaves[i]);
+    while (level.size() > 1) {
+        std::vector<bigint::BigInt> next;
+        next.reserve((level.size() + 1) / 2);
+        for (size_t i = 0; i + 1 < level.size(); i += 2) next.push_back(level[i] * level[i + 1]);
+        if (level.size() % 2) next.push_back(std::move(level.back()));
+        level = std::move(next);
+    }
+    if (level.empty()) {
+        *out_len = 0;
+        return 0;
+    }
+    return copy_out32(level[0].get_data(), out, cap, out_len);
+}
+
+}  // extern "C"

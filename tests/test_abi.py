@@ -1,0 +1,86 @@
+"""C-ABI surface checks that need no GPU: the library loads, exports every
+entry point declared in include/*.h, and rejects bad arguments on the host
+before touching a device."""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+LIB = os.path.join(ROOT, "bigint_b200", "libbigint_b200.so")
+
+
+def declared_functions() -> list[str]:
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*[A-Za-z_][\w\s\*]*?\b(bgpu_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from bigint_b200.build import build
+
+    build()
+    import bigint_b200
+
+    return bigint_b200.lib
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("bgpu_init", "bgpu_shutdown", "bgpu_strerror", "bgpu_mul_u64", "bgpu_mul_digits",
+                 "bgpu_mul_u64_device", "bgpu_device_status"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r"\bT\s+(bgpu_\w+)", out))
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+    for n in declared_functions():
+        assert hasattr(lib, n)
+
+
+def test_strerror(lib):
+    assert lib.bgpu_strerror(0) == b"ok"
+    assert b"output buffer" in lib.bgpu_strerror(-5)
+    assert lib.bgpu_strerror(12345) == b"unknown status"
+
+
+def test_invalid_arguments_rejected_on_host(lib):
+    u64p = C.POINTER(C.c_uint64)
+    n = C.c_size_t(0)
+    a = np.ones(4, dtype=np.uint64)
+    pa = a.ctypes.data_as(u64p)
+    assert lib.bgpu_mul_u64(None, 4, pa, 4, pa, 8, C.byref(n), 0, None) == -1
+    assert lib.bgpu_mul_u64(pa, 0, pa, 4, pa, 8, C.byref(n), 0, None) == -1
+    assert lib.bgpu_mul_u64(pa, 4, pa, 4, pa, 8, None, 0, None) == -1
+    assert lib.bgpu_mul_u64(pa, 4, pa, 4, pa, 8, C.byref(n), 7, None) == -1  # unknown method
+    u32p = C.POINTER(C.c_uint32)
+    d = np.ones(4, dtype=np.uint32)
+    pd = d.ctypes.data_as(u32p)
+    assert lib.bgpu_mul_digits(pd, 0, pd, 4, 0, None, pd, 8, C.byref(n), 0, None) == -1
+    assert lib.bgpu_mul_u64_device(None, 1, None, 1, None, 0, None) == -1
+
+
+def test_calls_before_init_report_not_initialized(lib):
+    lib.bgpu_shutdown()
+    u64p = C.POINTER(C.c_uint64)
+    n = C.c_size_t(0)
+    a = np.ones(4, dtype=np.uint64)
+    out = np.zeros(8, dtype=np.uint64)
+    pa = a.ctypes.data_as(u64p)
+    assert lib.bgpu_mul_u64(pa, 4, pa, 4, out.ctypes.data_as(u64p), 8, C.byref(n), 0, None) == -8
+    assert lib.bgpu_device_status(None) == -8
