@@ -1,0 +1,467 @@
+"""Benchmark: bit-exact big-integer products per second on one B200.
+
+Workload (one step = one product): the plain three-prime NTT multiply of two
+2^24-bit operands (262144 x 262144 u64 limbs), seeded uniform random limbs
+with the top bit set -- the size the project's roofline target is stated at.
+Inputs are generated on the host with a fixed seed and are synthetic.
+
+Our arm (default):
+  value      products/s with inputs resident in HBM (bgpu_mul_u64_device on a
+             torch stream), K products back to back between two CUDA events;
+             step i multiplies operand pair i mod P, where the P pairs together
+             are larger than L2, so no step starts with its inputs cached.
+  e2e        the same metric through the public host API (bgpu_mul_u64) from
+             pinned host buffers: H2D of both operands, the kernels, D2H of the
+             product, every step (wall clock around the synchronous call).
+  roofline   dominant kernel of the pipeline: its algorithmic bytes per launch
+             / its mean CUDA-event duration, against MEASURED_PEAKS.json.
+  cpu_baseline  the reference's own CPU multiply (oracle/_ref, its thread
+             pool at the host's core count) on a bounded sample, rank 0 only.
+Reference arm (--impl reference): the reference CPU multiply on the host
+cores for the same workload; rank 0 prints, other ranks exit.
+
+Multi-GPU: products are independent, so N GPUs run N replicas ("replicas
+only", weak scaling); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+SEED = 0x9E3779B97F4A7C15
+CONFIG_INDEX = 1  # the plain-NTT size sweep's 2^24-bit point
+OPERAND_BITS = 1 << 24
+L2_BYTES = 126 << 20  # B200 L2; inputs of all operand pairs together exceed it
+
+
+def make_operands(bits: int = OPERAND_BITS, seed: int = SEED + CONFIG_INDEX, pairs: int = 1):
+    """`pairs` seeded operand pairs (uniform limbs, top bit set), as (pairs, n) arrays."""
+    rng = np.random.default_rng(seed)
+    n = bits // 64
+    a = rng.integers(0, 2**64, (pairs, n), dtype=np.uint64, endpoint=False)
+    b = rng.integers(0, 2**64, (pairs, n), dtype=np.uint64, endpoint=False)
+    a[:, -1] |= np.uint64(1 << 63)
+    b[:, -1] |= np.uint64(1 << 63)
+    if pairs == 1:
+        return a[0], b[0]
+    return a, b
+
+
+def pairs_beyond_l2(bits: int) -> int:
+    """Distinct operand pairs whose inputs together are twice the L2 cache."""
+    per_pair = 2 * bits // 8
+    return max(2, -(-2 * L2_BYTES // per_pair))
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def workload_name(bits: int) -> str:
+    return (f"plain three-prime NTT multiply, 2^{bits.bit_length() - 1} x 2^{bits.bit_length() - 1}"
+            f"-bit operands ({bits // 64} x {bits // 64} u64 limbs), seeded uniform random limbs")
+
+
+# ---- distributed helpers -------------------------------------------------------
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reduce_max(value: float, world: int, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity when world == 1)."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ---- clocks sampling -------------------------------------------------------------
+
+def pci_bus_id(device) -> str | None:
+    """NVML-style PCI bus id ("00000000:1B:00.0") of a torch CUDA device."""
+    import torch
+
+    p = torch.cuda.get_device_properties(device)
+    try:
+        return f"{int(p.pci_domain_id):08X}:{int(p.pci_bus_id):02X}:{int(p.pci_device_id):02X}.0"
+    except (AttributeError, TypeError, ValueError):
+        return None
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML (the library
+    nvidia-smi reads) every `period` seconds on a background thread while the
+    timed region runs.  Read-only: no GPU setting is touched."""
+
+    NAMES = {
+        "nvmlClocksEventReasonSwPowerCap": "sw_power_cap",
+        "nvmlClocksEventReasonHwSlowdown": "hw_slowdown",
+        "nvmlClocksEventReasonHwThermalSlowdown": "hw_thermal_slowdown",
+        "nvmlClocksEventReasonSwThermalSlowdown": "sw_thermal_slowdown",
+        "nvmlClocksEventReasonHwPowerBrakeSlowdown": "hw_power_brake_slowdown",
+        "nvmlClocksEventReasonSyncBoost": "sync_boost",
+        "nvmlClocksEventReasonApplicationsClocksSetting": "applications_clocks_setting",
+        "nvmlClocksEventReasonDisplayClockSetting": "display_clock_setting",
+    }
+
+    def __init__(self, pci_bus_id: str | None, period: float = 0.002):
+        self.pci = pci_bus_id
+        self.period = period
+        self.samples: list[tuple[int, int]] = []
+        self.smax = None
+        self._stop = None
+        self._thread = None
+        self.error = None
+
+    def __enter__(self):
+        import threading
+
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = None
+            if self.pci:
+                try:
+                    h = pynvml.nvmlDeviceGetHandleByPciBusId(self.pci)
+                except Exception:
+                    h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(0)
+            self.smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self._pynvml, self._h, self._get_reasons = pynvml, h, get_reasons
+        except Exception as e:  # NVML missing: report unsampled
+            self.error = repr(e)
+            return self
+        self._stop = threading.Event()
+
+        def loop():
+            while not self._stop.is_set():
+                try:
+                    sm = self._pynvml.nvmlDeviceGetClockInfo(self._h, self._pynvml.NVML_CLOCK_SM)
+                    rs = int(self._get_reasons(self._h))
+                    self.samples.append((sm, rs))
+                except Exception as e:  # pragma: no cover
+                    self.error = repr(e)
+                    return
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["unsampled"],
+                    "samples": 0, "source": "nvml", "error": self.error}
+        reasons = set()
+        for _, rs in self.samples:
+            for attr, name in self.NAMES.items():
+                bit = getattr(self._pynvml, attr, 0)
+                if bit and rs & bit:
+                    reasons.add(name)
+        sm = [v for v, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.smax,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
+
+
+# ---- roofline --------------------------------------------------------------------
+
+def measured_peaks() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def kernel_bytes(name: str, na: int, nb: int, log_n: int, square: bool) -> int:
+    """Algorithmic global-memory bytes of one launch (minimal reads + writes)."""
+    n = 1 << log_n
+    s32 = 12 * n  # one operand's residues: 3 primes x u32 per point
+    ops = 1 if square else 2
+    inp = (na + (0 if square else nb)) * 8
+    chunk_bytes = n // 2 * 8 + n // 8 * 8  # 256-bit chunk sums + spills
+    return {
+        "k_fwd_cols": inp + ops * s32,
+        "k_mid_rows": ops * s32 + s32,
+        "k_inv_cols": s32 + chunk_bytes,
+        "k_carry": chunk_bytes + (na + nb) * 8,
+    }[name]
+
+
+def reference_model_bytes(na: int, nb: int) -> int:
+    """Whole-product bytes of the two-pass NTT model pinned to the reference's
+    28-bit digits: 10*S + 2*(a+b)/8 with S = 12*N, N = bit_ceil(da+db-1)."""
+    da, db = -(-na * 64 // 28), -(-nb * 64 // 28)
+    n = 1 << (da + db - 2).bit_length()
+    return 10 * 12 * n + 2 * (na + nb) * 8
+
+
+def profiled_traffic(kernel: str) -> float | None:
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ntt_2p24_traffic.json")
+    try:
+        return float(json.load(open(path))[kernel]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+# ---- CPU baseline ----------------------------------------------------------------
+
+def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int):
+    """Products/s of the reference CPU multiply (or the C port when the
+    reference library was not built), over a bounded sample."""
+    from oracle.pyoracle import Port, Reference, have_reference
+
+    if have_reference():
+        impl, kind, cores = Reference(), "reference", threads
+        impl.init_thread_pool(threads)
+        fn = impl.mul
+    else:
+        impl, kind, cores = Port(), "port", 1
+        fn = impl.ntt_mul
+    fn(a[:1024], b[:1024])  # warm the pool
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        fn(a, b)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= max_reps:
+            break
+    return reps / el, kind, cores, reps, el
+
+
+# ---- arms --------------------------------------------------------------------------
+
+def run_reference_arm(args) -> None:
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    a, b = make_operands(args.bits)
+    threads = host_cores()
+    from oracle.pyoracle import Port, Reference, have_reference
+
+    if have_reference():
+        impl, kind, cores = Reference(), "reference", threads
+        impl.init_thread_pool(threads)
+        fn = impl.mul
+    else:
+        impl, kind, cores = Port(), "port", 1
+        fn = impl.ntt_mul
+    for _ in range(args.warmup):
+        fn(a, b)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fn(a, b)
+    el = time.perf_counter() - t0
+    value = args.steps / el
+    line = {
+        "impl": "reference",
+        "metric": "bit-exact products/s (2^24 x 2^24-bit multiply)",
+        "value": value, "unit": "products/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name(args.bits), "call": "bigint::mul::_mul",
+                   "threads": cores, "parallelism": "host threads (init_thread_pool)"},
+        "cpu_baseline": {"value": value, "unit": "products/s", "cores": cores, "kind": kind,
+                         "sample": f"{args.steps} products of the full workload after "
+                                   f"{args.warmup} warm-up products"},
+        "e2e": {"value": value, "unit": "products/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_gpu_arm(args) -> None:
+    import torch
+
+    world, rank, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import bigint_b200 as bb
+    from oracle.pyoracle import Port
+
+    bb.init(local)
+    npairs = pairs_beyond_l2(args.bits)
+    A, B = make_operands(args.bits, pairs=npairs)
+    na = nb = A.shape[1]
+    dA = torch.from_numpy(A.view(np.int64)).to(device)
+    dB = torch.from_numpy(B.view(np.int64)).to(device)
+    dOut = torch.empty((npairs, na + nb), dtype=torch.int64, device=device)
+    stream = torch.cuda.Stream(device)
+    sptr = stream.cuda_stream
+
+    def step(i):
+        k = i % npairs
+        bb.mul_device(dA[k].data_ptr(), na, dB[k].data_ptr(), nb, dOut[k].data_ptr(), stream=sptr)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+    bb.device_status(sptr)
+    launches_per_step = bb.last_launch_count()
+
+    # Timed region: K back-to-back products on one stream.  Step i uses operand
+    # pair i mod npairs; all pairs together exceed L2, so no step finds its
+    # inputs cached by the previous one.  Per-kernel events ride along.
+    bb.set_kernel_timing(True)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world, device)
+    torch.cuda.synchronize(device)
+    with ClockSampler(pci_bus_id(device)) as clk:
+        with torch.cuda.stream(stream):
+            t0.record(stream)
+            for i in range(args.steps):
+                step(args.warmup + i)
+            t1.record(stream)
+        torch.cuda.synchronize(device)
+    barrier(world, device)
+    ktimes, kcount = bb.kernel_times()
+    bb.set_kernel_timing(False)
+    bb.device_status(sptr)
+    total_ms = reduce_max(t0.elapsed_time(t1), world, device)
+    clocks = clk.summary()
+
+    # correctness of every timed output: residue identity mod 2^61-1
+    port = Port()
+    M = (1 << 61) - 1
+    out_host = dOut.cpu().numpy().view(np.uint64)
+    for k in range(min(npairs, args.warmup + args.steps)):
+        if (port.mod_m61(A[k]) * port.mod_m61(B[k])) % M != port.mod_m61(out_host[k]):
+            raise SystemExit(f"bench: product {k} failed the mod 2^61-1 residue check")
+
+    # e2e through the public host API from pinned buffers (synchronous call)
+    pA = torch.from_numpy(A.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    pB = torch.from_numpy(B.view(np.int64)).pin_memory().numpy().view(np.uint64)
+    pOut = torch.empty((npairs, na + nb), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    e2e_steps = min(args.steps, 100)
+    for i in range(2):
+        bb.mul(pA[i], pB[i], out=pOut[i])
+    torch.cuda.synchronize(device)
+    barrier(world, device)
+    te = time.perf_counter()
+    for i in range(e2e_steps):
+        k = i % npairs
+        bb.mul(pA[k], pB[k], out=pOut[k])
+    e2e_s = reduce_max(time.perf_counter() - te, world, device)
+    for k in range(min(npairs, e2e_steps)):
+        if not np.array_equal(pOut[k], out_host[k]):
+            raise SystemExit("bench: host-API product differs from the device-resident product")
+
+    # roofline of the dominant kernel
+    log_n = (2 * na + 2 * nb - 2).bit_length()
+    mean_k = dict(ktimes)
+    dom = max(mean_k, key=mean_k.get)
+    dom_bytes = kernel_bytes(dom, na, nb, log_n, square=False)
+    peak, peak_kind = measured_peaks()
+    achieved = dom_bytes / (mean_k[dom] * 1e-3) / 1e9
+    prod_ms = total_ms / args.steps
+    model_b = reference_model_bytes(na, nb)
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, reps, el = cpu_reference_rate(A[0], B[0], args.cpu_seconds, 50,
+                                                         host_cores())
+        cpu = {"value": rate, "unit": "products/s", "cores": cores, "kind": kind,
+               "sample": f"{reps} full 2^24 x 2^24-bit products in {el:.1f} s "
+                         f"({'bigint::mul::_mul' if kind == 'reference' else 'C port ntt_mul'})"}
+
+    value = world * args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": "bit-exact products/s (2^24 x 2^24-bit multiply)",
+        "value": value, "unit": "products/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": prod_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name(args.bits), "method": "ntt",
+                   "transform_points": 1 << log_n, "digit_bits": 32,
+                   "l2": f"inputs larger than L2: {npairs} distinct operand pairs "
+                         f"({npairs * 2 * na * 8 >> 20} MiB) cycled, steps back to back",
+                   "parallelism": f"replicas x{world}", "verified": "residue mod 2^61-1, every output"},
+        "e2e": {"value": world * e2e_steps / e2e_s, "unit": "products/s",
+                "h2d_bytes_per_step": (na + nb) * 8, "d2h_bytes_per_step": (na + nb) * 8 + 4},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": profiled_traffic(dom), "algorithmic_bytes": dom_bytes,
+                     "kernel_ms": mean_k[dom], "kernels_ms": mean_k, "kernel_samples": kcount,
+                     "reference_model": {"bytes_per_product": model_b,
+                                         "achieved": model_b / (prod_ms * 1e-3) / 1e9,
+                                         "frac": model_b / (prod_ms * 1e-3) / 1e9 / peak}},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+    }
+    print(json.dumps(line))
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--bits", type=int, default=OPERAND_BITS)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

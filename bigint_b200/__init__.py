@@ -31,6 +31,7 @@ from ._lib import (  # noqa: F401
     brute_mul,
     device_status,
     init,
+    kernel_times,
     last_launch_count,
     lib,
     library_path,
@@ -38,5 +39,6 @@ from ._lib import (  # noqa: F401
     mul_device,
     mul_digits,
     ntt_mul,
+    set_kernel_timing,
     shutdown,
 )

@@ -81,6 +81,11 @@ def _load() -> C.CDLL:
     L.bgpu_device_status.restype = C.c_int
     L.bgpu_last_launch_count.argtypes = []
     L.bgpu_last_launch_count.restype = C.c_uint32
+    L.bgpu_set_kernel_timing.argtypes = [C.c_int]
+    L.bgpu_set_kernel_timing.restype = C.c_int
+    L.bgpu_kernel_times.argtypes = [C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int,
+                                    C.POINTER(C.c_uint32)]
+    L.bgpu_kernel_times.restype = C.c_int
     return L
 
 
@@ -133,14 +138,17 @@ def _stats(s: _Stats) -> Stats:
                  float(s.device_ms))
 
 
-def _mul_u64(A, B, flags: int, stats: bool):
+def _mul_u64(A, B, flags: int, stats: bool, out=None):
     _ensure_init()
     square = B is None or B is A
     a = _as_limbs(A)
     b = a if square else _as_limbs(B)
     if a.size == 0 or b.size == 0:
         raise BigIntGPUError(-1, "bgpu_mul_u64 (empty operand)")
-    out = np.empty(a.size + b.size, dtype=np.uint64)
+    if out is None:
+        out = np.empty(a.size + b.size, dtype=np.uint64)
+    elif out.dtype != np.uint64 or not out.flags.c_contiguous:
+        raise ValueError("out must be a contiguous uint64 array")
     n = C.c_size_t(0)
     st = _Stats()
     u64p = C.POINTER(C.c_uint64)
@@ -153,12 +161,13 @@ def _mul_u64(A, B, flags: int, stats: bool):
     return (res, _stats(st)) if stats else res
 
 
-def mul(A, B=None, *, stats: bool = False):
+def mul(A, B=None, *, stats: bool = False, out=None):
     """A*B for little-endian u64 limb arrays (``_mul``, mul.h:208-220).
 
     ``mul(A)`` or ``mul(A, A)`` squares.  Returns the product without leading
-    zero limbs (an empty array for a zero operand)."""
-    return _mul_u64(A, B, BGPU_METHOD_AUTO, stats)
+    zero limbs (an empty array for a zero operand).  ``out`` may supply the
+    destination (e.g. pinned host memory); the result is a view of it."""
+    return _mul_u64(A, B, BGPU_METHOD_AUTO, stats, out)
 
 
 def ntt_mul(A, B=None, *, stats: bool = False):
@@ -205,7 +214,9 @@ def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, stream: i
                method: int = BGPU_METHOD_AUTO) -> None:
     """Asynchronous product of device-resident limbs (``bgpu_mul_u64_device``).
 
-    ``out_ptr`` receives na+nb limbs.  Equal pointers and lengths square."""
+    ``out_ptr`` receives na+nb limbs.  Equal pointers and lengths square.
+    ``stream`` is a cudaStream_t handle (0 = legacy default stream), e.g.
+    ``torch.cuda.current_stream().cuda_stream``."""
     _ensure_init()
     rc = lib.bgpu_mul_u64_device(C.c_void_p(a_ptr), na, C.c_void_p(b_ptr), nb,
                                  C.c_void_p(out_ptr), method, C.c_void_p(stream or None))
@@ -219,3 +230,21 @@ def device_status(stream: int = 0) -> None:
 
 def last_launch_count() -> int:
     return int(lib.bgpu_last_launch_count())
+
+
+def set_kernel_timing(on: bool) -> None:
+    """Record CUDA events between the kernels of each NTT product."""
+    _ensure_init()
+    _check(lib.bgpu_set_kernel_timing(int(bool(on))), "bgpu_set_kernel_timing")
+
+
+def kernel_times() -> tuple[list[tuple[str, float]], int]:
+    """Mean (kernel name, ms) over the NTT products timed since
+    ``set_kernel_timing(True)``, in launch order, and the product count."""
+    names = (C.c_char_p * 8)()
+    ms = (C.c_float * 8)()
+    cnt = C.c_uint32(0)
+    n = lib.bgpu_kernel_times(names, ms, 8, C.byref(cnt))
+    if n < 0:
+        _check(n, "bgpu_kernel_times")
+    return [(names[i].decode(), float(ms[i])) for i in range(n)], int(cnt.value)

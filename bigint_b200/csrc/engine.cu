@@ -66,7 +66,14 @@ struct Engine {
     size_t io_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t last_launches = 0;
+    // optional per-kernel timing of NTT products: a ring of event sets, one
+    // set per product, read back (and averaged) without per-product syncs
+    bool kernel_timing = false;
+    std::vector<cudaEvent_t> kev;  // kTimingRing * (kNttLaunches + 1)
+    uint64_t kev_count = 0;
 };
+
+constexpr uint64_t kTimingRing = 1024;  // products whose kernel times are kept
 
 Engine g;
 std::mutex g_mu;
@@ -88,6 +95,7 @@ void release_locked() {
     cudaFree(g.d_io);
     if (g.ev0) cudaEventDestroy(g.ev0);
     if (g.ev1) cudaEventDestroy(g.ev1);
+    for (auto e : g.kev) cudaEventDestroy(e);
     if (g.stream) cudaStreamDestroy(g.stream);
     g = Engine{};
 }
@@ -246,8 +254,14 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
     cl.ticket_base = g.ticket_base;
     cl.epoch = ++g.epoch;
     g.ticket_base += carry_blocks((uint32_t)(((size_t)1 << ln) / 8));
-    cudaError_t e = launch_ntt_product(g.consts, a, b, square, ln, s, out, out_fmt, out_cap, cl, st);
-    g.last_launches = 4;
+    cudaEvent_t* ev = nullptr;
+    if (g.kernel_timing) {
+        ev = g.kev.data() + (g.kev_count % kTimingRing) * (kNttLaunches + 1);
+        ++g.kev_count;
+    }
+    cudaError_t e = launch_ntt_product(g.consts, a, b, square, ln, s, out, out_fmt, out_cap, cl, st,
+                                       ev);
+    g.last_launches = kNttLaunches;
     if (stats) {
         stats->method = BGPU_METHOD_NTT;
         stats->log2_points = (uint32_t)ln;
@@ -506,7 +520,7 @@ int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, siz
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);  // 0 = the legacy default stream
     const bool square = (d_a == d_b && na == nb);
     if (use_schoolbook(flags, na, nb)) {
         if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
@@ -523,12 +537,56 @@ int bgpu_device_status(void* stream) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g.stream;
-    cudaError_t e = cudaStreamSynchronize(st);
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return cuda_status(e);
     return check_device_error(BGPU_OK);
 }
 
 uint32_t bgpu_last_launch_count(void) { return g.last_launches; }
+
+int bgpu_set_kernel_timing(int on) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    if (on && g.kev.empty()) {
+        g.kev.resize((size_t)kTimingRing * (kNttLaunches + 1));
+        for (auto& e : g.kev) {
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                for (auto x : g.kev)
+                    if (x) cudaEventDestroy(x);
+                g.kev.clear();
+                return BGPU_ERR_CUDA;
+            }
+        }
+    }
+    g.kernel_timing = on != 0;
+    if (on) g.kev_count = 0;
+    return BGPU_OK;
+}
+
+int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* nproducts) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    if (nproducts) *nproducts = 0;
+    if (g.kev_count == 0 || g.kev.empty()) return 0;
+    cudaSetDevice(g.device);
+    const uint64_t n = g.kev_count < kTimingRing ? g.kev_count : kTimingRing;
+    const size_t last = ((g.kev_count - 1) % kTimingRing) * (kNttLaunches + 1) + kNttLaunches;
+    if (cudaEventSynchronize(g.kev[last]) != cudaSuccess) return BGPU_ERR_CUDA;
+    int k = 0;
+    for (; k < kNttLaunches && k < cap; ++k) {
+        double sum = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            float t = 0;
+            const cudaEvent_t* ev = g.kev.data() + i * (kNttLaunches + 1);
+            if (cudaEventElapsedTime(&t, ev[k], ev[k + 1]) != cudaSuccess) return BGPU_ERR_CUDA;
+            sum += t;
+        }
+        if (names) names[k] = kNttKernelNames[k];
+        if (mean_ms) mean_ms[k] = (float)(sum / (double)n);
+    }
+    if (nproducts) *nproducts = (uint32_t)n;
+    return k;
+}
 
 }  // extern "C"

@@ -68,10 +68,13 @@ struct CarryLaunch {
 
 // Launch the full NTT product pipeline (4 kernels) on `stream`.
 // out: device buffer in `out_fmt` with `out_cap` elements.
+// `ev` (optional) holds 5 events recorded around the 4 launches.
 cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
                                bool square, int log_n, const ProductScratch& s, void* out,
                                int out_fmt, size_t out_cap, const CarryLaunch& cl,
-                               cudaStream_t stream);
+                               cudaStream_t stream, cudaEvent_t* ev = nullptr);
+constexpr int kNttLaunches = 4;
+extern const char* const kNttKernelNames[kNttLaunches];
 
 uint32_t carry_blocks(uint32_t nchunks);
 

@@ -769,8 +769,9 @@ static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32
 cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
                                bool square, int log_n, const ProductScratch& s, void* out,
                                int out_fmt, size_t out_cap, const CarryLaunch& cl,
-                               cudaStream_t st) {
+                               cudaStream_t st, cudaEvent_t* ev) {
     if (!shape_supported(log_n, square)) return cudaErrorInvalidValue;
+    if (ev) cudaEventRecord(ev[0], st);
     const TransformShape sh = choose_shape(log_n);
     const size_t nn = (size_t)1 << log_n;
     const uint32_t tiles = (1u << sh.log_n1) / kCols;
@@ -783,6 +784,7 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     f.log_n1 = sh.log_n1;
     cudaError_t e = dispatch_outer(sh.log_n2, c, &f, nullptr, square ? 1 : 2, tiles, st);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[1], st);
 
     MidRowsArgs m{};
     m.ya = s.y;
@@ -802,6 +804,7 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     }
     e = dispatch_mid(sh.log_n1, c, m, square, 1u << sh.log_n2, st);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[2], st);
 
     InvColsArgs iv{};
     iv.z = s.y;
@@ -811,6 +814,7 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     iv.log_n1 = sh.log_n1;
     e = dispatch_outer(sh.log_n2, c, nullptr, &iv, 0, tiles, st);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[3], st);
 
     CarryArgs ca{};
     ca.chunks = s.chunks;
@@ -825,7 +829,12 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     ca.epoch = cl.epoch;
     ca.err = s.err;
     k_carry<<<carry_blocks(ca.nchunks), kCarryThreads, 0, st>>>(ca);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (ev) cudaEventRecord(ev[4], st);
+    return e;
 }
+
+const char* const kNttKernelNames[kNttLaunches] = {"k_fwd_cols", "k_mid_rows", "k_inv_cols",
+                                                   "k_carry"};
 
 }  // namespace bgpu

@@ -83,18 +83,33 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
                     size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
                     size_t* out_len, uint32_t flags, bgpu_stats* stats);
 
-/* Device-resident product (no host copies, asynchronous on `stream`):
- * d_out receives exactly na + nb limbs (zero padded).  d_a == d_b with
- * na == nb squares.  Errors found on the device are sticky and reported by
- * bgpu_device_status.  Not reentrant: one call in flight per process. */
+/* Device-resident product (no host copies, asynchronous on `stream`, a
+ * cudaStream_t; 0 is the legacy default stream): d_out receives exactly
+ * na + nb limbs (zero padded).  d_a == d_b with na == nb squares.  Errors
+ * found on the device are sticky and reported by bgpu_device_status.  The
+ * engine's scratch is shared: calls that overlap on the GPU (different
+ * streams, or this and the host-buffer entry points at once) race. */
 int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
                         uint64_t* d_out, uint32_t flags, void* stream);
 
-/* Synchronize `stream` and return (and clear) the sticky device status. */
+/* Synchronize `stream` (0 = legacy default stream) and return (and clear)
+ * the sticky device status. */
 int bgpu_device_status(void* stream);
 
 /* Number of kernel launches the last multiply issued (for bench accounting). */
 uint32_t bgpu_last_launch_count(void);
+
+/* Per-kernel device timing (CUDA events recorded between the launches of each
+ * NTT product, on the stream the kernels run on).  No reference counterpart:
+ * the reference has no tracing beyond std::chrono in its examples
+ * (examples/benchmark.cpp:17-38). */
+int bgpu_set_kernel_timing(int on);
+
+/* Mean device time of each kernel over the NTT products launched since
+ * timing was switched on (the last 1024 of them): names[i], mean_ms[i] in
+ * launch order, *nproducts = products averaged.  Returns the kernel count
+ * (0 if none recorded).  Synchronizes on the last recorded event. */
+int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* nproducts);
 
 #ifdef __cplusplus
 }
