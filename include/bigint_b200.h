@@ -111,6 +111,33 @@ int bgpu_set_kernel_timing(int on);
  * (0 if none recorded).  Synchronizes on the last recorded event. */
 int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* nproducts);
 
+/* Largest product of bgpu_mul_u64_device_noalloc: na + nb u64 limbs. */
+#define BGPU_NOALLOC_MAX_LIMBS 65536u
+
+/* Device-resident product that allocates nothing.  No counterpart in the
+ * reference (its CPU multiply allocates std::vectors freely); it exists for
+ * callers that cannot allocate device memory when they multiply: code running
+ * inside a fixed memory budget or a caller-managed pool that must not grow,
+ * and host threads that may not call cudaMalloc because it can synchronize the
+ * whole device.  It runs the same NTT kernels as bgpu_mul_u64_device, with all
+ * scratch in one static device array (about 3.8 MB, plus 0.8 MB of static
+ * twiddle tables) that every GPU loading this library holds until the process
+ * exits; it calls no cudaMalloc, cudaFree or other allocating routine.
+ *  - d_a, d_b, d_out are device pointers on the current device; d_out receives
+ *    na + nb limbs; d_a == d_b with na == nb squares.
+ *  - na + nb must be <= BGPU_NOALLOC_MAX_LIMBS, else BGPU_ERR_CAPACITY and
+ *    nothing is launched.
+ *  - the first call on each device does the set-up (table upload and the
+ *    static array's address, synchronous): make it before any stream capture.
+ *  - the work is queued on `stream` (0 = legacy default stream) and the call
+ *    returns after it completes, with BGPU_ERR_DEVICE_TIMEOUT if the carry
+ *    scan's bounded wait gave up.
+ *  - every call shares the static array (it keeps the last call's contents;
+ *    the carry-scan state is cleared at the start of each call): calls that
+ *    overlap on the GPU race and must be serialized by the caller. */
+int bgpu_mul_u64_device_noalloc(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
+                                uint64_t* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
