@@ -14,46 +14,16 @@
 
 #include "../../include/bigint_b200.h"
 #include "engine.h"
+#include "tables.h"
 
 namespace bgpu {
 namespace {
 
-constexpr uint32_t kPrimes[kNumPrimes] = {469762049u, 1811939329u, 2013265921u};
-constexpr uint32_t kGens[kNumPrimes] = {3u, 13u, 31u};
-
-uint64_t pow_mod(uint64_t b, uint64_t e, uint64_t p) {
-    uint64_t r = 1;
-    b %= p;
-    while (e) {
-        if (e & 1) r = r * b % p;
-        b = b * b % p;
-        e >>= 1;
-    }
-    return r;
-}
-
-uint32_t inv32(uint32_t p) {  // p^-1 mod 2^32, p odd
-    uint32_t x = 1;
-    for (int i = 0; i < 5; ++i) x *= 2u - p * x;
-    return x;
-}
-
-struct MontPair {
-    uint32_t w, wp;
-};
-
-MontPair mont(uint64_t v, uint32_t p) {
-    MontPair m;
-    m.w = (uint32_t)(((v % p) << 32) % p);
-    m.wp = m.w * inv32(p);
-    return m;
-}
-
 struct Engine {
     int device = -1;
     cudaStream_t stream = nullptr;
-    NttConsts consts{};
-    void* d_tables = nullptr;
+    NttConsts consts[kNumSets]{};
+    void* d_tables[kNumSets] = {};
     // scratch arena
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -88,7 +58,7 @@ void release_locked() {
     if (g.device < 0) return;
     cudaSetDevice(g.device);
     if (g.stream) cudaStreamSynchronize(g.stream);
-    cudaFree(g.d_tables);
+    for (auto t : g.d_tables) cudaFree(t);
     cudaFree(g.d_scratch);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
@@ -101,70 +71,18 @@ void release_locked() {
 }
 
 int build_tables_locked() {
-    const size_t stage_n = (size_t)1 << kMaxLogRow;
-    const size_t split_n = (size_t)1 << kTwSplit;
-    const size_t per_dir = stage_n + 2 * split_n;
-    std::vector<uint2> host(kNumPrimes * 2 * per_dir);
-    for (int q = 0; q < kNumPrimes; ++q) {
-        const uint32_t p = kPrimes[q];
-        for (int dir = 0; dir < 2; ++dir) {
-            uint2* base = host.data() + (q * 2 + dir) * per_dir;
-            // stage table: entry h + m = omega_{2h}^(+-m)
-            MontPair one = mont(1, p);
-            base[0] = make_uint2(one.w, one.wp);
-            for (size_t h = 1; h < stage_n; h <<= 1) {
-                uint64_t root = pow_mod(kGens[q], (p - 1) / (2 * h), p);
-                if (dir) root = pow_mod(root, p - 2, p);
-                uint64_t v = 1;
-                for (size_t m = 0; m < h; ++m) {
-                    MontPair mp = mont(v, p);
-                    base[h + m] = make_uint2(mp.w, mp.wp);
-                    v = v * root % p;
-                }
-            }
-            // split tables for omega_{2^26}^(+-e)
-            uint64_t r26 = pow_mod(kGens[q], (p - 1) >> kMaxLogN, p);
-            if (dir) r26 = pow_mod(r26, p - 2, p);
-            uint2* th = base + stage_n;
-            uint2* tl = th + split_n;
-            const uint64_t step_hi = pow_mod(r26, split_n, p);
-            uint64_t vh = 1, vl = 1;
-            for (size_t i = 0; i < split_n; ++i) {
-                MontPair mh = mont(vh, p), ml = mont(vl, p);
-                th[i] = make_uint2(mh.w, mh.wp);
-                tl[i] = make_uint2(ml.w, ml.wp);
-                vh = vh * step_hi % p;
-                vl = vl * r26 % p;
-            }
-        }
+    for (int ps = 0; ps < kNumSets; ++ps) {
+        std::vector<uint2> host(table_entries(ps, kMaxLogRow));
+        build_tables(ps, kMaxLogRow, host.data());
+        cudaError_t e = cudaMalloc(&g.d_tables[ps], host.size() * sizeof(uint2));
+        if (e != cudaSuccess) return cuda_status(e);
+        e = cudaMemcpy(g.d_tables[ps], host.data(), host.size() * sizeof(uint2),
+                       cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_status(e);
+        g.consts[ps] = make_consts(ps, kMaxLogRow, static_cast<const uint2*>(g.d_tables[ps]));
+        e = upload_consts(kSlotEngine + ps, g.consts[ps]);
+        if (e != cudaSuccess) return cuda_status(e);
     }
-    cudaError_t e = cudaMalloc(&g.d_tables, host.size() * sizeof(uint2));
-    if (e != cudaSuccess) return cuda_status(e);
-    e = cudaMemcpy(g.d_tables, host.data(), host.size() * sizeof(uint2), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return cuda_status(e);
-    const uint2* dt = static_cast<const uint2*>(g.d_tables);
-    NttConsts& c = g.consts;
-    for (int q = 0; q < kNumPrimes; ++q) {
-        c.pr[q].p = kPrimes[q];
-        c.pr[q].pinv = inv32(kPrimes[q]);
-        MontPair one = mont(1, kPrimes[q]);
-        c.one_w[q] = one.w;
-        c.one_wp[q] = one.wp;
-        for (int dir = 0; dir < 2; ++dir) {
-            const uint2* base = dt + (q * 2 + dir) * per_dir;
-            c.stage[q][dir] = base;
-            c.th[q][dir] = base + stage_n;
-            c.tl[q][dir] = base + stage_n + split_n;
-        }
-    }
-    const uint32_t p0 = kPrimes[0], p1 = kPrimes[1], p2 = kPrimes[2];
-    MontPair k1 = mont(pow_mod(p0, p1 - 2, p1), p1);
-    MontPair k2 = mont(p0 % p2, p2);
-    MontPair k3 = mont(pow_mod((uint64_t)p0 * p1 % p2, p2 - 2, p2), p2);
-    c.k1 = k1.w, c.k1p = k1.wp;
-    c.k2 = k2.w, c.k2p = k2.wp;
-    c.k3 = k3.w, c.k3p = k3.wp;
-    c.m01 = (uint64_t)p0 * p1;
     return BGPU_OK;
 }
 
@@ -259,8 +177,9 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
         ev = g.kev.data() + (g.kev_count % kTimingRing) * (kNttLaunches + 1);
         ++g.kev_count;
     }
-    cudaError_t e = launch_ntt_product(g.consts, a, b, square, ln, s, out, out_fmt, out_cap, cl, st,
-                                       ev);
+    const int ps = prime_set_for(ln);
+    cudaError_t e = launch_ntt_product(kSlotEngine + ps, g.consts[ps], a, b, square, ln, s, out,
+                                       out_fmt, out_cap, cl, st, ev);
     g.last_launches = kNttLaunches;
     if (stats) {
         stats->method = BGPU_METHOD_NTT;

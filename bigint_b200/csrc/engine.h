@@ -15,19 +15,27 @@ enum DigitFormat : int {
     kFmtDigit28 = 1, // little-endian uint32_t digits of 28 bits (the reference's Digits)
 };
 
-// Constants shared by all transform kernels (passed by value as a kernel parameter).
+// Constants of one prime set, kept in __constant__ memory (one slot per owner
+// and prime set) so kernels can index them by the runtime prime number.
 struct NttConsts {
     PrimeInfo pr[kNumPrimes];
     uint32_t one_w[kNumPrimes], one_wp[kNumPrimes];  // Montgomery form of 1 (reduces any u32 mod p)
-    const uint2* stage[kNumPrimes][2];  // [prime][dir]: entry h+m = omega_{2h}^{+-m}, h < 2^15
-    const uint2* th[kNumPrimes][2];     // omega_{2^26}^{+-(i << 13)}, i < 2^13
-    const uint2* tl[kNumPrimes][2];     // omega_{2^26}^{+-i}, i < 2^13
+    const uint2* stage[kNumPrimes][2];  // [prime][dir] Shoup pairs: entry h+m = omega_{2h}^{+-m}
+    const uint2* th[kNumPrimes][2];     // Montgomery pairs: omega_{2^log_max}^{+-(i << split)}
+    const uint2* tl[kNumPrimes][2];     // Montgomery pairs: omega_{2^log_max}^{+-i}
     // Garner CRT for p0 < p1 < p2 (Montgomery constants with their w').
     uint32_t k1, k1p;  // p0^-1 mod p1
     uint32_t k2, k2p;  // p0 mod p2
     uint32_t k3, k3p;  // (p0 p1)^-1 mod p2
     uint64_t m01;      // p0 * p1
+    int log_max, split;
 };
+
+// Constant slots: the engine's two prime sets, then the no-allocation path's.
+constexpr int kSlotEngine = 0;   // + prime set
+constexpr int kSlotNoAlloc = 2;  // + prime set
+constexpr int kConstSlots = 4;
+cudaError_t upload_consts(int slot, const NttConsts& c);
 
 // One operand of a transform: a device pointer in `fmt` with `nsrc` source
 // elements; `nd32` is its length in 32-bit digits.
@@ -68,11 +76,14 @@ struct CarryLaunch {
 
 // Launch the full NTT product pipeline (4 kernels) on `stream`.
 // out: device buffer in `out_fmt` with `out_cap` elements.
+// `slot` selects the constants (kSlotEngine/kSlotNoAlloc + prime_set_for(log_n));
+// `host` is the same constants on the host (for per-call scale factors).
 // `ev` (optional) holds 5 events recorded around the 4 launches.
-cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
-                               bool square, int log_n, const ProductScratch& s, void* out,
-                               int out_fmt, size_t out_cap, const CarryLaunch& cl,
-                               cudaStream_t stream, cudaEvent_t* ev = nullptr);
+cudaError_t launch_ntt_product(int slot, const NttConsts& host, const OperandDesc& a,
+                               const OperandDesc& b, bool square, int log_n,
+                               const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
+                               const CarryLaunch& cl, cudaStream_t stream,
+                               cudaEvent_t* ev = nullptr);
 constexpr int kNttLaunches = 4;
 extern const char* const kNttKernelNames[kNttLaunches];
 

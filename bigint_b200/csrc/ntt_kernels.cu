@@ -20,7 +20,8 @@
 // sweeps plus a serial carry (src/mul/ntt_multithread.cpp:333-379, 418-442);
 // here every pass keeps a whole row or column tile in shared memory and runs
 // radix-8/16 rounds in registers, so each product makes three sweeps over the
-// residues in global memory.
+// residues in global memory.  Template parameter PS selects the prime set
+// (arith.cuh): set 0 uses lazy butterflies, set 1 strict ones.
 #include <cuda/atomic>
 
 #include "engine.h"
@@ -28,6 +29,12 @@
 namespace bgpu {
 
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
+
+__constant__ NttConsts c_consts[kConstSlots];
+
+cudaError_t upload_consts(int slot, const NttConsts& c) {
+    return cudaMemcpyToSymbol(c_consts, &c, sizeof(NttConsts), slot * sizeof(NttConsts));
+}
 
 // Round split of a length-2^L transform into radix-2^r rounds (r <= 4),
 // top bits first (DIF order).
@@ -43,11 +50,22 @@ struct Plan {
     __host__ __device__ static constexpr int lo(int k) { return hi(k) - r(k) + 1; }
 };
 
+// Shared-memory placement of element i (of column col) in a [2^L][C] tile.
+// The XOR swizzles make every round's access pattern bank-conflict free
+// (rows: checked for L = 5..15; 8-column tiles: L = 2..11) and are bijective.
+template <int C>
+__device__ __forceinline__ uint32_t sidx(uint32_t i, int col) {
+    if constexpr (C == 1)
+        return i ^ (((i >> 3) ^ (i >> 4)) & 31u);
+    else
+        return (i ^ (((i >> 2) ^ (i >> 4)) & 3u)) * C + col;
+}
+
 // ---- register-resident butterflies ------------------------------------------
 
 // DIF stages for pair bits HI..LO on the 2^R elements base + (j << LO).
 // Element pair (i, i+h): (a, b) -> (a+b, (a-b) * omega_{2h}^(i mod h)).
-template <int R, int HI, int LO>
+template <bool LAZY, int R, int HI, int LO>
 __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_low,
                                          const uint2* __restrict__ tw, uint32_t p) {
 #pragma unroll
@@ -57,15 +75,12 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_lo
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
             if (j & dist) continue;
-            const uint32_t a = x[j], b = x[j + dist];
-            x[j] = mod_add(a, b, p);
-            const uint32_t d = mod_sub(a, b, p);
             if (LO == 0 && (j & (dist - 1)) == 0) {
-                x[j + dist] = d;  // twiddle omega^0 (base_low is 0 when LO == 0)
+                Bfly<LAZY>::dif1(x[j], x[j + dist], p);  // omega^0 (base_low is 0 when LO == 0)
             } else {
                 const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
                 const uint2 w = __ldg(tw + h + m);
-                x[j + dist] = mont_mul_pre(d, w.x, w.y, p);
+                Bfly<LAZY>::dif(x[j], x[j + dist], w.x, w.y, p);
             }
         }
     }
@@ -73,7 +88,7 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_lo
 
 // DIT stages for pair bits LO..HI (inverse table):
 // (a, b) -> (a + b*w, a - b*w), w = omega_{2h}^-(i mod h).
-template <int R, int HI, int LO>
+template <bool LAZY, int R, int HI, int LO>
 __device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_low,
                                          const uint2* __restrict__ tw, uint32_t p) {
 #pragma unroll
@@ -83,15 +98,13 @@ __device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_lo
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
             if (j & dist) continue;
-            uint32_t b = x[j + dist];
-            if (!(LO == 0 && (j & (dist - 1)) == 0)) {
+            if (LO == 0 && (j & (dist - 1)) == 0) {
+                Bfly<LAZY>::dit1(x[j], x[j + dist], p);
+            } else {
                 const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
                 const uint2 w = __ldg(tw + h + m);
-                b = mont_mul_pre(b, w.x, w.y, p);
+                Bfly<LAZY>::dit(x[j], x[j + dist], w.x, w.y, p);
             }
-            const uint32_t a = x[j];
-            x[j] = mod_add(a, b, p);
-            x[j + dist] = mod_sub(a, b, p);
         }
     }
 }
@@ -110,57 +123,64 @@ struct Group {
         base = ((q >> LO) << (HI + 1)) | base_low;
     }
     __device__ __forceinline__ uint32_t idx(int j) const { return base + ((uint32_t)j << LO); }
+    __device__ __forceinline__ uint32_t at(int j) const { return sidx<C>(idx(j), col); }
 };
 
 // One smem round (load -> butterflies -> store back); no sync inside.
-template <int L, int C, int T, int K, bool INV>
+template <bool LAZY, int L, int C, int T, int K, bool INV>
 __device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict__ tw,
                                            uint32_t p) {
     using Gr = Group<L, C, K>;
     constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = threadIdx.x; g < Gr::G; g += T) {
         const Gr gr(g);
         uint32_t x[1 << R];
 #pragma unroll
-        for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.idx(j) * C + gr.col];
+        for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.at(j)];
         if constexpr (INV)
-            dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
         else
-            dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
 #pragma unroll
-        for (int j = 0; j < (1 << R); ++j) sm[gr.idx(j) * C + gr.col] = x[j];
+        for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
     }
 }
 
-// DIF rounds K0..K1 (inclusive) in smem, each followed by a block barrier.
-template <int L, int C, int T, int K, int KEND>
+// DIF rounds K..KEND in smem, each followed by a block barrier.
+template <bool LAZY, int L, int C, int T, int K, int KEND>
 __device__ __forceinline__ void dif_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
     if constexpr (K <= KEND) {
-        smem_round<L, C, T, K, false>(sm, tw, p);
+        smem_round<LAZY, L, C, T, K, false>(sm, tw, p);
         __syncthreads();
-        dif_rounds<L, C, T, K + 1, KEND>(sm, tw, p);
+        dif_rounds<LAZY, L, C, T, K + 1, KEND>(sm, tw, p);
     }
 }
 
-// DIT rounds K down to KEND (inclusive) in smem, each followed by a barrier.
-template <int L, int C, int T, int K, int KEND>
+// DIT rounds K down to KEND in smem, each followed by a barrier.
+template <bool LAZY, int L, int C, int T, int K, int KEND>
 __device__ __forceinline__ void dit_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
     if constexpr (K >= KEND) {
-        smem_round<L, C, T, K, true>(sm, tw, p);
+        smem_round<LAZY, L, C, T, K, true>(sm, tw, p);
         __syncthreads();
-        dit_rounds<L, C, T, K - 1, KEND>(sm, tw, p);
+        dit_rounds<LAZY, L, C, T, K - 1, KEND>(sm, tw, p);
     }
 }
 
-// omega_N^(+-e) in Montgomery form from the two split tables (N = 2^log_n).
+// omega_N^(+-e) as a fully reduced Montgomery form from the two split tables.
 __device__ __forceinline__ uint32_t inter_twiddle(const NttConsts& c, int q, int dir, uint32_t e,
-                                                  int log_n, uint32_t p, uint32_t pinv) {
-    const uint32_t e26 = e << (kMaxLogN - log_n);
-    const uint32_t hi = __ldg(&c.th[q][dir][e26 >> kTwSplit].x);
-    const uint2 lo = __ldg(&c.tl[q][dir][e26 & ((1u << kTwSplit) - 1u)]);
+                                                  int log_n, uint32_t p) {
+    const uint32_t em = e << (c.log_max - log_n);
+    const uint32_t hi = __ldg(&c.th[q][dir][em >> c.split].x);
+    const uint2 lo = __ldg(&c.tl[q][dir][em & ((1u << c.split) - 1u)]);
     return mont_mul_pre(hi, lo.x, lo.y, p);
-    (void)pinv;
+}
+
+// x * omega (omega from inter_twiddle), lazily (0, 2p) or strictly [0, p).
+template <bool LAZY>
+__device__ __forceinline__ uint32_t twiddle_mul(uint32_t x, uint32_t w, uint32_t p, uint32_t pinv) {
+    const uint32_t r = mont_lazy(x, w, w * pinv, p);
+    return LAZY ? r : csub(r, p);
 }
 
 __device__ __forceinline__ uint32_t bitrev(uint32_t v, int bits) {
@@ -184,18 +204,20 @@ __device__ __forceinline__ uint32_t load_digit32(const OperandDesc& in, uint32_t
 struct FwdColsArgs {
     OperandDesc op[2];
     uint32_t* y;  // [op][prime][N]
-    int log_n, log_n1;
+    int log_n, log_n1, slot;
 };
 
-template <int L2, int T>
-__global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a, const NttConsts c) {
+template <int PS, int L2, int T>
+__global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
+    constexpr bool LAZY = PS == 0;
     extern __shared__ __align__(16) uint32_t sm[];  // [2^L2][kCols]
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
+    const NttConsts& c = c_consts[a.slot];
     const int q = blockIdx.y, opi = blockIdx.z;
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
-    const OperandDesc in = a.op[opi];
+    const OperandDesc in = opi == 0 ? a.op[0] : a.op[1];
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     uint32_t* y = a.y + ((size_t)opi * kNumPrimes + q) * nn;
@@ -208,33 +230,39 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a, const NttCo
 #pragma unroll 1
         for (int g = threadIdx.x; g < Gr::G; g += T) {
             const Gr gr(g);
-            uint32_t x[1 << R];
+            uint32_t v[1 << R], x[1 << R];
             uint32_t any = 0;
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) {
-                const uint32_t n = c0 + gr.col + n1_len * gr.idx(j);
-                uint32_t v = load_digit32(in, n);
-                any |= v;
-                x[j] = mont_mul_pre(v, one_w, one_wp, p);
+                v[j] = load_digit32(in, c0 + gr.col + n1_len * gr.idx(j));
+                any |= v[j];
             }
-            if (any) dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j)
+                x[j] = LAZY ? mont_lazy(v[j], one_w, one_wp, p) : mont_mul_pre(v[j], one_w, one_wp, p);
+            if (any) {
+                dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            } else {
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) x[j] = 0;
+            }
             if constexpr (NR == 1) {
 #pragma unroll
                 for (int j = 0; j < (1 << R); ++j) {
                     const uint32_t slot = gr.idx(j), n1 = c0 + gr.col;
                     const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
-                    const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p, pinv);
-                    y[(size_t)slot * n1_len + n1] = mont_mul(x[j], w, p, pinv);
+                    y[(size_t)slot * n1_len + n1] =
+                        twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 0, e, a.log_n, p), p, pinv);
                 }
             } else {
 #pragma unroll
-                for (int j = 0; j < (1 << R); ++j) sm[gr.idx(j) * kCols + gr.col] = x[j];
+                for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
             }
         }
     }
     if constexpr (NR > 1) {
         __syncthreads();
-        dif_rounds<L2, kCols, T, 1, NR - 2>(sm, tw, p);
+        dif_rounds<LAZY, L2, kCols, T, 1, NR - 2>(sm, tw, p);
         // Last round: butterflies, inter-pass twiddle, store to global.
         using Gr = Group<L2, kCols, NR - 1>;
         constexpr int R = Gr::R;
@@ -243,15 +271,15 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a, const NttCo
             const Gr gr(g);
             uint32_t x[1 << R];
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.idx(j) * kCols + gr.col];
-            dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.at(j)];
+            dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
             const uint32_t n1 = c0 + gr.col;
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) {
                 const uint32_t slot = gr.idx(j);
                 const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
-                const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p, pinv);
-                y[(size_t)slot * n1_len + n1] = mont_mul(x[j], w, p, pinv);
+                y[(size_t)slot * n1_len + n1] =
+                    twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 0, e, a.log_n, p), p, pinv);
             }
         }
     }
@@ -262,13 +290,25 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a, const NttCo
 struct MidRowsArgs {
     uint32_t* ya;        // [prime][N], result written in place
     const uint32_t* yb;  // [prime][N] or null (square)
-    int log_n, log_n2;
+    int log_n, log_n2, slot;
     uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
 };
 
+// Pointwise product a*b*N^-1 (cancelling the Montgomery 2^-32 with the scale).
+template <bool LAZY>
+__device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t sw, uint32_t swp,
+                                              uint32_t p, uint32_t pinv) {
+    if constexpr (LAZY) {
+        const uint32_t y = csub(mont_lazy(a, b, b * pinv, p), p);  // b < 2p: result < 2p
+        return mont_lazy(y, sw, swp, p);
+    } else {
+        return mont_mul_pre(mont_mul(a, b, p, pinv), sw, swp, p);
+    }
+}
+
 // Last DIF round of B (or A when squaring) fused with the pointwise product
 // and the first DIT round; with a single round also the inverse twiddle.
-template <int L1, int T, bool SQR, bool SINGLE>
+template <bool LAZY, int L1, int T, bool SQR, bool SINGLE>
 __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& c, uint32_t* sa,
                                          uint32_t* sb, const uint32_t* row_a, const uint32_t* row_b,
                                          uint32_t* row_out, int q, uint32_t k2) {
@@ -279,7 +319,8 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* twf = c.stage[q][0];
     const uint2* twi = c.stage[q][1];
-    const uint32_t sw = a.scale_w[q], swp = a.scale_wp[q];
+    const uint32_t sw = q == 0 ? a.scale_w[0] : (q == 1 ? a.scale_w[1] : a.scale_w[2]);
+    const uint32_t swp = q == 0 ? a.scale_wp[0] : (q == 1 ? a.scale_wp[1] : a.scale_wp[2]);
     const uint32_t* src = SQR ? sa : sb;
 #pragma unroll 1
     for (int g = threadIdx.x; g < Gr::G; g += T) {
@@ -290,57 +331,58 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
             if constexpr (SINGLE)
                 x[j] = (SQR ? row_a : row_b)[gr.idx(j)];
             else
-                x[j] = src[gr.idx(j)];
+                x[j] = src[gr.at(j)];
         }
-        dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+        dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
-            const uint32_t other = SQR ? x[j] : sa[gr.idx(j)];
-            x[j] = mont_mul_pre(mont_mul(x[j], other, p, pinv), sw, swp, p);
+            const uint32_t other = SQR ? x[j] : sa[gr.at(j)];
+            x[j] = pointwise<LAZY>(x[j], other, sw, swp, p, pinv);
         }
-        dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+        dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
         if constexpr (SINGLE) {
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) {
                 const uint32_t n1 = gr.idx(j);
                 const uint32_t e = (n1 * k2) & ((1u << a.log_n) - 1u);
-                const uint32_t w = inter_twiddle(c, q, 1, e, a.log_n, p, pinv);
-                row_out[n1] = mont_mul(x[j], w, p, pinv);
+                row_out[n1] = twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 1, e, a.log_n, p), p, pinv);
             }
         } else {
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) sa[gr.idx(j)] = x[j];
+            for (int j = 0; j < (1 << R); ++j) sa[gr.at(j)] = x[j];
         }
     }
 }
 
 // DIF of one row: round 0 from global into smem, then rounds 1..nr-2 (the
 // last round is done by mid_turn).
-template <int L1, int T>
+template <bool LAZY, int L1, int T>
 __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, const uint2* twf,
                                             uint32_t p) {
     using P1 = Plan<L1>;
     using Gr = Group<L1, 1, 0>;
     constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
     for (int g = threadIdx.x; g < Gr::G; g += T) {
         const Gr gr(g);
         uint32_t x[1 << R];
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) x[j] = row[gr.idx(j)];
-        dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+        dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
 #pragma unroll
-        for (int j = 0; j < (1 << R); ++j) s[gr.idx(j)] = x[j];
+        for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
     }
     __syncthreads();
-    dif_rounds<L1, 1, T, 1, P1::nr - 2>(s, twf, p);
+    dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p);
 }
 
-template <int L1, int T, bool SQR>
-__global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a, const NttConsts c) {
+template <int PS, int L1, int T, bool SQR>
+__global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
+    constexpr bool LAZY = PS == 0;
     extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1])
     using P1 = Plan<L1>;
     constexpr int NR = P1::nr;
+    const NttConsts& c = c_consts[a.slot];
     uint32_t* sa = sm;
     uint32_t* sb = sm + (1u << L1);
     const int q = blockIdx.y;
@@ -355,7 +397,6 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a, const NttCo
 
     if constexpr (NR == 1) {
         if constexpr (!SQR) {
-            // A's single DIF round into smem first.
             using Gr = Group<L1, 1, 0>;
             constexpr int R = Gr::R;
 #pragma unroll 1
@@ -364,39 +405,37 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a, const NttCo
                 uint32_t x[1 << R];
 #pragma unroll
                 for (int j = 0; j < (1 << R); ++j) x[j] = row_a[gr.idx(j)];
-                dif_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
+                dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
 #pragma unroll
-                for (int j = 0; j < (1 << R); ++j) sa[gr.idx(j)] = x[j];
+                for (int j = 0; j < (1 << R); ++j) sa[gr.at(j)] = x[j];
             }
             __syncthreads();
         }
-        mid_turn<L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+        mid_turn<LAZY, L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
     } else {
-        mid_dif_row<L1, T>(row_a, sa, twf, p);
+        mid_dif_row<LAZY, L1, T>(row_a, sa, twf, p);
         if constexpr (!SQR) {
-            // A's last DIF round in place, then B's rounds.
-            smem_round<L1, 1, T, NR - 1, false>(sa, twf, p);
-            mid_dif_row<L1, T>(row_b, sb, twf, p);
+            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p);  // A's last DIF round
+            mid_dif_row<LAZY, L1, T>(row_b, sb, twf, p);
         }
-        mid_turn<L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+        mid_turn<LAZY, L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
         __syncthreads();
-        dit_rounds<L1, 1, T, NR - 2, 1>(sa, twi, p);
+        dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sa, twi, p);
         // Round 0 (top bits): DIT, inverse twiddle, store to global.
         using Gr = Group<L1, 1, 0>;
         constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
         for (int g = threadIdx.x; g < Gr::G; g += T) {
             const Gr gr(g);
             uint32_t x[1 << R];
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) x[j] = sa[gr.idx(j)];
-            dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+            for (int j = 0; j < (1 << R); ++j) x[j] = sa[gr.at(j)];
+            dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) {
                 const uint32_t n1 = gr.idx(j);
                 const uint32_t e = (n1 * k2) & (uint32_t)(nn - 1);
-                const uint32_t w = inter_twiddle(c, q, 1, e, a.log_n, p, pinv);
-                row_a[n1] = mont_mul(x[j], w, p, pinv);
+                row_a[n1] = twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 1, e, a.log_n, p), p, pinv);
             }
         }
     }
@@ -408,10 +447,10 @@ struct InvColsArgs {
     const uint32_t* z;  // [prime][N]
     uint64_t* chunks;   // 4 limbs per chunk
     uint64_t* spill;    // per chunk
-    int log_n, log_n1;
+    int log_n, log_n1, slot;
 };
 
-// Garner: residues (r0,r1,r2) -> the coefficient as 96 bits (< 2^89).
+// Garner: residues (r0,r1,r2), each in [0, p_q) -> the coefficient as 96 bits.
 __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r1, uint32_t r2,
                                      uint32_t& w0, uint32_t& w1, uint32_t& w2) {
     const uint32_t p1 = c.pr[1].p, p2 = c.pr[2].p, p0 = c.pr[0].p;
@@ -430,12 +469,14 @@ __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r
     w2 = (uint32_t)hi;
 }
 
-template <int L2, int T>
-__global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a, const NttConsts c) {
+template <int PS, int L2, int T>
+__global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a) {
+    constexpr bool LAZY = PS == 0;
     extern __shared__ __align__(16) uint32_t sm[];  // 3 x [2^L2][kCols]
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
     constexpr int TILE = kCols << L2;
+    const NttConsts& c = c_consts[a.slot];
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
 
@@ -456,22 +497,43 @@ __global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a, const NttCo
 #pragma unroll
                 for (int j = 0; j < (1 << R); ++j)
                     x[j] = z[(size_t)gr.idx(j) * n1_len + c0 + gr.col];
-                dit_regs<R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+                dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+                if constexpr (NR == 1) {
 #pragma unroll
-                for (int j = 0; j < (1 << R); ++j) s[gr.idx(j) * kCols + gr.col] = x[j];
+                    for (int j = 0; j < (1 << R); ++j) x[j] = Bfly<LAZY>::reduce(x[j], p);
+                }
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
             }
         }
         __syncthreads();
-        dit_rounds<L2, kCols, T, NR - 2, 0>(s, twi, p);
+        if constexpr (NR > 1) {
+            dit_rounds<LAZY, L2, kCols, T, NR - 2, 1>(s, twi, p);
+            // Round 0: DIT then reduce to [0, p) for the CRT.
+            using Gr = Group<L2, kCols, 0>;
+            constexpr int R = Gr::R;
+#pragma unroll 1
+            for (int g = threadIdx.x; g < Gr::G; g += T) {
+                const Gr gr(g);
+                uint32_t x[1 << R];
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) x[j] = s[gr.at(j)];
+                dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = Bfly<LAZY>::reduce(x[j], p);
+            }
+            __syncthreads();
+        }
     }
 
     // CRT and chunk sums: row n2 of the tile is chunk (c0 + N1*n2)/8.
 #pragma unroll 1
     for (uint32_t n2 = threadIdx.x; n2 < (1u << L2); n2 += T) {
         uint32_t w0[kCols], w1[kCols], w2[kCols];
-        const uint4* s0 = reinterpret_cast<const uint4*>(sm + n2 * kCols);
-        const uint4* s1 = reinterpret_cast<const uint4*>(sm + TILE + n2 * kCols);
-        const uint4* s2 = reinterpret_cast<const uint4*>(sm + 2 * TILE + n2 * kCols);
+        const uint32_t row = sidx<kCols>(n2, 0);
+        const uint4* s0 = reinterpret_cast<const uint4*>(sm + row);
+        const uint4* s1 = reinterpret_cast<const uint4*>(sm + TILE + row);
+        const uint4* s2 = reinterpret_cast<const uint4*>(sm + 2 * TILE + row);
         uint32_t r0[kCols], r1[kCols], r2[kCols];
 #pragma unroll
         for (int h = 0; h < kCols / 4; ++h) {
@@ -683,56 +745,60 @@ size_t smem_inv_cols(int l2) { return (size_t)kNumPrimes * kCols * 4 << l2; }
 
 static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1 << (l1 - 4)) : 32); }
 
-template <int L2>
-static cudaError_t launch_outer(const NttConsts& c, const FwdColsArgs* f, const InvColsArgs* inv,
-                                int nops, uint32_t tiles, cudaStream_t st) {
+template <class K>
+static void allow_smem(K k, size_t bytes) {
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int PS, int L2>
+static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, int nops,
+                                uint32_t tiles, cudaStream_t st) {
     constexpr int T = 256;
     if (f) {
-        auto k = k_fwd_cols<L2, T>;
-        size_t sm = smem_fwd_cols(L2);
-        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k<<<dim3(tiles, kNumPrimes, nops), T, sm, st>>>(*f, c);
+        auto k = k_fwd_cols<PS, L2, T>;
+        const size_t sm = smem_fwd_cols(L2);
+        allow_smem(k, sm);
+        k<<<dim3(tiles, kNumPrimes, nops), T, sm, st>>>(*f);
     } else {
-        auto k = k_inv_cols<L2, T>;
-        size_t sm = smem_inv_cols(L2);
-        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k<<<dim3(tiles), T, sm, st>>>(*inv, c);
+        auto k = k_inv_cols<PS, L2, T>;
+        const size_t sm = smem_inv_cols(L2);
+        allow_smem(k, sm);
+        k<<<dim3(tiles), T, sm, st>>>(*inv);
     }
     return cudaGetLastError();
 }
 
-static cudaError_t dispatch_outer(int l2, const NttConsts& c, const FwdColsArgs* f,
-                                  const InvColsArgs* inv, int nops, uint32_t tiles,
-                                  cudaStream_t st) {
+template <int PS>
+static cudaError_t dispatch_outer(int l2, const FwdColsArgs* f, const InvColsArgs* inv, int nops,
+                                  uint32_t tiles, cudaStream_t st) {
     switch (l2) {
-        case 2: return launch_outer<2>(c, f, inv, nops, tiles, st);
-        case 3: return launch_outer<3>(c, f, inv, nops, tiles, st);
-        case 4: return launch_outer<4>(c, f, inv, nops, tiles, st);
-        case 5: return launch_outer<5>(c, f, inv, nops, tiles, st);
-        case 6: return launch_outer<6>(c, f, inv, nops, tiles, st);
-        case 7: return launch_outer<7>(c, f, inv, nops, tiles, st);
-        case 8: return launch_outer<8>(c, f, inv, nops, tiles, st);
-        case 9: return launch_outer<9>(c, f, inv, nops, tiles, st);
-        case 10: return launch_outer<10>(c, f, inv, nops, tiles, st);
-        case 11: return launch_outer<11>(c, f, inv, nops, tiles, st);
+        case 2: return launch_outer<PS, 2>(f, inv, nops, tiles, st);
+        case 3: return launch_outer<PS, 3>(f, inv, nops, tiles, st);
+        case 4: return launch_outer<PS, 4>(f, inv, nops, tiles, st);
+        case 5: return launch_outer<PS, 5>(f, inv, nops, tiles, st);
+        case 6: return launch_outer<PS, 6>(f, inv, nops, tiles, st);
+        case 7: return launch_outer<PS, 7>(f, inv, nops, tiles, st);
+        case 8: return launch_outer<PS, 8>(f, inv, nops, tiles, st);
+        case 9: return launch_outer<PS, 9>(f, inv, nops, tiles, st);
+        case 10: return launch_outer<PS, 10>(f, inv, nops, tiles, st);
+        case 11: return launch_outer<PS, 11>(f, inv, nops, tiles, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-template <int L1>
-static cudaError_t launch_mid(const NttConsts& c, const MidRowsArgs& m, bool square, uint32_t rows,
-                              cudaStream_t st) {
+template <int PS, int L1>
+static cudaError_t launch_mid(const MidRowsArgs& m, bool square, uint32_t rows, cudaStream_t st) {
     constexpr int T = mid_threads(L1);
-    size_t sm = smem_mid_rows(L1, square);
+    const size_t sm = smem_mid_rows(L1, square);
     if (square) {
-        auto k = k_mid_rows<L1, T, true>;
-        if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m, c);
+        auto k = k_mid_rows<PS, L1, T, true>;
+        allow_smem(k, sm);
+        k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m);
     } else {
         if constexpr (L1 <= 14) {
-            auto k = k_mid_rows<L1, T, false>;
-            if (sm > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m, c);
+            auto k = k_mid_rows<PS, L1, T, false>;
+            allow_smem(k, sm);
+            k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m);
         } else {
             return cudaErrorInvalidValue;
         }
@@ -740,22 +806,25 @@ static cudaError_t launch_mid(const NttConsts& c, const MidRowsArgs& m, bool squ
     return cudaGetLastError();
 }
 
-static cudaError_t dispatch_mid(int l1, const NttConsts& c, const MidRowsArgs& m, bool square,
-                                uint32_t rows, cudaStream_t st) {
+template <int PS>
+static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint32_t rows,
+                                cudaStream_t st) {
     switch (l1) {
-        case 3: return launch_mid<3>(c, m, square, rows, st);
-        case 4: return launch_mid<4>(c, m, square, rows, st);
-        case 5: return launch_mid<5>(c, m, square, rows, st);
-        case 6: return launch_mid<6>(c, m, square, rows, st);
-        case 7: return launch_mid<7>(c, m, square, rows, st);
-        case 8: return launch_mid<8>(c, m, square, rows, st);
-        case 9: return launch_mid<9>(c, m, square, rows, st);
-        case 10: return launch_mid<10>(c, m, square, rows, st);
-        case 11: return launch_mid<11>(c, m, square, rows, st);
-        case 12: return launch_mid<12>(c, m, square, rows, st);
-        case 13: return launch_mid<13>(c, m, square, rows, st);
-        case 14: return launch_mid<14>(c, m, square, rows, st);
-        case 15: return launch_mid<15>(c, m, square, rows, st);
+        case 3: return launch_mid<PS, 3>(m, square, rows, st);
+        case 4: return launch_mid<PS, 4>(m, square, rows, st);
+        case 5: return launch_mid<PS, 5>(m, square, rows, st);
+        case 6: return launch_mid<PS, 6>(m, square, rows, st);
+        case 7: return launch_mid<PS, 7>(m, square, rows, st);
+        case 8: return launch_mid<PS, 8>(m, square, rows, st);
+        case 9: return launch_mid<PS, 9>(m, square, rows, st);
+        case 10: return launch_mid<PS, 10>(m, square, rows, st);
+        case 11: return launch_mid<PS, 11>(m, square, rows, st);
+        case 12: return launch_mid<PS, 12>(m, square, rows, st);
+        case 13: return launch_mid<PS, 13>(m, square, rows, st);
+        case 14: return launch_mid<PS, 14>(m, square, rows, st);
+        case 15:
+            if constexpr (PS == 1) return launch_mid<PS, 15>(m, square, rows, st);
+            return cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
     }
 }
@@ -766,15 +835,16 @@ uint32_t carry_blocks(uint32_t nchunks) {
 
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
 
-cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const OperandDesc& b,
-                               bool square, int log_n, const ProductScratch& s, void* out,
-                               int out_fmt, size_t out_cap, const CarryLaunch& cl,
-                               cudaStream_t st, cudaEvent_t* ev) {
-    if (!shape_supported(log_n, square)) return cudaErrorInvalidValue;
-    if (ev) cudaEventRecord(ev[0], st);
+cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& a,
+                               const OperandDesc& b, bool square, int log_n,
+                               const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
+                               const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev) {
+    if (!shape_supported(log_n, square) || log_n > c.log_max) return cudaErrorInvalidValue;
+    const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
     const TransformShape sh = choose_shape(log_n);
     const size_t nn = (size_t)1 << log_n;
     const uint32_t tiles = (1u << sh.log_n1) / kCols;
+    if (ev) cudaEventRecord(ev[0], st);
 
     FwdColsArgs f{};
     f.op[0] = a;
@@ -782,7 +852,9 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     f.y = s.y;
     f.log_n = log_n;
     f.log_n1 = sh.log_n1;
-    cudaError_t e = dispatch_outer(sh.log_n2, c, &f, nullptr, square ? 1 : 2, tiles, st);
+    f.slot = slot;
+    cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, &f, nullptr, square ? 1 : 2, tiles, st)
+                            : dispatch_outer<1>(sh.log_n2, &f, nullptr, square ? 1 : 2, tiles, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[1], st);
 
@@ -791,6 +863,7 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     m.yb = square ? nullptr : s.y + kNumPrimes * nn;
     m.log_n = log_n;
     m.log_n2 = sh.log_n2;
+    m.slot = slot;
     for (int q = 0; q < kNumPrimes; ++q) {
         const uint32_t p = c.pr[q].p;
         // The pointwise Montgomery product leaves a factor 2^-32; the scale
@@ -802,7 +875,8 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
         m.scale_w[q] = mont_of(v, p);
         m.scale_wp[q] = m.scale_w[q] * c.pr[q].pinv;
     }
-    e = dispatch_mid(sh.log_n1, c, m, square, 1u << sh.log_n2, st);
+    e = ps == 0 ? dispatch_mid<0>(sh.log_n1, m, square, 1u << sh.log_n2, st)
+                : dispatch_mid<1>(sh.log_n1, m, square, 1u << sh.log_n2, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[2], st);
 
@@ -812,7 +886,9 @@ cudaError_t launch_ntt_product(const NttConsts& c, const OperandDesc& a, const O
     iv.spill = s.spill;
     iv.log_n = log_n;
     iv.log_n1 = sh.log_n1;
-    e = dispatch_outer(sh.log_n2, c, nullptr, &iv, 0, tiles, st);
+    iv.slot = slot;
+    e = ps == 0 ? dispatch_outer<0>(sh.log_n2, nullptr, &iv, 0, tiles, st)
+                : dispatch_outer<1>(sh.log_n2, nullptr, &iv, 0, tiles, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[3], st);
 

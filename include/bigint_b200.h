@@ -120,7 +120,7 @@ int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* npr
  * inside a fixed memory budget or a caller-managed pool that must not grow,
  * and host threads that may not call cudaMalloc because it can synchronize the
  * whole device.  It runs the same NTT kernels as bgpu_mul_u64_device, with all
- * scratch in one static device array (about 3.8 MB, plus 0.8 MB of static
+ * scratch in one static device array (about 3.8 MB, plus 0.35 MB of static
  * twiddle tables) that every GPU loading this library holds until the process
  * exits; it calls no cudaMalloc, cudaFree or other allocating routine.
  *  - d_a, d_b, d_out are device pointers on the current device; d_out receives
