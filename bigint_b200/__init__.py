@@ -30,6 +30,7 @@ from ._lib import (  # noqa: F401
     Stats,
     brute_mul,
     device_status,
+    get_split,
     init,
     kernel_times,
     last_launch_count,
@@ -39,6 +40,7 @@ from ._lib import (  # noqa: F401
     mul_device,
     mul_digits,
     ntt_mul,
+    set_split,
     set_kernel_timing,
     shutdown,
 )

@@ -81,6 +81,10 @@ def _load() -> C.CDLL:
     L.bgpu_device_status.restype = C.c_int
     L.bgpu_last_launch_count.argtypes = []
     L.bgpu_last_launch_count.restype = C.c_uint32
+    L.bgpu_set_split.argtypes = [C.c_uint32, C.c_uint32]
+    L.bgpu_set_split.restype = C.c_int
+    L.bgpu_get_split.argtypes = [C.c_uint32]
+    L.bgpu_get_split.restype = C.c_int
     L.bgpu_set_kernel_timing.argtypes = [C.c_int]
     L.bgpu_set_kernel_timing.restype = C.c_int
     L.bgpu_kernel_times.argtypes = [C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int,
@@ -230,6 +234,18 @@ def device_status(stream: int = 0) -> None:
 
 def last_launch_count() -> int:
     return int(lib.bgpu_last_launch_count())
+
+
+def set_split(log2_points: int, log2_column: int) -> None:
+    """Column-pass length 2^log2_column for 2^log2_points-point transforms (0 = default)."""
+    _check(lib.bgpu_set_split(int(log2_points), int(log2_column)), "bgpu_set_split")
+
+
+def get_split(log2_points: int) -> int:
+    r = lib.bgpu_get_split(int(log2_points))
+    if r < 0:
+        _check(r, "bgpu_get_split")
+    return r
 
 
 def set_kernel_timing(on: bool) -> None:

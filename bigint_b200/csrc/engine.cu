@@ -463,6 +463,16 @@ int bgpu_device_status(void* stream) {
 
 uint32_t bgpu_last_launch_count(void) { return g.last_launches; }
 
+int bgpu_set_split(uint32_t log2_points, uint32_t log2_column) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return set_split((int)log2_points, (int)log2_column) == 0 ? BGPU_OK : BGPU_ERR_INVALID_ARG;
+}
+
+int bgpu_get_split(uint32_t log2_points) {
+    if (log2_points < 5 || log2_points > kMaxLogN) return BGPU_ERR_INVALID_ARG;
+    return choose_shape((int)log2_points).log_n2;
+}
+
 int bgpu_set_kernel_timing(int on) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;

@@ -54,6 +54,7 @@ struct TransformShape {
 };
 
 TransformShape choose_shape(int log_n);
+int set_split(int log_n, int log_n2);  // 0 on success; log_n2 == 0 restores the default
 bool shape_supported(int log_n, bool square);
 size_t smem_fwd_cols(int log_n2);
 size_t smem_mid_rows(int log_n1, bool square);

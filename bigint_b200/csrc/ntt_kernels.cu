@@ -53,12 +53,19 @@ struct Plan {
 // Shared-memory placement of element i (of column col) in a [2^L][C] tile.
 // The XOR swizzles make every round's access pattern bank-conflict free
 // (rows: checked for L = 5..15; 8-column tiles: L = 2..11) and are bijective.
+// Both are linear over GF(2): sidx(i ^ k, col) = sidx(i, col) ^ soff(k), so a
+// group's element addresses are one base address XOR compile-time constants.
 template <int C>
-__device__ __forceinline__ uint32_t sidx(uint32_t i, int col) {
+__host__ __device__ constexpr uint32_t soff(uint32_t i) {
     if constexpr (C == 1)
         return i ^ (((i >> 3) ^ (i >> 4)) & 31u);
     else
-        return (i ^ (((i >> 2) ^ (i >> 4)) & 3u)) * C + col;
+        return (i ^ (((i >> 2) ^ (i >> 4)) & 3u)) * C;
+}
+
+template <int C>
+__device__ __forceinline__ uint32_t sidx(uint32_t i, int col) {
+    return soff<C>(i) | (uint32_t)col;
 }
 
 // ---- register-resident butterflies ------------------------------------------
@@ -68,6 +75,7 @@ __device__ __forceinline__ uint32_t sidx(uint32_t i, int col) {
 template <bool LAZY, int R, int HI, int LO>
 __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_low,
                                          const uint2* __restrict__ tw, uint32_t p) {
+    const uint2* twb = tw + base_low;  // every twiddle below is twb[compile-time offset]
 #pragma unroll
     for (int t = 0; t < R; ++t) {
         const uint32_t h = 1u << (HI - t);
@@ -78,8 +86,7 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_lo
             if (LO == 0 && (j & (dist - 1)) == 0) {
                 Bfly<LAZY>::dif1(x[j], x[j + dist], p);  // omega^0 (base_low is 0 when LO == 0)
             } else {
-                const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
-                const uint2 w = __ldg(tw + h + m);
+                const uint2 w = __ldg(twb + h + ((uint32_t)(j & (dist - 1)) << LO));
                 Bfly<LAZY>::dif(x[j], x[j + dist], w.x, w.y, p);
             }
         }
@@ -91,6 +98,7 @@ __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_lo
 template <bool LAZY, int R, int HI, int LO>
 __device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_low,
                                          const uint2* __restrict__ tw, uint32_t p) {
+    const uint2* twb = tw + base_low;
 #pragma unroll
     for (int t = R - 1; t >= 0; --t) {
         const uint32_t h = 1u << (HI - t);
@@ -101,8 +109,7 @@ __device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_lo
             if (LO == 0 && (j & (dist - 1)) == 0) {
                 Bfly<LAZY>::dit1(x[j], x[j + dist], p);
             } else {
-                const uint32_t m = base_low + ((uint32_t)(j & (dist - 1)) << LO);
-                const uint2 w = __ldg(tw + h + m);
+                const uint2 w = __ldg(twb + h + ((uint32_t)(j & (dist - 1)) << LO));
                 Bfly<LAZY>::dit(x[j], x[j + dist], w.x, w.y, p);
             }
         }
@@ -115,25 +122,28 @@ struct Group {
     static constexpr int R = Plan<L>::r(K), HI = Plan<L>::hi(K), LO = Plan<L>::lo(K);
     static constexpr int G = (1 << (L - R)) * C;
     int col;
-    uint32_t base, base_low;
+    uint32_t base, base_low, a0;
     __device__ __forceinline__ explicit Group(int g) {
         col = g % C;
         const uint32_t q = (uint32_t)(g / C);
         base_low = q & ((1u << LO) - 1u);
         base = ((q >> LO) << (HI + 1)) | base_low;
+        a0 = sidx<C>(base, col);
     }
     __device__ __forceinline__ uint32_t idx(int j) const { return base + ((uint32_t)j << LO); }
-    __device__ __forceinline__ uint32_t at(int j) const { return sidx<C>(idx(j), col); }
+    // smem address of element j: base's bits [LO, LO+R) are zero, so
+    // idx(j) = base ^ (j << LO) and the swizzle splits linearly.
+    __device__ __forceinline__ uint32_t at(int j) const { return a0 ^ soff<C>((uint32_t)j << LO); }
 };
 
 // One smem round (load -> butterflies -> store back); no sync inside.
 template <bool LAZY, int L, int C, int T, int K, bool INV>
-__device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict__ tw,
-                                           uint32_t p) {
+__device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict__ tw, uint32_t p,
+                                           int tid) {
     using Gr = Group<L, C, K>;
     constexpr int R = Gr::R;
 #pragma unroll 2
-    for (int g = threadIdx.x; g < Gr::G; g += T) {
+    for (int g = tid; g < Gr::G; g += T) {
         const Gr gr(g);
         uint32_t x[1 << R];
 #pragma unroll
@@ -149,23 +159,31 @@ __device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict
 
 // DIF rounds K..KEND in smem, each followed by a block barrier.
 template <bool LAZY, int L, int C, int T, int K, int KEND>
-__device__ __forceinline__ void dif_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
+__device__ __forceinline__ void dif_rounds(uint32_t* sm, const uint2* tw, uint32_t p, int tid) {
     if constexpr (K <= KEND) {
-        smem_round<LAZY, L, C, T, K, false>(sm, tw, p);
+        smem_round<LAZY, L, C, T, K, false>(sm, tw, p, tid);
         __syncthreads();
-        dif_rounds<LAZY, L, C, T, K + 1, KEND>(sm, tw, p);
+        dif_rounds<LAZY, L, C, T, K + 1, KEND>(sm, tw, p, tid);
     }
 }
 
 // DIT rounds K down to KEND in smem, each followed by a barrier.
 template <bool LAZY, int L, int C, int T, int K, int KEND>
-__device__ __forceinline__ void dit_rounds(uint32_t* sm, const uint2* tw, uint32_t p) {
+__device__ __forceinline__ void dit_rounds(uint32_t* sm, const uint2* tw, uint32_t p, int tid) {
     if constexpr (K >= KEND) {
-        smem_round<LAZY, L, C, T, K, true>(sm, tw, p);
+        smem_round<LAZY, L, C, T, K, true>(sm, tw, p, tid);
         __syncthreads();
-        dit_rounds<LAZY, L, C, T, K - 1, KEND>(sm, tw, p);
+        dit_rounds<LAZY, L, C, T, K - 1, KEND>(sm, tw, p, tid);
     }
 }
+
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while its predecessor finishes; pdl_wait() blocks
+// until every earlier kernel in the stream has completed and its writes are
+// visible (a no-op for an ordinary launch), pdl_trigger() lets the next
+// kernel's launch begin.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // omega_N^(+-e) as a fully reduced Montgomery form from the two split tables.
 __device__ __forceinline__ uint32_t inter_twiddle(const NttConsts& c, int q, int dir, uint32_t e,
@@ -181,6 +199,22 @@ template <bool LAZY>
 __device__ __forceinline__ uint32_t twiddle_mul(uint32_t x, uint32_t w, uint32_t p, uint32_t pinv) {
     const uint32_t r = mont_lazy(x, w, w * pinv, p);
     return LAZY ? r : csub(r, p);
+}
+
+// x * S * B for Montgomery pairs S = (w, w') and B = (bw, bw'): the
+// inter-pass twiddle split as a per-CTA power table entry times a per-group
+// factor, lazily (0, 2p) or strictly [0, p).
+template <bool LAZY>
+__device__ __forceinline__ uint32_t mul2(uint32_t x, uint2 sp, uint32_t bw, uint32_t bwp,
+                                         uint32_t p) {
+    const uint32_t y = mont_lazy(mont_lazy(x, sp.x, sp.y, p), bw, bwp, p);
+    return LAZY ? y : csub(y, p);
+}
+
+__host__ __device__ constexpr uint32_t brev_c(uint32_t v, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; ++i) r |= ((v >> i) & 1u) << (bits - 1 - i);
+    return r;
 }
 
 __device__ __forceinline__ uint32_t bitrev(uint32_t v, int bits) {
@@ -223,6 +257,22 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     uint32_t* y = a.y + ((size_t)opi * kNumPrimes + q) * nn;
     const uint32_t one_w = c.one_w[q], one_wp = c.one_wp[q];
 
+    // The last round's groups hold slots base + j (LO = 0) of one column n1;
+    // k2 = bitrev(base) + bitrev_RL(j) << (L2-RL), so the inter-pass twiddle
+    // omega_N^(n1*k2) = B(group) * S_col^bitrev_RL(j).  sS[col][m] holds the
+    // column powers S_col^m = omega_N^(n1 * m << (L2-RL)).
+    constexpr int RL = P2::r(NR - 1);
+    uint2* sS = reinterpret_cast<uint2*>(sm + (kCols << L2));
+    for (int t = threadIdx.x; t < (kCols << RL); t += T) {
+        const uint32_t col = (uint32_t)t >> RL, m = (uint32_t)t & ((1u << RL) - 1u);
+        const uint32_t e = (((c0 + col) * m) << (L2 - RL)) & (uint32_t)(nn - 1);
+        const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p);
+        sS[t] = make_uint2(w, w * pinv);
+    }
+    if constexpr (NR == 1) __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+
     // Round 0: rows n2 = base + (j << LO) read from the caller's digits.
     {
         using Gr = Group<L2, kCols, 0>;
@@ -247,13 +297,14 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
                 for (int j = 0; j < (1 << R); ++j) x[j] = 0;
             }
             if constexpr (NR == 1) {
+                const uint32_t n1 = c0 + gr.col;
+                const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & (uint32_t)(nn - 1),
+                                                  a.log_n, p);
+                const uint32_t bwp = bw * pinv;
+                const uint2* srow = sS + (gr.col << RL);
 #pragma unroll
-                for (int j = 0; j < (1 << R); ++j) {
-                    const uint32_t slot = gr.idx(j), n1 = c0 + gr.col;
-                    const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
-                    y[(size_t)slot * n1_len + n1] =
-                        twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 0, e, a.log_n, p), p, pinv);
-                }
+                for (int j = 0; j < (1 << R); ++j)
+                    y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
             } else {
 #pragma unroll
                 for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
@@ -262,7 +313,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     }
     if constexpr (NR > 1) {
         __syncthreads();
-        dif_rounds<LAZY, L2, kCols, T, 1, NR - 2>(sm, tw, p);
+        dif_rounds<LAZY, L2, kCols, T, 1, NR - 2>(sm, tw, p, threadIdx.x);
         // Last round: butterflies, inter-pass twiddle, store to global.
         using Gr = Group<L2, kCols, NR - 1>;
         constexpr int R = Gr::R;
@@ -274,13 +325,13 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
             for (int j = 0; j < (1 << R); ++j) x[j] = sm[gr.at(j)];
             dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
             const uint32_t n1 = c0 + gr.col;
+            const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & (uint32_t)(nn - 1),
+                                              a.log_n, p);
+            const uint32_t bwp = bw * pinv;
+            const uint2* srow = sS + (gr.col << RL);
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) {
-                const uint32_t slot = gr.idx(j);
-                const uint32_t e = (n1 * bitrev(slot, L2)) & (uint32_t)(nn - 1);
-                y[(size_t)slot * n1_len + n1] =
-                    twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 0, e, a.log_n, p), p, pinv);
-            }
+            for (int j = 0; j < (1 << R); ++j)
+                y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
         }
     }
 }
@@ -311,7 +362,7 @@ __device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t s
 template <bool LAZY, int L1, int T, bool SQR, bool SINGLE>
 __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& c, uint32_t* sa,
                                          uint32_t* sb, const uint32_t* row_a, const uint32_t* row_b,
-                                         uint32_t* row_out, int q, uint32_t k2) {
+                                         uint32_t* row_out, int q, uint32_t k2, const uint2* sT) {
     using P1 = Plan<L1>;
     constexpr int K = P1::nr - 1;
     using Gr = Group<L1, 1, K>;
@@ -341,12 +392,10 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
         }
         dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
         if constexpr (SINGLE) {
+            // one round covers the row: n1 = j, twiddle omega^-(k2 j) = sT[j]
+            const uint32_t bw = c.one_w[q], bwp = c.one_wp[q];
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) {
-                const uint32_t n1 = gr.idx(j);
-                const uint32_t e = (n1 * k2) & ((1u << a.log_n) - 1u);
-                row_out[n1] = twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 1, e, a.log_n, p), p, pinv);
-            }
+            for (int j = 0; j < (1 << R); ++j) row_out[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
         } else {
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) sa[gr.at(j)] = x[j];
@@ -373,7 +422,7 @@ __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, co
         for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
     }
     __syncthreads();
-    dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p);
+    dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p, threadIdx.x);
 }
 
 template <int PS, int L1, int T, bool SQR>
@@ -395,6 +444,20 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
     const uint32_t* row_b = SQR ? nullptr : a.yb + q * nn + (size_t)slot * (1u << L1);
     const uint32_t k2 = bitrev(slot, a.log_n2);
 
+    // The last DIT round's groups hold n1 = q + (j << LO0); the inverse
+    // inter-pass twiddle omega_N^-(k2 n1) = B(q) * T^j with the row-constant
+    // powers sT[j] = omega_N^-(k2 j << LO0).
+    constexpr int R0 = P1::r(0), LO0 = P1::lo(0);
+    uint2* sT = reinterpret_cast<uint2*>(sm + ((SQR ? 1u : 2u) << L1));
+    for (int t = threadIdx.x; t < (1 << R0); t += T) {
+        const uint32_t w = inter_twiddle(c, q, 1, ((k2 * (uint32_t)t) << LO0) & (uint32_t)(nn - 1),
+                                         a.log_n, p);
+        sT[t] = make_uint2(w, w * pinv);
+    }
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+
     if constexpr (NR == 1) {
         if constexpr (!SQR) {
             using Gr = Group<L1, 1, 0>;
@@ -411,16 +474,16 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
             }
             __syncthreads();
         }
-        mid_turn<LAZY, L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+        mid_turn<LAZY, L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
     } else {
         mid_dif_row<LAZY, L1, T>(row_a, sa, twf, p);
         if constexpr (!SQR) {
-            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p);  // A's last DIF round
+            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, threadIdx.x);  // A's last DIF round
             mid_dif_row<LAZY, L1, T>(row_b, sb, twf, p);
         }
-        mid_turn<LAZY, L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2);
+        mid_turn<LAZY, L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
         __syncthreads();
-        dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sa, twi, p);
+        dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sa, twi, p, threadIdx.x);
         // Round 0 (top bits): DIT, inverse twiddle, store to global.
         using Gr = Group<L1, 1, 0>;
         constexpr int R = Gr::R;
@@ -431,12 +494,10 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) x[j] = sa[gr.at(j)];
             dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+            const uint32_t bw = inter_twiddle(c, q, 1, (k2 * gr.base) & (uint32_t)(nn - 1), a.log_n, p);
+            const uint32_t bwp = bw * pinv;
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j) {
-                const uint32_t n1 = gr.idx(j);
-                const uint32_t e = (n1 * k2) & (uint32_t)(nn - 1);
-                row_a[n1] = twiddle_mul<LAZY>(x[j], inter_twiddle(c, q, 1, e, a.log_n, p), p, pinv);
-            }
+            for (int j = 0; j < (1 << R); ++j) row_a[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
         }
     }
 }
@@ -469,9 +530,12 @@ __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r
     w2 = (uint32_t)hi;
 }
 
-template <int PS, int L2, int T>
-__global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a) {
+template <int PS, int L2, int TP>
+__global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs a) {
+    // Three thread groups of TP threads, one per prime, transform their
+    // prime's column tile side by side; then all threads do the CRT.
     constexpr bool LAZY = PS == 0;
+    constexpr int T = kNumPrimes * TP;
     extern __shared__ __align__(16) uint32_t sm[];  // 3 x [2^L2][kCols]
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
@@ -479,51 +543,50 @@ __global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a) {
     const NttConsts& c = c_consts[a.slot];
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
-
+    const int q = threadIdx.x / TP, tq = threadIdx.x % TP;
+    uint32_t* s = sm + q * TILE;
+    const uint32_t p = c.pr[q].p;
+    const uint2* twi = c.stage[q][1];
+    const uint32_t* z = a.z + q * nn;
+    pdl_wait();
+    pdl_trigger();
+    // Round NR-1 (lowest bits): load slots from global.
+    {
+        using Gr = Group<L2, kCols, NR - 1>;
+        constexpr int R = Gr::R;
 #pragma unroll 1
-    for (int q = 0; q < kNumPrimes; ++q) {
-        uint32_t* s = sm + q * TILE;
-        const uint32_t p = c.pr[q].p;
-        const uint2* twi = c.stage[q][1];
-        const uint32_t* z = a.z + q * nn;
-        // Round NR-1 (lowest bits): load slots from global.
-        {
-            using Gr = Group<L2, kCols, NR - 1>;
-            constexpr int R = Gr::R;
-#pragma unroll 1
-            for (int g = threadIdx.x; g < Gr::G; g += T) {
-                const Gr gr(g);
-                uint32_t x[1 << R];
+        for (int g = tq; g < Gr::G; g += TP) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
 #pragma unroll
-                for (int j = 0; j < (1 << R); ++j)
-                    x[j] = z[(size_t)gr.idx(j) * n1_len + c0 + gr.col];
-                dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
-                if constexpr (NR == 1) {
+            for (int j = 0; j < (1 << R); ++j)
+                x[j] = z[(size_t)gr.idx(j) * n1_len + c0 + gr.col];
+            dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+            if constexpr (NR == 1) {
 #pragma unroll
-                    for (int j = 0; j < (1 << R); ++j) x[j] = Bfly<LAZY>::reduce(x[j], p);
-                }
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
+                for (int j = 0; j < (1 << R); ++j) x[j] = Bfly<LAZY>::reduce(x[j], p);
             }
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
+        }
+    }
+    __syncthreads();
+    if constexpr (NR > 1) {
+        dit_rounds<LAZY, L2, kCols, TP, NR - 2, 1>(s, twi, p, tq);
+        // Round 0: DIT then reduce to [0, p) for the CRT.
+        using Gr = Group<L2, kCols, 0>;
+        constexpr int R = Gr::R;
+#pragma unroll 1
+        for (int g = tq; g < Gr::G; g += TP) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) x[j] = s[gr.at(j)];
+            dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = Bfly<LAZY>::reduce(x[j], p);
         }
         __syncthreads();
-        if constexpr (NR > 1) {
-            dit_rounds<LAZY, L2, kCols, T, NR - 2, 1>(s, twi, p);
-            // Round 0: DIT then reduce to [0, p) for the CRT.
-            using Gr = Group<L2, kCols, 0>;
-            constexpr int R = Gr::R;
-#pragma unroll 1
-            for (int g = threadIdx.x; g < Gr::G; g += T) {
-                const Gr gr(g);
-                uint32_t x[1 << R];
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j) x[j] = s[gr.at(j)];
-                dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = Bfly<LAZY>::reduce(x[j], p);
-            }
-            __syncthreads();
-        }
     }
 
     // CRT and chunk sums: row n2 of the tile is chunk (c0 + N1*n2)/8.
@@ -567,6 +630,7 @@ __global__ void __launch_bounds__(T) k_inv_cols(const InvColsArgs a) {
 // ---- kernel 4: carry scan with decoupled look-back ----------------------------
 
 constexpr int kCarryThreads = 256;
+constexpr int kCarryPer = 4;  // consecutive chunks per thread
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait, then error exit
 
 struct CarryArgs {
@@ -589,39 +653,60 @@ __device__ __forceinline__ uint64_t make_flag(uint64_t epoch, uint32_t status, u
     return (epoch << 4) | ((uint64_t)status << 2) | ((uint64_t)g << 1) | pbit;
 }
 
+// Carry resolution over chunks of 8 coefficients.  Chunk c's final value is
+// (D_c + spill_{c-1} + carry_c) mod 2^256 with carry_{c+1} = G_c | (P_c & carry_c),
+// G_c = "D_c + spill_{c-1} >= 2^256", P_c = "D_c + spill_{c-1} == 2^256 - 1".
+// Each thread owns kCarryPer consecutive chunks and folds their (G, P); the
+// threads' pairs are scanned by warp ballots, a fold over warps, and a
+// decoupled look-back over blocks taken in ticket order.
 __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     __shared__ uint32_t s_bid, s_cin;
     __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
     if (threadIdx.x == 0) s_bid = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticket_base);
     __syncthreads();
+    pdl_wait();
+    pdl_trigger();
     const uint32_t bid = s_bid;
-    const uint32_t j = bid * kCarryThreads + threadIdx.x;
+    const uint32_t c0 = (bid * kCarryThreads + threadIdx.x) * kCarryPer;
     const uint32_t ntot = a.nchunks + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-    uint64_t S[4] = {0, 0, 0, 0};
-    uint32_t G = 0, P = 0;
-    uint64_t next_lo = 0, my_spill = 0;
-    if (j < ntot) {
-        if (j < a.nchunks) {
-            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(a.chunks + (size_t)j * 4);
-            ulonglong2 u = src[0], v = src[1];
-            S[0] = u.x, S[1] = u.y, S[2] = v.x, S[3] = v.y;
-            my_spill = a.spill[j];
-            if (j + 1 < a.nchunks) next_lo = a.chunks[(size_t)(j + 1) * 4];
-        }
-        const uint64_t s = j > 0 ? a.spill[j - 1] : 0;
-        uint64_t t = S[0] + s;
-        uint32_t cy = t < s;
-        S[0] = t;
+    uint64_t S[kCarryPer][4];
+    uint32_t Gc[kCarryPer], Pc[kCarryPer];
+    uint64_t sp = (c0 > 0 && c0 - 1 < a.nchunks) ? a.spill[c0 - 1] : 0;
 #pragma unroll
-        for (int k = 1; k < 4; ++k) {
-            t = S[k] + cy;
-            cy = cy & (t == 0);
-            S[k] = t;
+    for (int i = 0; i < kCarryPer; ++i) {
+        const uint32_t cc = c0 + i;
+        S[i][0] = S[i][1] = S[i][2] = S[i][3] = 0;
+        Gc[i] = 0;
+        Pc[i] = 1;  // chunks past the end pass carries through untouched
+        if (cc < ntot) {
+            uint64_t nsp = 0;
+            if (cc < a.nchunks) {
+                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(a.chunks + (size_t)cc * 4);
+                const ulonglong2 u = src[0], v = src[1];
+                S[i][0] = u.x, S[i][1] = u.y, S[i][2] = v.x, S[i][3] = v.y;
+                nsp = a.spill[cc];
+            }
+            uint64_t t = S[i][0] + sp;
+            uint32_t cy = t < sp;
+            S[i][0] = t;
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                t = S[i][k] + cy;
+                cy = cy & (t == 0);
+                S[i][k] = t;
+            }
+            Gc[i] = cy;
+            Pc[i] = (!cy) && ((S[i][0] & S[i][1] & S[i][2] & S[i][3]) == ~0ull);
+            sp = nsp;
         }
-        G = cy;
-        P = (!cy) && ((S[0] & S[1] & S[2] & S[3]) == ~0ull);
+    }
+    uint32_t G = 0, P = 1;
+#pragma unroll
+    for (int i = 0; i < kCarryPer; ++i) {
+        G = Gc[i] | (Pc[i] & G);
+        P = P & Pc[i];
     }
     const uint32_t gm = __ballot_sync(0xffffffffu, G);
     const uint32_t pm = __ballot_sync(0xffffffffu, P);
@@ -683,41 +768,78 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     for (int w = 0; w < warp; ++w) cw = s_wg[w] | (s_wp[w] & cw);
     const uint64_t sum = (uint64_t)gm + bm + cw;
     const uint32_t carries = (uint32_t)sum ^ gm ^ bm;
-    const uint32_t cin = (carries >> lane) & 1u;
-    if (j >= ntot) return;
-    uint32_t cy = cin;
+    uint32_t cin = (carries >> lane) & 1u;
+    if (c0 >= ntot) return;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint64_t t = S[k] + cy;
-        cy = cy & (t == 0);
-        S[k] = t;
+    for (int i = 0; i < kCarryPer; ++i) {
+        const uint32_t nxt = Gc[i] | (Pc[i] & cin);
+        uint32_t cy = cin;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint64_t t = S[i][k] + cy;
+            cy = cy & (t == 0);
+            S[i][k] = t;
+        }
+        cin = nxt;  // carry into chunk c0 + i + 1
     }
+    const uint32_t nvalid = min((uint32_t)kCarryPer, ntot - c0);
     if (a.out_fmt == kFmtLimb64) {
         uint64_t* o = static_cast<uint64_t*>(a.out);
-        const size_t base = (size_t)j * 4;
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (base + k < a.out_cap) o[base + k] = S[k];
+        for (int i = 0; i < kCarryPer; ++i) {
+            const size_t base = (size_t)(c0 + i) * 4;
+            if ((uint32_t)i < nvalid) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (base + k < a.out_cap) o[base + k] = S[i][k];
+            }
+        }
     } else {
-        // Final low limb of chunk j+1: its raw limb + this chunk's spill + carry out.
-        const uint32_t cout = G | (P & cin);
-        const uint64_t nl = next_lo + my_spill + cout;
+        // 28-bit digits starting in this thread's chunks; the last one may
+        // reach into chunk c0+kCarryPer, whose final low limb is its raw limb
+        // plus the spill and carry this thread passes on.
+        uint64_t nl = 0;
+        if (c0 + kCarryPer < a.nchunks) nl = a.chunks[(size_t)(c0 + kCarryPer) * 4];
+        nl += sp + cin;
         uint32_t* o = static_cast<uint32_t*>(a.out);
-        const uint64_t bit0 = (uint64_t)j * 256;
-        const uint64_t k0 = (bit0 + 27) / 28, k1 = (bit0 + 256 + 27) / 28;
-        for (uint64_t k = k0; k < k1 && k < a.out_cap; ++k) {
-            const uint32_t off = (uint32_t)(k * 28 - bit0);  // < 256
-            const uint32_t w = off >> 6, sh = off & 63;
-            const uint64_t lo = S[w];
-            const uint64_t hi = (w + 1 < 4) ? S[w + 1] : nl;
-            uint64_t v = lo >> sh;
-            if (sh > 36) v |= hi << (64 - sh);
-            o[k] = (uint32_t)v & ((1u << 28) - 1u);
+        const uint64_t bit0 = (uint64_t)c0 * 256;
+        uint64_t k = (bit0 + 27) / 28;
+        const uint64_t kend = min(((uint64_t)(c0 + nvalid) * 256 + 27) / 28, (uint64_t)a.out_cap);
+        const uint32_t off0 = (uint32_t)(k * 28 - bit0);  // < 28
+        uint64_t cur = S[0][0] >> off0;
+        int have = 64 - (int)off0;
+        const uint64_t mask = (1u << 28) - 1u;
+#pragma unroll
+        for (int w = 1; w <= kCarryPer * 4; ++w) {
+            const uint64_t nxtw = (w < kCarryPer * 4) ? S[w / 4][w % 4] : nl;
+            while (have >= 28) {
+                if (k < kend) o[k] = (uint32_t)(cur & mask);
+                ++k;
+                cur >>= 28;
+                have -= 28;
+            }
+            if (k < kend) o[k] = (uint32_t)((cur | (nxtw << have)) & mask);
+            ++k;
+            cur = nxtw >> (28 - have);
+            have = 36 + have;
         }
     }
 }
 
 // ---- host launchers -------------------------------------------------------------
+
+// Column length per transform length, as set by the tuner (0 = default split).
+static int g_split[kMaxLogN + 1] = {};
+
+int set_split(int log_n, int log_n2) {
+    if (log_n < 5 || log_n > kMaxLogN) return -1;
+    if (log_n2 != 0) {
+        const int l1 = log_n - log_n2;
+        if (log_n2 < 2 || log_n2 > 11 || l1 < 3 || l1 > 15) return -1;
+    }
+    g_split[log_n] = log_n2;
+    return 0;
+}
 
 TransformShape choose_shape(int log_n) {
     TransformShape s;
@@ -725,6 +847,7 @@ TransformShape choose_shape(int log_n) {
     int l2 = (log_n - 1) / 2;
     if (l2 > 11) l2 = 11;
     if (l2 < 2) l2 = 2;
+    if (log_n >= 0 && log_n <= kMaxLogN && g_split[log_n]) l2 = g_split[log_n];
     s.log_n2 = l2;
     s.log_n1 = log_n - l2;
     return s;
@@ -739,8 +862,10 @@ bool shape_supported(int log_n, bool square) {
     return true;
 }
 
-size_t smem_fwd_cols(int l2) { return (size_t)kCols * 4 << l2; }
-size_t smem_mid_rows(int l1, bool square) { return (square ? 1 : 2) * ((size_t)4 << l1); }
+size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 16 * sizeof(uint2); }
+size_t smem_mid_rows(int l1, bool square) {
+    return (square ? 1 : 2) * ((size_t)4 << l1) + 16 * sizeof(uint2);
+}
 size_t smem_inv_cols(int l2) { return (size_t)kNumPrimes * kCols * 4 << l2; }
 
 static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1 << (l1 - 4)) : 32); }
@@ -750,22 +875,39 @@ static void allow_smem(K k, size_t bytes) {
     if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Launch with programmatic stream serialization, so the kernel's launch
+// overlaps the tail of the previous kernel in the stream (each kernel waits in
+// pdl_wait() before touching memory an earlier kernel wrote).
+template <class Arg>
+static cudaError_t launch_k(void (*k)(Arg), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                            const Arg& arg) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, arg);
+}
+
 template <int PS, int L2>
 static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, int nops,
                                 uint32_t tiles, cudaStream_t st) {
-    constexpr int T = 256;
+    constexpr int T = 256, TP = 128;
     if (f) {
         auto k = k_fwd_cols<PS, L2, T>;
         const size_t sm = smem_fwd_cols(L2);
         allow_smem(k, sm);
-        k<<<dim3(tiles, kNumPrimes, nops), T, sm, st>>>(*f);
-    } else {
-        auto k = k_inv_cols<PS, L2, T>;
-        const size_t sm = smem_inv_cols(L2);
-        allow_smem(k, sm);
-        k<<<dim3(tiles), T, sm, st>>>(*inv);
+        return launch_k(k, dim3(tiles, kNumPrimes, nops), dim3(T), sm, st, *f);
     }
-    return cudaGetLastError();
+    auto k = k_inv_cols<PS, L2, TP>;
+    const size_t sm = smem_inv_cols(L2);
+    allow_smem(k, sm);
+    return launch_k(k, dim3(tiles), dim3(kNumPrimes * TP), sm, st, *inv);
 }
 
 template <int PS>
@@ -793,17 +935,15 @@ static cudaError_t launch_mid(const MidRowsArgs& m, bool square, uint32_t rows, 
     if (square) {
         auto k = k_mid_rows<PS, L1, T, true>;
         allow_smem(k, sm);
-        k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m);
-    } else {
-        if constexpr (L1 <= 14) {
-            auto k = k_mid_rows<PS, L1, T, false>;
-            allow_smem(k, sm);
-            k<<<dim3(rows, kNumPrimes), T, sm, st>>>(m);
-        } else {
-            return cudaErrorInvalidValue;
-        }
+        return launch_k(k, dim3(rows, kNumPrimes), dim3(T), sm, st, m);
     }
-    return cudaGetLastError();
+    if constexpr (L1 <= 14) {
+        auto k = k_mid_rows<PS, L1, T, false>;
+        allow_smem(k, sm);
+        return launch_k(k, dim3(rows, kNumPrimes), dim3(T), sm, st, m);
+    } else {
+        return cudaErrorInvalidValue;
+    }
 }
 
 template <int PS>
@@ -830,7 +970,8 @@ static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint3
 }
 
 uint32_t carry_blocks(uint32_t nchunks) {
-    return (nchunks + 1 + kCarryThreads - 1) / kCarryThreads;
+    constexpr uint32_t per_block = kCarryThreads * kCarryPer;
+    return (nchunks + 1 + per_block - 1) / per_block;
 }
 
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
@@ -904,8 +1045,7 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& 
     ca.ticket_base = cl.ticket_base;
     ca.epoch = cl.epoch;
     ca.err = s.err;
-    k_carry<<<carry_blocks(ca.nchunks), kCarryThreads, 0, st>>>(ca);
-    e = cudaGetLastError();
+    e = launch_k(k_carry, dim3(carry_blocks(ca.nchunks)), dim3(kCarryThreads), 0, st, ca);
     if (ev) cudaEventRecord(ev[4], st);
     return e;
 }

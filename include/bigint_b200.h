@@ -111,6 +111,15 @@ int bgpu_set_kernel_timing(int on);
  * (0 if none recorded).  Synchronizes on the last recorded event. */
 int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* nproducts);
 
+/* Transform split used for 2^log2_points-point products: the column pass
+ * length 2^log2_column (the row pass gets the rest).  Set by the autotuner
+ * (bigint_b200/autotune.py); log2_column = 0 restores the built-in choice.
+ * No reference counterpart (the reference has one radix-2 schedule,
+ * src/mul/ntt_multithread.cpp:333-379). */
+int bgpu_set_split(uint32_t log2_points, uint32_t log2_column);
+/* The column length exponent currently used for 2^log2_points points. */
+int bgpu_get_split(uint32_t log2_points);
+
 /* Largest product of bgpu_mul_u64_device_noalloc: na + nb u64 limbs. */
 #define BGPU_NOALLOC_MAX_LIMBS 65536u
 
