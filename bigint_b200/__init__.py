@@ -9,6 +9,7 @@ this package           reference                                       C-ABI
 ``mul(A, B)``          ``bigint::mul::_mul`` (mul.h:208-220)           ``bgpu_mul_u64``
 ``ntt_mul(A, B)``      ``bigint::mul::ntt::mul`` (ntt_multithread.cpp:444) ``bgpu_mul_u64`` + NTT
 ``brute_mul(A, B)``    ``bigint::mul::brute::mul`` (mul.h:82-102)      ``bgpu_mul_u64`` + schoolbook
+``fft_mul(A, B)``      ``bigint::mul::fft::mul`` (fft.cpp:281)         ``bgpu_mul_u64`` + FFT
 ``mul_digits(a, b,``   ``bigint::mul::mul_digits`` (mul.h:223-318)     ``bgpu_mul_digits``
 ``  precision, pos)``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
@@ -23,13 +24,16 @@ CPU fallback, and importing raises if the library is missing.
 from __future__ import annotations
 
 from ._lib import (  # noqa: F401
+    BGPU_FFT_AVERAGE_BOUND,
     BGPU_METHOD_AUTO,
+    BGPU_METHOD_FFT,
     BGPU_METHOD_NTT,
     BGPU_METHOD_SCHOOLBOOK,
     BigIntGPUError,
     Stats,
     brute_mul,
     device_status,
+    fft_mul,
     get_split,
     init,
     kernel_times,

@@ -15,6 +15,8 @@ BGPU_OK = 0
 BGPU_METHOD_AUTO = 0
 BGPU_METHOD_NTT = 1
 BGPU_METHOD_SCHOOLBOOK = 2
+BGPU_METHOD_FFT = 3
+BGPU_FFT_AVERAGE_BOUND = 0x10
 
 ERRORS = {
     -1: "BGPU_ERR_INVALID_ARG",
@@ -42,6 +44,7 @@ class _Stats(C.Structure):
         ("max_round_err", C.c_double),
         ("fell_back", C.c_int32),
         ("device_ms", C.c_float),
+        ("fft_bits", C.c_int32),
     ]
 
 
@@ -52,6 +55,7 @@ class Stats:
     max_round_err: float
     fell_back: bool
     device_ms: float
+    fft_bits: int
 
 
 def _load() -> C.CDLL:
@@ -139,7 +143,7 @@ def _as_digits(x) -> np.ndarray:
 
 def _stats(s: _Stats) -> Stats:
     return Stats(int(s.method), int(s.log2_points), float(s.max_round_err), bool(s.fell_back),
-                 float(s.device_ms))
+                 float(s.device_ms), int(s.fft_bits))
 
 
 def _mul_u64(A, B, flags: int, stats: bool, out=None):
@@ -182,6 +186,16 @@ def ntt_mul(A, B=None, *, stats: bool = False):
 def brute_mul(A, B=None, *, stats: bool = False):
     """A*B on the schoolbook kernel (``brute::mul``, mul.h:82-102); na+nb <= 256."""
     return _mul_u64(A, B, BGPU_METHOD_SCHOOLBOOK, stats)
+
+
+def fft_mul(A, B=None, *, digit_bits: int = 0, average_bound: bool = False, stats: bool = False):
+    """A*B through the FP64 complex-FFT form (``fft::mul``, fft.cpp:281).
+
+    ``digit_bits`` forces the bits per point (8..20; 0 = from the error
+    bound).  The result is exact: a product whose max rounding distance
+    exceeds 1/4 is recomputed on the NTT (reported in ``stats``)."""
+    flags = BGPU_METHOD_FFT | (int(digit_bits) << 8) | (BGPU_FFT_AVERAGE_BOUND if average_bound else 0)
+    return _mul_u64(A, B, flags, stats)
 
 
 def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = None, *,

@@ -7,6 +7,7 @@
 //   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -24,6 +25,8 @@ struct Engine {
     cudaStream_t stream = nullptr;
     NttConsts consts[kNumSets]{};
     void* d_tables[kNumSets] = {};
+    void* d_fft_tables = nullptr;
+    unsigned long long* d_fft_err = nullptr;
     // scratch arena
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -59,6 +62,8 @@ void release_locked() {
     cudaSetDevice(g.device);
     if (g.stream) cudaStreamSynchronize(g.stream);
     for (auto t : g.d_tables) cudaFree(t);
+    cudaFree(g.d_fft_tables);
+    cudaFree(g.d_fft_err);
     cudaFree(g.d_scratch);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
@@ -83,7 +88,14 @@ int build_tables_locked() {
         e = upload_consts(kSlotEngine + ps, g.consts[ps]);
         if (e != cudaSuccess) return cuda_status(e);
     }
-    return BGPU_OK;
+    std::vector<double2> fh(2 * fft_table_block());
+    build_fft_tables(fh.data());
+    cudaError_t e = cudaMalloc(&g.d_fft_tables, fh.size() * sizeof(double2));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(g.d_fft_tables, fh.data(), fh.size() * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = upload_fft_consts(make_fft_consts(static_cast<const double2*>(g.d_fft_tables)));
+    if (e == cudaSuccess) e = cudaMalloc(&g.d_fft_err, sizeof(unsigned long long));
+    return cuda_status(e);
 }
 
 int init_locked(int device) {
@@ -192,9 +204,11 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
 bool use_schoolbook(uint32_t flags, size_t na, size_t nb) {
     const uint32_t m = flags & BGPU_METHOD_MASK;
     if (m == BGPU_METHOD_SCHOOLBOOK) return true;
-    if (m == BGPU_METHOD_NTT) return false;
+    if (m == BGPU_METHOD_NTT || m == BGPU_METHOD_FFT) return false;
     return na + nb <= kSchoolbookMaxLimbs;
 }
+
+constexpr double kFftMaxErr = 0.25;  // larger rounding distances are recomputed on the NTT
 
 int check_device_error(int rc) {
     if (rc != BGPU_OK) return rc;
@@ -218,6 +232,73 @@ size_t strip64(const uint64_t* x, size_t n) {
 size_t strip32(const uint32_t* x, size_t n) {
     while (n > 0 && x[n - 1] == 0) --n;
     return n;
+}
+
+// Bits per FFT point.  Worst-case mode: the largest b in [8, 20] with
+//   2b <= 46 - L - log2(L + 1),   L = log2 of the transform length,
+// which keeps the error of every coefficient below 1/4 by Percival's bound for
+// FFT convolution (Math. Comp. 72 (2003), Thm. 5.1) applied to x = A + iB,
+// ||x||^2 <= 2N(2^b - 1)^2, with one extra complex multiply per point for the
+// two-pass twiddle and a one-bit margin.  Average mode (BGPU_FFT_AVERAGE_BOUND):
+//   2b <= 50 - L/2 - log2(L + 1),
+// the random-walk growth of the error; products whose measured error exceeds
+// 1/4 are recomputed on the NTT.
+int fft_pick(size_t na, size_t nb, uint32_t flags, int* bits, int* log_n) {
+    const int forced = (int)((flags >> 8) & 0x1Fu);
+    const bool avg = (flags & BGPU_FFT_AVERAGE_BOUND) != 0;
+    for (int b = forced ? forced : 20; b >= (forced ? forced : 8); --b) {
+        const uint64_t npa = (na * 64 + b - 1) / b, npb = (nb * 64 + b - 1) / b;
+        int L = 0;
+        while (((uint64_t)1 << L) < npa + npb - 1) ++L;
+        if (L < 8) L = 8;
+        if (!fft_shape_supported(L)) continue;
+        const double lim = avg ? 50.0 - L / 2.0 - std::log2(L + 1.0) : 46.0 - L - std::log2(L + 1.0);
+        if (!forced && 2.0 * b > lim) continue;
+        *bits = b;
+        *log_n = L;
+        return BGPU_OK;
+    }
+    return BGPU_ERR_CAPACITY;
+}
+
+// FFT product into dout (na + nb limbs); returns the measured max error.
+int fft_product_locked(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, int bits,
+                       int log_n, uint64_t* dout, cudaStream_t st, double* maxerr) {
+    const size_t nn = (size_t)1 << log_n;
+    const uint32_t nchunks = (uint32_t)((uint64_t)bits * nn / 256);
+    const size_t y_bytes = align256(nn * sizeof(double2)), co_bytes = align256(nn * 8);
+    const size_t ch_bytes = align256((size_t)nchunks * 32), sp_bytes = align256((size_t)nchunks * 8);
+    const size_t fl_bytes = align256((size_t)carry_blocks(nchunks) * 8);
+    int rc = ensure(&g.d_scratch, &g.scratch_bytes, y_bytes + co_bytes + ch_bytes + sp_bytes + fl_bytes);
+    if (rc != BGPU_OK) return rc;
+    char* base = static_cast<char*>(g.d_scratch);
+    FftScratch fs{};
+    fs.y = reinterpret_cast<double2*>(base);
+    fs.coef = reinterpret_cast<uint64_t*>(base + y_bytes);
+    fs.chunks = reinterpret_cast<uint64_t*>(base + y_bytes + co_bytes);
+    fs.spill = reinterpret_cast<uint64_t*>(base + y_bytes + co_bytes + ch_bytes);
+    fs.maxerr = g.d_fft_err;
+    fs.nchunks = nchunks;
+    ProductScratch ps{};
+    ps.flags = reinterpret_cast<uint64_t*>(base + y_bytes + co_bytes + ch_bytes + sp_bytes);
+    ps.ticket = g.d_ticket;
+    ps.err = g.d_err;
+    cudaError_t e = cudaMemsetAsync(g.d_fft_err, 0, sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = launch_fft_product(da, (uint32_t)na, db, (uint32_t)nb, bits, log_n, fs, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    CarryLaunch cl;
+    cl.ticket_base = g.ticket_base;
+    cl.epoch = ++g.epoch;
+    g.ticket_base += carry_blocks(nchunks);
+    e = launch_carry(fs.chunks, fs.spill, nchunks, dout, kFmtLimb64, na + nb, ps, cl, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    g.last_launches = 5;
+    unsigned long long bitsv = 0;
+    e = cudaMemcpyAsync(&bitsv, g.d_fft_err, sizeof(bitsv), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    memcpy(maxerr, &bitsv, sizeof(double));
+    return BGPU_OK;
 }
 
 int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
@@ -244,7 +325,26 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
     if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, b, nb * 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_status(e);
     if (stats) cudaEventRecord(g.ev0, st);
-    if (use_schoolbook(flags, na, nb)) {
+    int fbits = 0, flog = 0;
+    const bool want_fft = (flags & BGPU_METHOD_MASK) == BGPU_METHOD_FFT &&
+                          fft_pick(na, nb, flags, &fbits, &flog) == BGPU_OK;
+    if (want_fft) {
+        double err = 0;
+        rc = fft_product_locked(da, na, db, nb, fbits, flog, dout, st, &err);
+        if (rc != BGPU_OK) return rc;
+        if (stats) {
+            stats->method = BGPU_METHOD_FFT;
+            stats->log2_points = (uint32_t)flog;
+            stats->fft_bits = fbits;
+            stats->max_round_err = err;
+        }
+        if (!(err <= kFftMaxErr)) {  // also catches NaN
+            OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
+            OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
+            rc = multiply_device(oa, ob, square, dout, kFmtLimb64, nout, flags, st, nullptr);
+            if (stats) stats->fell_back = 1;
+        }
+    } else if (use_schoolbook(flags, na, nb)) {
         if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
         rc = cuda_status(launch_schoolbook(da, (uint32_t)na, db, (uint32_t)nb, dout, st));
         g.last_launches = 1;
@@ -413,7 +513,9 @@ const char* bgpu_strerror(int code) {
 int bgpu_mul_u64(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
                  size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats) {
     if (!a || !b || !out_len || (!out && out_cap) || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
-    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_FFT) return BGPU_ERR_INVALID_ARG;
+    const uint32_t fb = (flags >> 8) & 0x1Fu;
+    if (fb && (fb < 8 || fb > 20)) return BGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);

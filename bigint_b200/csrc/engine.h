@@ -90,6 +90,42 @@ extern const char* const kNttKernelNames[kNttLaunches];
 
 uint32_t carry_blocks(uint32_t nchunks);
 
+// ---- FP64 complex-FFT form ----
+constexpr int kFftMaxLogN = 23;     // largest FFT transform (2^23 complex points)
+constexpr int kFftStageLog = 13;    // FFT stage tables cover pair distances < 2^13
+constexpr int kFftTwLog = 26, kFftTwSplit = 13;
+
+struct FftConsts {
+    const double2* stage[2];  // [dir]: entry h+m = exp(-+ i pi m / h)
+    const double2* th[2];     // exp(-+ 2 pi i (i << split) / 2^log_max)
+    const double2* tl[2];     // exp(-+ 2 pi i i / 2^log_max)
+    int log_max, split;
+};
+cudaError_t upload_fft_consts(const FftConsts& c);
+
+struct FftShape {
+    int log_n, log_n1, log_n2;
+};
+FftShape fft_choose_shape(int log_n);
+bool fft_shape_supported(int log_n);
+
+struct FftScratch {
+    double2* y;                  // N complex points
+    uint64_t* coef;              // N rounded coefficients
+    unsigned long long* maxerr;  // largest |x - round(x)| as double bits
+    uint64_t* chunks;            // nchunks * 4 limbs
+    uint64_t* spill;             // nchunks
+    uint32_t nchunks;            // bits * N / 256
+};
+
+// Forward FFT of (A + iB), square, inverse, rounding and chunk sums (4 launches);
+// the caller then runs the carry scan over `nchunks` chunks.
+cudaError_t launch_fft_product(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
+                               int bits, int log_n, const FftScratch& s, cudaStream_t stream);
+cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,
+                         int out_fmt, size_t out_cap, const ProductScratch& s, const CarryLaunch& cl,
+                         cudaStream_t stream);
+
 // Schoolbook product for small operands (one CTA); out has na+nb limbs.
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
                               uint64_t* out, cudaStream_t stream);

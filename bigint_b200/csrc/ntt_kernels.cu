@@ -25,6 +25,7 @@
 #include <cuda/atomic>
 
 #include "engine.h"
+#include "pass_common.cuh"
 
 namespace bgpu {
 
@@ -34,38 +35,6 @@ __constant__ NttConsts c_consts[kConstSlots];
 
 cudaError_t upload_consts(int slot, const NttConsts& c) {
     return cudaMemcpyToSymbol(c_consts, &c, sizeof(NttConsts), slot * sizeof(NttConsts));
-}
-
-// Round split of a length-2^L transform into radix-2^r rounds (r <= 4),
-// top bits first (DIF order).
-template <int L>
-struct Plan {
-    static constexpr int nr = (L + 3) / 4;
-    __host__ __device__ static constexpr int r(int k) { return L / nr + (k < L % nr ? 1 : 0); }
-    __host__ __device__ static constexpr int hi(int k) {
-        int h = L - 1;
-        for (int i = 0; i < k; ++i) h -= r(i);
-        return h;
-    }
-    __host__ __device__ static constexpr int lo(int k) { return hi(k) - r(k) + 1; }
-};
-
-// Shared-memory placement of element i (of column col) in a [2^L][C] tile.
-// The XOR swizzles make every round's access pattern bank-conflict free
-// (rows: checked for L = 5..15; 8-column tiles: L = 2..11) and are bijective.
-// Both are linear over GF(2): sidx(i ^ k, col) = sidx(i, col) ^ soff(k), so a
-// group's element addresses are one base address XOR compile-time constants.
-template <int C>
-__host__ __device__ constexpr uint32_t soff(uint32_t i) {
-    if constexpr (C == 1)
-        return i ^ (((i >> 3) ^ (i >> 4)) & 31u);
-    else
-        return (i ^ (((i >> 2) ^ (i >> 4)) & 3u)) * C;
-}
-
-template <int C>
-__device__ __forceinline__ uint32_t sidx(uint32_t i, int col) {
-    return soff<C>(i) | (uint32_t)col;
 }
 
 // ---- register-resident butterflies ------------------------------------------
@@ -116,26 +85,6 @@ __device__ __forceinline__ void dit_regs(uint32_t (&x)[1 << R], uint32_t base_lo
     }
 }
 
-// Group g of round K on a [2^L][C] tile: column and base element index.
-template <int L, int C, int K>
-struct Group {
-    static constexpr int R = Plan<L>::r(K), HI = Plan<L>::hi(K), LO = Plan<L>::lo(K);
-    static constexpr int G = (1 << (L - R)) * C;
-    int col;
-    uint32_t base, base_low, a0;
-    __device__ __forceinline__ explicit Group(int g) {
-        col = g % C;
-        const uint32_t q = (uint32_t)(g / C);
-        base_low = q & ((1u << LO) - 1u);
-        base = ((q >> LO) << (HI + 1)) | base_low;
-        a0 = sidx<C>(base, col);
-    }
-    __device__ __forceinline__ uint32_t idx(int j) const { return base + ((uint32_t)j << LO); }
-    // smem address of element j: base's bits [LO, LO+R) are zero, so
-    // idx(j) = base ^ (j << LO) and the swizzle splits linearly.
-    __device__ __forceinline__ uint32_t at(int j) const { return a0 ^ soff<C>((uint32_t)j << LO); }
-};
-
 // One smem round (load -> butterflies -> store back); no sync inside.
 template <bool LAZY, int L, int C, int T, int K, bool INV>
 __device__ __forceinline__ void smem_round(uint32_t* sm, const uint2* __restrict__ tw, uint32_t p,
@@ -176,14 +125,6 @@ __device__ __forceinline__ void dit_rounds(uint32_t* sm, const uint2* tw, uint32
         dit_rounds<LAZY, L, C, T, K - 1, KEND>(sm, tw, p, tid);
     }
 }
-
-// Programmatic dependent launch: a kernel launched with programmatic stream
-// serialization may start while its predecessor finishes; pdl_wait() blocks
-// until every earlier kernel in the stream has completed and its writes are
-// visible (a no-op for an ordinary launch), pdl_trigger() lets the next
-// kernel's launch begin.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // omega_N^(+-e) as a fully reduced Montgomery form from the two split tables.
 __device__ __forceinline__ uint32_t inter_twiddle(const NttConsts& c, int q, int dir, uint32_t e,
@@ -870,29 +811,6 @@ size_t smem_inv_cols(int l2) { return (size_t)kNumPrimes * kCols * 4 << l2; }
 
 static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1 << (l1 - 4)) : 32); }
 
-template <class K>
-static void allow_smem(K k, size_t bytes) {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
-// Launch with programmatic stream serialization, so the kernel's launch
-// overlaps the tail of the previous kernel in the stream (each kernel waits in
-// pdl_wait() before touching memory an earlier kernel wrote).
-template <class Arg>
-static cudaError_t launch_k(void (*k)(Arg), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                            const Arg& arg) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k, arg);
-}
 
 template <int PS, int L2>
 static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, int nops,
@@ -1048,6 +966,24 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& 
     e = launch_k(k_carry, dim3(carry_blocks(ca.nchunks)), dim3(kCarryThreads), 0, st, ca);
     if (ev) cudaEventRecord(ev[4], st);
     return e;
+}
+
+cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,
+                         int out_fmt, size_t out_cap, const ProductScratch& s, const CarryLaunch& cl,
+                         cudaStream_t st) {
+    CarryArgs ca{};
+    ca.chunks = chunks;
+    ca.spill = spill;
+    ca.nchunks = nchunks;
+    ca.out = out;
+    ca.out_fmt = out_fmt;
+    ca.out_cap = out_cap;
+    ca.flags = s.flags;
+    ca.ticket = s.ticket;
+    ca.ticket_base = cl.ticket_base;
+    ca.epoch = cl.epoch;
+    ca.err = s.err;
+    return launch_k(k_carry, dim3(carry_blocks(nchunks)), dim3(kCarryThreads), 0, st, ca);
 }
 
 const char* const kNttKernelNames[kNttLaunches] = {"k_fwd_cols", "k_mid_rows", "k_inv_cols",

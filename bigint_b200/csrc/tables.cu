@@ -1,6 +1,8 @@
 // Host-side construction of twiddle tables and constants (see tables.h).
 #include "tables.h"
 
+#include <cmath>
+
 namespace bgpu {
 namespace {
 
@@ -63,6 +65,45 @@ void build_tables(int ps, int stage_log, uint2* host) {
             for (size_t i = 0; i < tl_n; ++i, v = v * r % p) tl[i] = mont_pair(v, p);
         }
     }
+}
+
+// exp(sign * 2 pi i * num / den) rounded from long double.
+static double2 root_of_unity(uint64_t num, uint64_t den, int sign) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    const long double ang = 2.0L * pi * (long double)num / (long double)den;
+    return make_double2((double)cosl(ang), (double)(sign * sinl(ang)));
+}
+
+void build_fft_tables(double2* host) {
+    const size_t stage_n = (size_t)1 << kFftStageLog;
+    const size_t th_n = (size_t)1 << (kFftTwLog - kFftTwSplit), tl_n = (size_t)1 << kFftTwSplit;
+    for (int dir = 0; dir < 2; ++dir) {
+        const int sign = dir ? 1 : -1;  // forward uses exp(-2 pi i / N)
+        double2* base = host + (size_t)dir * fft_table_block();
+        base[0] = make_double2(1.0, 0.0);
+        for (size_t h = 1; h < stage_n; h <<= 1)
+            for (size_t m = 0; m < h; ++m) base[h + m] = root_of_unity(m, 2 * h, sign);
+        double2* th = base + stage_n;
+        double2* tl = th + th_n;
+        const uint64_t full = (uint64_t)1 << kFftTwLog;
+        for (size_t i = 0; i < th_n; ++i) th[i] = root_of_unity((uint64_t)i << kFftTwSplit, full, sign);
+        for (size_t i = 0; i < tl_n; ++i) tl[i] = root_of_unity(i, full, sign);
+    }
+}
+
+FftConsts make_fft_consts(const double2* dev_tables) {
+    FftConsts c{};
+    const size_t stage_n = (size_t)1 << kFftStageLog;
+    const size_t th_n = (size_t)1 << (kFftTwLog - kFftTwSplit);
+    for (int dir = 0; dir < 2; ++dir) {
+        const double2* base = dev_tables + (size_t)dir * fft_table_block();
+        c.stage[dir] = base;
+        c.th[dir] = base + stage_n;
+        c.tl[dir] = base + stage_n + th_n;
+    }
+    c.log_max = kFftTwLog;
+    c.split = kFftTwSplit;
+    return c;
 }
 
 NttConsts make_consts(int ps, int stage_log, const uint2* dev_tables) {

@@ -39,7 +39,14 @@ extern "C" {
 #define BGPU_METHOD_AUTO 0u
 #define BGPU_METHOD_NTT 1u        /* three-prime NTT (the plain method) */
 #define BGPU_METHOD_SCHOOLBOOK 2u /* O(n*m) kernel; na + nb <= BGPU_SCHOOLBOOK_MAX_LIMBS */
+#define BGPU_METHOD_FFT 3u        /* FP64 complex FFT (bgpu_mul_u64 only); products whose
+                                     max |x - round(x)| exceeds 1/4 are redone on the NTT */
 #define BGPU_METHOD_MASK 0xFu
+/* FFT form: choose bits per point from the average-case error growth instead
+ * of the worst-case bound (more bits, runtime check + NTT fallback). */
+#define BGPU_FFT_AVERAGE_BOUND 0x10u
+/* FFT form: force b bits per point (8..20) in flags bits 8..12. */
+#define BGPU_FFT_BITS(b) ((uint32_t)(b) << 8)
 
 #define BGPU_SCHOOLBOOK_MAX_LIMBS 256u
 #define BGPU_MAX_LOG2_POINTS 26u  /* transform points are 32-bit digits */
@@ -47,9 +54,10 @@ extern "C" {
 typedef struct bgpu_stats {
     int32_t method;          /* BGPU_METHOD_* actually used */
     uint32_t log2_points;    /* transform length (0 for schoolbook) */
-    double max_round_err;    /* floating-point forms: max |x - round(x)|; 0 otherwise */
-    int32_t fell_back;       /* floating-point forms: recomputed on the NTT */
+    double max_round_err;    /* FFT form: max |x - round(x)| over all coefficients; 0 otherwise */
+    int32_t fell_back;       /* FFT form: 1 if the product was recomputed on the NTT */
     float device_ms;         /* device time of the multiply kernels */
+    int32_t fft_bits;        /* FFT form: bits per point used */
 } bgpu_stats;
 
 /* Select the CUDA device and build the twiddle tables.  Idempotent; a second

@@ -1,0 +1,81 @@
+"""The FP64 complex-FFT form (fft::mul, src/mul/fft.cpp:281-384) on the GPU:
+every product must come out exact -- either the FFT's rounding distance
+stays within 1/4 or the product is recomputed on the NTT -- and the recorded
+error statistics must behave as the error bound says."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import SEED, golden_u64_cases, rand_limbs
+from oracle.pyoracle import limbs_to_int
+
+pytestmark = pytest.mark.gpu
+ONES = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def test_golden_through_fft(bb, golden):
+    for kind, a, b, c in golden_u64_cases(golden):
+        args = (a,) if b is None else (a, b)
+        got, st = bb.fft_mul(*args, stats=True)
+        assert np.array_equal(got, c), (kind, a.size)
+        if st.method == bb.BGPU_METHOD_FFT:
+            assert st.max_round_err < 0.25 and not st.fell_back, (kind, st)
+
+
+@pytest.mark.parametrize("n", [1000, 20000, 1 << 16, 1 << 18])
+def test_worst_case_bound_random_never_falls_back(bb, port, n):
+    rng = np.random.default_rng(SEED + n)
+    a, b = rand_limbs(rng, n), rand_limbs(rng, n)
+    got, st = bb.fft_mul(a, b, stats=True)
+    assert st.method == bb.BGPU_METHOD_FFT and not st.fell_back
+    assert 0.0 <= st.max_round_err < 0.25
+    assert np.array_equal(got, port.mul(a, b))
+
+
+@pytest.mark.parametrize("n", [4096, 1 << 16, 1 << 18])
+def test_worst_case_bound_all_ones(bb, port, n):
+    ones = np.full(n, ONES)
+    got, st = bb.fft_mul(ones, stats=True)
+    assert st.method == bb.BGPU_METHOD_FFT and not st.fell_back and st.max_round_err < 0.25
+    assert np.array_equal(got, port.ntt_mul(ones))
+
+
+def test_average_bound_uses_more_bits_and_stays_exact(bb, port):
+    rng = np.random.default_rng(SEED + 21)
+    n = 1 << 16
+    a, b = rand_limbs(rng, n), rand_limbs(rng, n)
+    _, st_w = bb.fft_mul(a, b, stats=True)
+    got, st_a = bb.fft_mul(a, b, average_bound=True, stats=True)
+    assert st_a.fft_bits > st_w.fft_bits
+    assert np.array_equal(got, port.mul(a, b))
+
+
+def test_oversized_points_fall_back_to_ntt(bb, port):
+    """20-bit points on all-ones operands of 2^18 limbs: coefficients near
+    2^58 cannot be represented in FP64, the error check trips and the NTT
+    recomputes the product, so the result is still exact."""
+    ones = np.full(1 << 18, ONES)
+    got, st = bb.fft_mul(ones, digit_bits=20, stats=True)
+    assert st.fell_back and st.max_round_err > 0.25
+    assert np.array_equal(got, port.ntt_mul(ones))
+
+
+@pytest.mark.parametrize("bits", range(8, 21))
+def test_forced_bits_small(bb, bits):
+    """Forced b = 8..20 at small sizes (the reference's forced-B regression,
+    tests/measure_digit_bits.cpp:186-201)."""
+    rng = np.random.default_rng(SEED + 100 + bits)
+    for _ in range(3):
+        a, b = rand_limbs(rng, 40), rand_limbs(rng, 31)
+        got, st = bb.fft_mul(a, b, digit_bits=bits, stats=True)
+        assert st.fft_bits == bits
+        assert limbs_to_int(got) == limbs_to_int(a) * limbs_to_int(b)
+
+
+def test_fft_square_and_unbalanced(bb, port):
+    rng = np.random.default_rng(SEED + 22)
+    a = rand_limbs(rng, 30000)
+    assert np.array_equal(bb.fft_mul(a), port.ntt_mul(a))
+    b = rand_limbs(rng, 300)
+    assert np.array_equal(bb.fft_mul(a, b), port.mul(a, b))
