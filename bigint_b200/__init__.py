@@ -29,6 +29,7 @@ from ._lib import (  # noqa: F401
     BGPU_METHOD_FFT,
     BGPU_METHOD_NTT,
     BGPU_METHOD_SCHOOLBOOK,
+    BatchPlan,
     BigIntGPUError,
     Stats,
     brute_mul,
@@ -41,6 +42,7 @@ from ._lib import (  # noqa: F401
     lib,
     library_path,
     mul,
+    mul_batch_device,
     mul_device,
     mul_digits,
     ntt_mul,

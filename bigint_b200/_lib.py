@@ -58,6 +58,11 @@ class Stats:
     fft_bits: int
 
 
+class Product(C.Structure):
+    _fields_ = [("a", C.c_void_p), ("na", C.c_size_t), ("b", C.c_void_p), ("nb", C.c_size_t),
+                ("out", C.c_void_p)]
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(library_path):
         raise ImportError(
@@ -85,6 +90,17 @@ def _load() -> C.CDLL:
     L.bgpu_device_status.restype = C.c_int
     L.bgpu_last_launch_count.argtypes = []
     L.bgpu_last_launch_count.restype = C.c_uint32
+    L.bgpu_batch_plan_create.argtypes = [C.POINTER(Product), C.c_size_t, C.c_uint32,
+                                         C.POINTER(C.c_void_p)]
+    L.bgpu_batch_plan_create.restype = C.c_int
+    L.bgpu_batch_plan_run.argtypes = [C.c_void_p, C.c_void_p]
+    L.bgpu_batch_plan_run.restype = C.c_int
+    L.bgpu_batch_plan_destroy.argtypes = [C.c_void_p]
+    L.bgpu_batch_plan_destroy.restype = C.c_int
+    L.bgpu_batch_plan_launches.argtypes = [C.c_void_p]
+    L.bgpu_batch_plan_launches.restype = C.c_uint32
+    L.bgpu_mul_batch_device.argtypes = [C.POINTER(Product), C.c_size_t, C.c_uint32, C.c_void_p]
+    L.bgpu_mul_batch_device.restype = C.c_int
     L.bgpu_set_split.argtypes = [C.c_uint32, C.c_uint32]
     L.bgpu_set_split.restype = C.c_int
     L.bgpu_get_split.argtypes = [C.c_uint32]
@@ -278,3 +294,47 @@ def kernel_times() -> tuple[list[tuple[str, float]], int]:
     if n < 0:
         _check(n, "bgpu_kernel_times")
     return [(names[i].decode(), float(ms[i])) for i in range(n)], int(cnt.value)
+
+
+class BatchPlan:
+    """A batch of independent device-resident products, captured in one CUDA
+    graph (``bgpu_batch_plan_*``).  ``products`` is a list of
+    ``(a_ptr, na, b_ptr, nb, out_ptr)`` device pointers/lengths."""
+
+    def __init__(self, products, flags: int = 0):
+        _ensure_init()
+        arr = (Product * max(1, len(products)))()
+        for i, (a, na, b, nb, out) in enumerate(products):
+            arr[i] = Product(C.c_void_p(a), na, C.c_void_p(b), nb, C.c_void_p(out))
+        self._h = C.c_void_p()
+        _check(lib.bgpu_batch_plan_create(arr, len(products), flags, C.byref(self._h)),
+               "bgpu_batch_plan_create")
+        self.count = len(products)
+
+    @property
+    def launches(self) -> int:
+        return int(lib.bgpu_batch_plan_launches(self._h))
+
+    def run(self, stream: int = 0) -> None:
+        _check(lib.bgpu_batch_plan_run(self._h, C.c_void_p(stream or None)), "bgpu_batch_plan_run")
+
+    def close(self) -> None:
+        if self._h:
+            lib.bgpu_batch_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mul_batch_device(products, stream: int = 0, flags: int = 0) -> None:
+    """One-shot batch (create, run, synchronize, destroy)."""
+    _ensure_init()
+    arr = (Product * max(1, len(products)))()
+    for i, (a, na, b, nb, out) in enumerate(products):
+        arr[i] = Product(C.c_void_p(a), na, C.c_void_p(b), nb, C.c_void_p(out))
+    _check(lib.bgpu_mul_batch_device(arr, len(products), flags, C.c_void_p(stream or None)),
+           "bgpu_mul_batch_device")

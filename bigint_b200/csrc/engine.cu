@@ -565,6 +565,50 @@ int bgpu_device_status(void* stream) {
 
 uint32_t bgpu_last_launch_count(void) { return g.last_launches; }
 
+static EngineHooks hooks_locked() {
+    EngineHooks h{};
+    for (int ps = 0; ps < kNumSets; ++ps) h.consts[ps] = g.consts[ps];
+    h.err = g.d_err;
+    return h;
+}
+
+int bgpu_batch_plan_create(const bgpu_product* products, size_t count, uint32_t flags,
+                           bgpu_batch_plan* plan) {
+    if (!plan || (!products && count)) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return batch_plan_create(products, count, flags, g.device, hooks_locked(), plan);
+}
+
+int bgpu_batch_plan_run(bgpu_batch_plan plan, void* stream) {
+    if (!plan) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    const int rc = batch_plan_run(plan, static_cast<cudaStream_t>(stream));
+    if (rc == BGPU_OK) g.last_launches = batch_plan_launches(plan);
+    return rc;
+}
+
+int bgpu_batch_plan_destroy(bgpu_batch_plan plan) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    batch_plan_destroy(plan);
+    return BGPU_OK;
+}
+
+uint32_t bgpu_batch_plan_launches(bgpu_batch_plan plan) { return batch_plan_launches(plan); }
+
+int bgpu_mul_batch_device(const bgpu_product* products, size_t count, uint32_t flags, void* stream) {
+    bgpu_batch_plan plan = nullptr;
+    int rc = bgpu_batch_plan_create(products, count, flags, &plan);
+    if (rc != BGPU_OK) return rc;
+    rc = bgpu_batch_plan_run(plan, stream);
+    if (rc == BGPU_OK) rc = bgpu_device_status(stream);
+    bgpu_batch_plan_destroy(plan);
+    return rc;
+}
+
 int bgpu_set_split(uint32_t log2_points, uint32_t log2_column) {
     std::lock_guard<std::mutex> lk(g_mu);
     return set_split((int)log2_points, (int)log2_column) == 0 ? BGPU_OK : BGPU_ERR_INVALID_ARG;

@@ -46,6 +46,18 @@ struct OperandDesc {
     int fmt;
 };
 
+// Everything one product needs; the products of one launch share N and
+// whether they are squares.
+struct ProductDesc {
+    OperandDesc op[2];  // op[1] == op[0] when squaring
+    uint32_t* y;        // (square ? 1 : 2) * 3 * N residues
+    uint64_t* chunks;   // N/2 limbs (8-coefficient chunk sums)
+    uint64_t* spill;    // N/8 spills
+    uint64_t* flags;    // carry-scan block status words
+    void* out;          // output in the launch's format
+    size_t out_cap;     // elements of out
+};
+
 // Shape of a two-pass transform of N = N1 * N2 points.
 struct TransformShape {
     int log_n;   // log2 N
@@ -73,6 +85,8 @@ struct ProductScratch {
 struct CarryLaunch {
     uint64_t ticket_base;
     uint64_t epoch;
+    unsigned long long* ticket = nullptr;  // batch launches: ticket counter
+    uint32_t* err = nullptr;               // batch launches: sticky error word
 };
 
 // Launch the full NTT product pipeline (4 kernels) on `stream`.
@@ -89,6 +103,13 @@ constexpr int kNttLaunches = 4;
 extern const char* const kNttKernelNames[kNttLaunches];
 
 uint32_t carry_blocks(uint32_t nchunks);
+
+// Batched NTT products: `count` products of 2^log_n points described by the
+// device array `descs`, four launches in all (one per pass, a grid slice per
+// product); the carry scan takes count * carry_blocks(N/8) tickets.
+cudaError_t launch_ntt_batch(int slot, const NttConsts& host, const ProductDesc* descs, int count,
+                             bool square, int log_n, int out_fmt, const CarryLaunch& cl,
+                             cudaStream_t stream);
 
 // ---- FP64 complex-FFT form ----
 constexpr int kFftMaxLogN = 23;     // largest FFT transform (2^23 complex points)
@@ -125,6 +146,21 @@ cudaError_t launch_fft_product(const uint64_t* a, uint32_t na, const uint64_t* b
 cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,
                          int out_fmt, size_t out_cap, const ProductScratch& s, const CarryLaunch& cl,
                          cudaStream_t stream);
+
+// ---- batched products (batch.cu) ----
+struct EngineHooks {
+    NttConsts consts[kNumSets];
+    uint32_t* err;
+};
+}  // namespace bgpu
+struct bgpu_batch_plan_s;
+struct bgpu_product;
+namespace bgpu {
+int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, int device,
+                      const EngineHooks& hooks, bgpu_batch_plan_s** out);
+int batch_plan_run(bgpu_batch_plan_s* p, cudaStream_t st);
+void batch_plan_destroy(bgpu_batch_plan_s* p);
+uint32_t batch_plan_launches(const bgpu_batch_plan_s* p);
 
 // Schoolbook product for small operands (one CTA); out has na+nb limbs.
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,

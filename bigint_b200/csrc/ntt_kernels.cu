@@ -176,11 +176,18 @@ __device__ __forceinline__ uint32_t load_digit32(const OperandDesc& in, uint32_t
 
 // ---- kernel 1: forward column pass ------------------------------------------
 
+// Per-launch argument blocks: a device descriptor array for batches, or the
+// single product's descriptor inline (descs == nullptr).
 struct FwdColsArgs {
-    OperandDesc op[2];
-    uint32_t* y;  // [op][prime][N]
-    int log_n, log_n1, slot;
+    const ProductDesc* descs;
+    ProductDesc one;
+    int nops, log_n, log_n1, slot;
 };
+
+__device__ __forceinline__ const ProductDesc& product(const ProductDesc* descs, const ProductDesc& one,
+                                                      uint32_t p) {
+    return descs ? descs[p] : one;
+}
 
 template <int PS, int L2, int T>
 __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
@@ -189,13 +196,14 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
     const NttConsts& c = c_consts[a.slot];
-    const int q = blockIdx.y, opi = blockIdx.z;
+    const int q = blockIdx.y, opi = blockIdx.z % a.nops;
+    const ProductDesc& pd = product(a.descs, a.one, blockIdx.z / a.nops);
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
-    const OperandDesc in = opi == 0 ? a.op[0] : a.op[1];
+    const OperandDesc in = opi == 0 ? pd.op[0] : pd.op[1];
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
-    uint32_t* y = a.y + ((size_t)opi * kNumPrimes + q) * nn;
+    uint32_t* y = pd.y + ((size_t)opi * kNumPrimes + q) * nn;
     const uint32_t one_w = c.one_w[q], one_wp = c.one_wp[q];
 
     // The last round's groups hold slots base + j (LO = 0) of one column n1;
@@ -280,8 +288,8 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
 // ---- kernel 2: middle row pass ----------------------------------------------
 
 struct MidRowsArgs {
-    uint32_t* ya;        // [prime][N], result written in place
-    const uint32_t* yb;  // [prime][N] or null (square)
+    const ProductDesc* descs;  // y: A's planes (result in place), then B's unless squaring
+    ProductDesc one;
     int log_n, log_n2, slot;
     uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
 };
@@ -375,14 +383,15 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
     const NttConsts& c = c_consts[a.slot];
     uint32_t* sa = sm;
     uint32_t* sb = sm + (1u << L1);
-    const int q = blockIdx.y;
+    const int q = blockIdx.y % kNumPrimes;
+    const ProductDesc& pd = product(a.descs, a.one, blockIdx.y / kNumPrimes);
     const uint32_t slot = blockIdx.x;
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* twf = c.stage[q][0];
     const uint2* twi = c.stage[q][1];
     const size_t nn = (size_t)1 << a.log_n;
-    uint32_t* row_a = a.ya + q * nn + (size_t)slot * (1u << L1);
-    const uint32_t* row_b = SQR ? nullptr : a.yb + q * nn + (size_t)slot * (1u << L1);
+    uint32_t* row_a = pd.y + q * nn + (size_t)slot * (1u << L1);
+    const uint32_t* row_b = SQR ? nullptr : pd.y + (kNumPrimes + q) * nn + (size_t)slot * (1u << L1);
     const uint32_t k2 = bitrev(slot, a.log_n2);
 
     // The last DIT round's groups hold n1 = q + (j << LO0); the inverse
@@ -446,9 +455,8 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
 // ---- kernel 3: inverse column pass + CRT + chunk sums -------------------------
 
 struct InvColsArgs {
-    const uint32_t* z;  // [prime][N]
-    uint64_t* chunks;   // 4 limbs per chunk
-    uint64_t* spill;    // per chunk
+    const ProductDesc* descs;  // y (A's planes after the middle pass), chunks, spill
+    ProductDesc one;
     int log_n, log_n1, slot;
 };
 
@@ -485,10 +493,11 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     const int q = threadIdx.x / TP, tq = threadIdx.x % TP;
+    const ProductDesc& pd = product(a.descs, a.one, blockIdx.y);
     uint32_t* s = sm + q * TILE;
     const uint32_t p = c.pr[q].p;
     const uint2* twi = c.stage[q][1];
-    const uint32_t* z = a.z + q * nn;
+    const uint32_t* z = pd.y + q * nn;
     pdl_wait();
     pdl_trigger();
     // Round NR-1 (lowest bits): load slots from global.
@@ -561,10 +570,10 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
             carry = s >> 32;
         }
         const size_t chunk = (size_t)(c0 / kCols) + (size_t)(n1_len / kCols) * n2;
-        ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.chunks + chunk * 4);
+        ulonglong2* dst = reinterpret_cast<ulonglong2*>(pd.chunks + chunk * 4);
         dst[0] = make_ulonglong2(d[0] | ((uint64_t)d[1] << 32), d[2] | ((uint64_t)d[3] << 32));
         dst[1] = make_ulonglong2(d[4] | ((uint64_t)d[5] << 32), d[6] | ((uint64_t)d[7] << 32));
-        a.spill[chunk] = d[8] | ((uint64_t)d[9] << 32);
+        pd.spill[chunk] = d[8] | ((uint64_t)d[9] << 32);
     }
 }
 
@@ -575,13 +584,11 @@ constexpr int kCarryPer = 4;  // consecutive chunks per thread
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait, then error exit
 
 struct CarryArgs {
-    const uint64_t* chunks;
-    const uint64_t* spill;
-    uint32_t nchunks;  // real chunks; chunk nchunks is a virtual all-zero chunk
-    void* out;
+    const ProductDesc* descs;  // chunks, spill, flags, out, out_cap per product
+    ProductDesc one;
+    uint32_t nchunks;  // real chunks per product; chunk nchunks is a virtual all-zero chunk
+    uint32_t bpp;      // carry blocks per product
     int out_fmt;
-    size_t out_cap;
-    uint64_t* flags;
     unsigned long long* ticket;
     uint64_t ticket_base;
     uint64_t epoch;
@@ -607,14 +614,21 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     __syncthreads();
     pdl_wait();
     pdl_trigger();
-    const uint32_t bid = s_bid;
+    // tickets enumerate (product, block) in order, so a block's predecessor
+    // within its product always holds a smaller ticket
+    const ProductDesc& pd = product(a.descs, a.one, s_bid / a.bpp);
+    const uint32_t bid = s_bid % a.bpp;
+    const uint64_t* chunks = pd.chunks;
+    const uint64_t* spill = pd.spill;
+    uint64_t* flags = pd.flags;
+    const size_t out_cap = pd.out_cap;
     const uint32_t c0 = (bid * kCarryThreads + threadIdx.x) * kCarryPer;
     const uint32_t ntot = a.nchunks + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     uint64_t S[kCarryPer][4];
     uint32_t Gc[kCarryPer], Pc[kCarryPer];
-    uint64_t sp = (c0 > 0 && c0 - 1 < a.nchunks) ? a.spill[c0 - 1] : 0;
+    uint64_t sp = (c0 > 0 && c0 - 1 < a.nchunks) ? spill[c0 - 1] : 0;
 #pragma unroll
     for (int i = 0; i < kCarryPer; ++i) {
         const uint32_t cc = c0 + i;
@@ -624,10 +638,10 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         if (cc < ntot) {
             uint64_t nsp = 0;
             if (cc < a.nchunks) {
-                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(a.chunks + (size_t)cc * 4);
+                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)cc * 4);
                 const ulonglong2 u = src[0], v = src[1];
                 S[i][0] = u.x, S[i][1] = u.y, S[i][2] = v.x, S[i][3] = v.y;
-                nsp = a.spill[cc];
+                nsp = spill[cc];
             }
             uint64_t t = S[i][0] + sp;
             uint32_t cy = t < sp;
@@ -665,7 +679,7 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         }
         uint32_t cin = 0;
         cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> self(
-            *reinterpret_cast<unsigned long long*>(a.flags + bid));
+            *reinterpret_cast<unsigned long long*>(flags + bid));
         if (bid == 0) {
             self.store(make_flag(a.epoch, 2, bG, 0), cuda::memory_order_release);
         } else {
@@ -674,7 +688,7 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
             uint32_t spins = 0;
             while (true) {
                 cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pred(
-                    *reinterpret_cast<unsigned long long*>(a.flags + k));
+                    *reinterpret_cast<unsigned long long*>(flags + k));
                 const uint64_t f = pred.load(cuda::memory_order_acquire);
                 if ((f >> 4) != a.epoch) {
                     if (++spins > kSpinLimit) {
@@ -725,14 +739,14 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     }
     const uint32_t nvalid = min((uint32_t)kCarryPer, ntot - c0);
     if (a.out_fmt == kFmtLimb64) {
-        uint64_t* o = static_cast<uint64_t*>(a.out);
+        uint64_t* o = static_cast<uint64_t*>(pd.out);
 #pragma unroll
         for (int i = 0; i < kCarryPer; ++i) {
             const size_t base = (size_t)(c0 + i) * 4;
             if ((uint32_t)i < nvalid) {
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
-                    if (base + k < a.out_cap) o[base + k] = S[i][k];
+                    if (base + k < out_cap) o[base + k] = S[i][k];
             }
         }
     } else {
@@ -740,12 +754,12 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         // reach into chunk c0+kCarryPer, whose final low limb is its raw limb
         // plus the spill and carry this thread passes on.
         uint64_t nl = 0;
-        if (c0 + kCarryPer < a.nchunks) nl = a.chunks[(size_t)(c0 + kCarryPer) * 4];
+        if (c0 + kCarryPer < a.nchunks) nl = chunks[(size_t)(c0 + kCarryPer) * 4];
         nl += sp + cin;
-        uint32_t* o = static_cast<uint32_t*>(a.out);
+        uint32_t* o = static_cast<uint32_t*>(pd.out);
         const uint64_t bit0 = (uint64_t)c0 * 256;
         uint64_t k = (bit0 + 27) / 28;
-        const uint64_t kend = min(((uint64_t)(c0 + nvalid) * 256 + 27) / 28, (uint64_t)a.out_cap);
+        const uint64_t kend = min(((uint64_t)(c0 + nvalid) * 256 + 27) / 28, (uint64_t)out_cap);
         const uint32_t off0 = (uint32_t)(k * 28 - bit0);  // < 28
         uint64_t cur = S[0][0] >> off0;
         int have = 64 - (int)off0;
@@ -813,75 +827,77 @@ static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1
 
 
 template <int PS, int L2>
-static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, int nops,
-                                uint32_t tiles, cudaStream_t st) {
+static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, uint32_t tiles,
+                                int count, cudaStream_t st) {
     constexpr int T = 256, TP = 128;
     if (f) {
         auto k = k_fwd_cols<PS, L2, T>;
         const size_t sm = smem_fwd_cols(L2);
         allow_smem(k, sm);
-        return launch_k(k, dim3(tiles, kNumPrimes, nops), dim3(T), sm, st, *f);
+        return launch_k(k, dim3(tiles, kNumPrimes, f->nops * count), dim3(T), sm, st, *f);
     }
     auto k = k_inv_cols<PS, L2, TP>;
     const size_t sm = smem_inv_cols(L2);
     allow_smem(k, sm);
-    return launch_k(k, dim3(tiles), dim3(kNumPrimes * TP), sm, st, *inv);
+    return launch_k(k, dim3(tiles, count), dim3(kNumPrimes * TP), sm, st, *inv);
 }
 
 template <int PS>
-static cudaError_t dispatch_outer(int l2, const FwdColsArgs* f, const InvColsArgs* inv, int nops,
-                                  uint32_t tiles, cudaStream_t st) {
+static cudaError_t dispatch_outer(int l2, const FwdColsArgs* f, const InvColsArgs* inv,
+                                  uint32_t tiles, int count, cudaStream_t st) {
     switch (l2) {
-        case 2: return launch_outer<PS, 2>(f, inv, nops, tiles, st);
-        case 3: return launch_outer<PS, 3>(f, inv, nops, tiles, st);
-        case 4: return launch_outer<PS, 4>(f, inv, nops, tiles, st);
-        case 5: return launch_outer<PS, 5>(f, inv, nops, tiles, st);
-        case 6: return launch_outer<PS, 6>(f, inv, nops, tiles, st);
-        case 7: return launch_outer<PS, 7>(f, inv, nops, tiles, st);
-        case 8: return launch_outer<PS, 8>(f, inv, nops, tiles, st);
-        case 9: return launch_outer<PS, 9>(f, inv, nops, tiles, st);
-        case 10: return launch_outer<PS, 10>(f, inv, nops, tiles, st);
-        case 11: return launch_outer<PS, 11>(f, inv, nops, tiles, st);
+        case 2: return launch_outer<PS, 2>(f, inv, tiles, count, st);
+        case 3: return launch_outer<PS, 3>(f, inv, tiles, count, st);
+        case 4: return launch_outer<PS, 4>(f, inv, tiles, count, st);
+        case 5: return launch_outer<PS, 5>(f, inv, tiles, count, st);
+        case 6: return launch_outer<PS, 6>(f, inv, tiles, count, st);
+        case 7: return launch_outer<PS, 7>(f, inv, tiles, count, st);
+        case 8: return launch_outer<PS, 8>(f, inv, tiles, count, st);
+        case 9: return launch_outer<PS, 9>(f, inv, tiles, count, st);
+        case 10: return launch_outer<PS, 10>(f, inv, tiles, count, st);
+        case 11: return launch_outer<PS, 11>(f, inv, tiles, count, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <int PS, int L1>
-static cudaError_t launch_mid(const MidRowsArgs& m, bool square, uint32_t rows, cudaStream_t st) {
+static cudaError_t launch_mid(const MidRowsArgs& m, bool square, uint32_t rows, int count,
+                              cudaStream_t st) {
     constexpr int T = mid_threads(L1);
     const size_t sm = smem_mid_rows(L1, square);
+    const dim3 grid(rows, kNumPrimes * count);
     if (square) {
         auto k = k_mid_rows<PS, L1, T, true>;
         allow_smem(k, sm);
-        return launch_k(k, dim3(rows, kNumPrimes), dim3(T), sm, st, m);
+        return launch_k(k, grid, dim3(T), sm, st, m);
     }
     if constexpr (L1 <= 14) {
         auto k = k_mid_rows<PS, L1, T, false>;
         allow_smem(k, sm);
-        return launch_k(k, dim3(rows, kNumPrimes), dim3(T), sm, st, m);
+        return launch_k(k, grid, dim3(T), sm, st, m);
     } else {
         return cudaErrorInvalidValue;
     }
 }
 
 template <int PS>
-static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint32_t rows,
+static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint32_t rows, int count,
                                 cudaStream_t st) {
     switch (l1) {
-        case 3: return launch_mid<PS, 3>(m, square, rows, st);
-        case 4: return launch_mid<PS, 4>(m, square, rows, st);
-        case 5: return launch_mid<PS, 5>(m, square, rows, st);
-        case 6: return launch_mid<PS, 6>(m, square, rows, st);
-        case 7: return launch_mid<PS, 7>(m, square, rows, st);
-        case 8: return launch_mid<PS, 8>(m, square, rows, st);
-        case 9: return launch_mid<PS, 9>(m, square, rows, st);
-        case 10: return launch_mid<PS, 10>(m, square, rows, st);
-        case 11: return launch_mid<PS, 11>(m, square, rows, st);
-        case 12: return launch_mid<PS, 12>(m, square, rows, st);
-        case 13: return launch_mid<PS, 13>(m, square, rows, st);
-        case 14: return launch_mid<PS, 14>(m, square, rows, st);
+        case 3: return launch_mid<PS, 3>(m, square, rows, count, st);
+        case 4: return launch_mid<PS, 4>(m, square, rows, count, st);
+        case 5: return launch_mid<PS, 5>(m, square, rows, count, st);
+        case 6: return launch_mid<PS, 6>(m, square, rows, count, st);
+        case 7: return launch_mid<PS, 7>(m, square, rows, count, st);
+        case 8: return launch_mid<PS, 8>(m, square, rows, count, st);
+        case 9: return launch_mid<PS, 9>(m, square, rows, count, st);
+        case 10: return launch_mid<PS, 10>(m, square, rows, count, st);
+        case 11: return launch_mid<PS, 11>(m, square, rows, count, st);
+        case 12: return launch_mid<PS, 12>(m, square, rows, count, st);
+        case 13: return launch_mid<PS, 13>(m, square, rows, count, st);
+        case 14: return launch_mid<PS, 14>(m, square, rows, count, st);
         case 15:
-            if constexpr (PS == 1) return launch_mid<PS, 15>(m, square, rows, st);
+            if constexpr (PS == 1) return launch_mid<PS, 15>(m, square, rows, count, st);
             return cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
     }
@@ -894,11 +910,12 @@ uint32_t carry_blocks(uint32_t nchunks) {
 
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
 
-cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& a,
-                               const OperandDesc& b, bool square, int log_n,
-                               const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
-                               const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev) {
-    if (!shape_supported(log_n, square) || log_n > c.log_max) return cudaErrorInvalidValue;
+// The four launches of `count` products (descs on the device, or `one`).
+static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDesc* descs,
+                                   const ProductDesc& one, int count, bool square, int log_n,
+                                   int out_fmt, const CarryLaunch& cl, cudaStream_t st,
+                                   cudaEvent_t* ev) {
+    if (!shape_supported(log_n, square) || log_n > c.log_max || count < 1) return cudaErrorInvalidValue;
     const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
     const TransformShape sh = choose_shape(log_n);
     const size_t nn = (size_t)1 << log_n;
@@ -906,20 +923,20 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& 
     if (ev) cudaEventRecord(ev[0], st);
 
     FwdColsArgs f{};
-    f.op[0] = a;
-    f.op[1] = square ? a : b;
-    f.y = s.y;
+    f.descs = descs;
+    f.one = one;
+    f.nops = square ? 1 : 2;
     f.log_n = log_n;
     f.log_n1 = sh.log_n1;
     f.slot = slot;
-    cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, &f, nullptr, square ? 1 : 2, tiles, st)
-                            : dispatch_outer<1>(sh.log_n2, &f, nullptr, square ? 1 : 2, tiles, st);
+    cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, &f, nullptr, tiles, count, st)
+                            : dispatch_outer<1>(sh.log_n2, &f, nullptr, tiles, count, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[1], st);
 
     MidRowsArgs m{};
-    m.ya = s.y;
-    m.yb = square ? nullptr : s.y + kNumPrimes * nn;
+    m.descs = descs;
+    m.one = one;
     m.log_n = log_n;
     m.log_n2 = sh.log_n2;
     m.slot = slot;
@@ -934,56 +951,80 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& 
         m.scale_w[q] = mont_of(v, p);
         m.scale_wp[q] = m.scale_w[q] * c.pr[q].pinv;
     }
-    e = ps == 0 ? dispatch_mid<0>(sh.log_n1, m, square, 1u << sh.log_n2, st)
-                : dispatch_mid<1>(sh.log_n1, m, square, 1u << sh.log_n2, st);
+    e = ps == 0 ? dispatch_mid<0>(sh.log_n1, m, square, 1u << sh.log_n2, count, st)
+                : dispatch_mid<1>(sh.log_n1, m, square, 1u << sh.log_n2, count, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[2], st);
 
     InvColsArgs iv{};
-    iv.z = s.y;
-    iv.chunks = s.chunks;
-    iv.spill = s.spill;
+    iv.descs = descs;
+    iv.one = one;
     iv.log_n = log_n;
     iv.log_n1 = sh.log_n1;
     iv.slot = slot;
-    e = ps == 0 ? dispatch_outer<0>(sh.log_n2, nullptr, &iv, 0, tiles, st)
-                : dispatch_outer<1>(sh.log_n2, nullptr, &iv, 0, tiles, st);
+    e = ps == 0 ? dispatch_outer<0>(sh.log_n2, nullptr, &iv, tiles, count, st)
+                : dispatch_outer<1>(sh.log_n2, nullptr, &iv, tiles, count, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[3], st);
 
     CarryArgs ca{};
-    ca.chunks = s.chunks;
-    ca.spill = s.spill;
+    ca.descs = descs;
+    ca.one = one;
     ca.nchunks = (uint32_t)(nn / kCols);
-    ca.out = out;
+    ca.bpp = carry_blocks(ca.nchunks);
     ca.out_fmt = out_fmt;
-    ca.out_cap = out_cap;
-    ca.flags = s.flags;
-    ca.ticket = s.ticket;
+    ca.ticket = cl.ticket;
     ca.ticket_base = cl.ticket_base;
     ca.epoch = cl.epoch;
-    ca.err = s.err;
-    e = launch_k(k_carry, dim3(carry_blocks(ca.nchunks)), dim3(kCarryThreads), 0, st, ca);
+    ca.err = cl.err;
+    e = launch_k(k_carry, dim3(ca.bpp * count), dim3(kCarryThreads), 0, st, ca);
     if (ev) cudaEventRecord(ev[4], st);
     return e;
+}
+
+cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& a,
+                               const OperandDesc& b, bool square, int log_n,
+                               const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
+                               const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev) {
+    ProductDesc one{};
+    one.op[0] = a;
+    one.op[1] = square ? a : b;
+    one.y = s.y;
+    one.chunks = s.chunks;
+    one.spill = s.spill;
+    one.flags = s.flags;
+    one.out = out;
+    one.out_cap = out_cap;
+    CarryLaunch c2 = cl;
+    c2.ticket = s.ticket;
+    c2.err = s.err;
+    return launch_ntt_core(slot, c, nullptr, one, 1, square, log_n, out_fmt, c2, st, ev);
+}
+
+cudaError_t launch_ntt_batch(int slot, const NttConsts& c, const ProductDesc* descs, int count,
+                             bool square, int log_n, int out_fmt, const CarryLaunch& cl,
+                             cudaStream_t st) {
+    return launch_ntt_core(slot, c, descs, ProductDesc{}, count, square, log_n, out_fmt, cl, st,
+                           nullptr);
 }
 
 cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,
                          int out_fmt, size_t out_cap, const ProductScratch& s, const CarryLaunch& cl,
                          cudaStream_t st) {
     CarryArgs ca{};
-    ca.chunks = chunks;
-    ca.spill = spill;
+    ca.one.chunks = const_cast<uint64_t*>(chunks);
+    ca.one.spill = const_cast<uint64_t*>(spill);
+    ca.one.flags = s.flags;
+    ca.one.out = out;
+    ca.one.out_cap = out_cap;
     ca.nchunks = nchunks;
-    ca.out = out;
+    ca.bpp = carry_blocks(nchunks);
     ca.out_fmt = out_fmt;
-    ca.out_cap = out_cap;
-    ca.flags = s.flags;
     ca.ticket = s.ticket;
     ca.ticket_base = cl.ticket_base;
     ca.epoch = cl.epoch;
     ca.err = s.err;
-    return launch_k(k_carry, dim3(carry_blocks(nchunks)), dim3(kCarryThreads), 0, st, ca);
+    return launch_k(k_carry, dim3(ca.bpp), dim3(kCarryThreads), 0, st, ca);
 }
 
 const char* const kNttKernelNames[kNttLaunches] = {"k_fwd_cols", "k_mid_rows", "k_inv_cols",

@@ -119,6 +119,36 @@ int bgpu_set_kernel_timing(int on);
  * (0 if none recorded).  Synchronizes on the last recorded event. */
 int bgpu_kernel_times(const char** names, float* mean_ms, int cap, uint32_t* nproducts);
 
+/* ---- batches of independent products ----
+ * The reference multiplies one pair per call; its binary-splitting caller
+ * (examples/pi.cpp:41-80) and fast_pow produce many independent products per
+ * step.  A plan groups a batch by size (schoolbook below
+ * BGPU_SCHOOLBOOK_MAX_LIMBS, then one NTT class per transform length),
+ * allocates its scratch once and captures every launch of the batch into one
+ * CUDA graph; running the plan is one graph launch.  Pointers are device
+ * pointers; out receives na + nb limbs; a == b with na == nb squares.  A plan
+ * is bound to the pointers it was made with (rebuild it for new buffers). */
+typedef struct bgpu_product {
+    const uint64_t* a;
+    size_t na;
+    const uint64_t* b;
+    size_t nb;
+    uint64_t* out;
+} bgpu_product;
+
+typedef struct bgpu_batch_plan_s* bgpu_batch_plan;
+
+int bgpu_batch_plan_create(const bgpu_product* products, size_t count, uint32_t flags,
+                           bgpu_batch_plan* plan);
+/* Launch the plan's graph on `stream` (asynchronous); device-side errors are
+ * reported by bgpu_device_status.  Runs of one plan must not overlap. */
+int bgpu_batch_plan_run(bgpu_batch_plan plan, void* stream);
+int bgpu_batch_plan_destroy(bgpu_batch_plan plan);
+/* Kernel launches one run of the plan makes (its graph's kernel nodes). */
+uint32_t bgpu_batch_plan_launches(bgpu_batch_plan plan);
+/* One-shot: create, run, synchronize, destroy. */
+int bgpu_mul_batch_device(const bgpu_product* products, size_t count, uint32_t flags, void* stream);
+
 /* Transform split used for 2^log2_points-point products: the column pass
  * length 2^log2_column (the row pass gets the rest).  Set by the autotuner
  * (bigint_b200/autotune.py); log2_column = 0 restores the built-in choice.
