@@ -46,6 +46,8 @@ from ._lib import (  # noqa: F401
     mul_device,
     mul_digits,
     ntt_mul,
+    product_tree,
+    product_tree_device,
     set_split,
     set_kernel_timing,
     shutdown,

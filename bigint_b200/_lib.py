@@ -101,6 +101,10 @@ def _load() -> C.CDLL:
     L.bgpu_batch_plan_launches.restype = C.c_uint32
     L.bgpu_mul_batch_device.argtypes = [C.POINTER(Product), C.c_size_t, C.c_uint32, C.c_void_p]
     L.bgpu_mul_batch_device.restype = C.c_int
+    L.bgpu_product_tree_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p]
+    L.bgpu_product_tree_device.restype = C.c_int
+    L.bgpu_product_tree_u64.argtypes = [u64p, C.c_size_t, u64p, C.c_size_t, szp]
+    L.bgpu_product_tree_u64.restype = C.c_int
     L.bgpu_set_split.argtypes = [C.c_uint32, C.c_uint32]
     L.bgpu_set_split.restype = C.c_int
     L.bgpu_get_split.argtypes = [C.c_uint32]
@@ -338,3 +342,25 @@ def mul_batch_device(products, stream: int = 0, flags: int = 0) -> None:
         arr[i] = Product(C.c_void_p(a), na, C.c_void_p(b), nb, C.c_void_p(out))
     _check(lib.bgpu_mul_batch_device(arr, len(products), flags, C.c_void_p(stream or None)),
            "bgpu_mul_batch_device")
+
+
+def product_tree(leaves) -> np.ndarray:
+    """Pairwise product tree of u64 values (binary splitting, examples/pi.cpp:41-80)."""
+    _ensure_init()
+    x = _as_limbs(leaves)
+    if x.size == 0:
+        raise BigIntGPUError(-1, "bgpu_product_tree_u64 (no leaves)")
+    width = 1 << max(0, (x.size - 1).bit_length())
+    out = np.empty(width, dtype=np.uint64)
+    n = C.c_size_t(0)
+    u64p = C.POINTER(C.c_uint64)
+    _check(lib.bgpu_product_tree_u64(x.ctypes.data_as(u64p), x.size, out.ctypes.data_as(u64p),
+                                     out.size, C.byref(n)), "bgpu_product_tree_u64")
+    return out[: n.value]
+
+
+def product_tree_device(leaves_ptr: int, n: int, out_ptr: int, out_cap: int, stream: int = 0) -> None:
+    """Device-resident product tree; out receives the power-of-two width >= n limbs."""
+    _ensure_init()
+    _check(lib.bgpu_product_tree_device(C.c_void_p(leaves_ptr), n, C.c_void_p(out_ptr), out_cap,
+                                        C.c_void_p(stream or None)), "bgpu_product_tree_device")

@@ -326,3 +326,190 @@ uint32_t batch_plan_launches(const bgpu_batch_plan_s* p) { return p ? p->launche
 size_t batch_plan_classes(const bgpu_batch_plan_s* p) { return p ? p->classes.size() : 0; }
 
 }  // namespace bgpu
+
+// ---- product tree --------------------------------------------------------------
+//
+// The binary-splitting caller pattern (examples/pi.cpp:41-80; config "product
+// tree"): n values multiplied pairwise level by level until one is left, the
+// odd tail carried up unchanged.  Every level keeps its values at one width W
+// (limbs, zero-padded), so a level is one uniform batch: a thread per product
+// for W <= 4, the batched schoolbook kernel while 2W <= 256 limbs, then one
+// NTT class.  Each level is a single set of launches; values stay on the GPU.
+
+namespace bgpu {
+
+template <int W>
+__global__ void k_tree_small(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint32_t m2) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m2) return;
+    const uint64_t* a = in + (size_t)(2 * i) * W;
+    const uint64_t* b = a + W;
+    uint64_t r[2 * W];
+#pragma unroll
+    for (int k = 0; k < 2 * W; ++k) r[k] = 0;
+#pragma unroll
+    for (int x = 0; x < W; ++x) {
+        uint64_t carry = 0;
+#pragma unroll
+        for (int y = 0; y < W; ++y) {
+            const unsigned __int128 t = (unsigned __int128)a[x] * b[y] + r[x + y] + carry;
+            r[x + y] = (uint64_t)t;
+            carry = (uint64_t)(t >> 64);
+        }
+        r[x + W] = carry;
+    }
+    uint64_t* o = out + (size_t)i * 2 * W;
+#pragma unroll
+    for (int k = 0; k < 2 * W; ++k) o[k] = r[k];
+}
+
+// Copy the odd tail value (width W) into slot m2 of the next level (width 2W).
+__global__ void k_tree_tail(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst, uint32_t w) {
+    for (uint32_t k = threadIdx.x; k < 2 * w; k += blockDim.x) dst[k] = k < w ? src[k] : 0;
+}
+
+int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
+                        const EngineHooks& hooks, cudaStream_t st, uint32_t* launches) {
+    if (n == 0) return BGPU_ERR_INVALID_ARG;
+    // Final width: smallest power of two >= n limbs.
+    size_t wfin = 1;
+    while (wfin < n) wfin <<= 1;
+    if (out_cap < wfin) return BGPU_ERR_OUT_CAPACITY;
+    const size_t cap_limbs = 2 * wfin + 16;
+    uint64_t *buf[2] = {nullptr, nullptr};
+    void* scratch = nullptr;
+    void* descs = nullptr;
+    size_t scratch_bytes = 0, desc_bytes = 0;
+    uint32_t nl = 0;
+    auto fail = [&](int rc) {
+        cudaStreamSynchronize(st);
+        cudaFree(buf[0]);
+        cudaFree(buf[1]);
+        cudaFree(scratch);
+        cudaFree(descs);
+        return rc;
+    };
+    if (cudaMalloc(&buf[0], cap_limbs * 8) != cudaSuccess || cudaMalloc(&buf[1], cap_limbs * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BGPU_ERR_OOM);
+    }
+    if (cudaMemcpyAsync(buf[0], d_leaves, n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return fail(BGPU_ERR_CUDA);
+    size_t m = n, w = 1;
+    int cur = 0;
+    std::vector<SchoolDesc> sd;
+    std::vector<ProductDesc> pd;
+    while (m > 1) {
+        const uint32_t m2 = (uint32_t)(m / 2);
+        const uint64_t* in = buf[cur];
+        uint64_t* out = buf[cur ^ 1];
+        cudaError_t e = cudaSuccess;
+        if (w <= 4) {
+            const unsigned blocks = (m2 + 255) / 256;
+            if (w == 1) k_tree_small<1><<<blocks, 256, 0, st>>>(in, out, m2);
+            else if (w == 2) k_tree_small<2><<<blocks, 256, 0, st>>>(in, out, m2);
+            else k_tree_small<4><<<blocks, 256, 0, st>>>(in, out, m2);
+            e = cudaGetLastError();
+            nl += 1;
+        } else if (2 * w <= kSchoolbookMaxLimbs) {
+            sd.resize(m2);
+            for (uint32_t i = 0; i < m2; ++i)
+                sd[i] = SchoolDesc{in + (size_t)2 * i * w, in + (size_t)(2 * i + 1) * w, out + (size_t)2 * i * w,
+                                   (uint32_t)w, (uint32_t)w};
+            const size_t need = m2 * sizeof(SchoolDesc);
+            if (need > desc_bytes) {
+                cudaStreamSynchronize(st);
+                cudaFree(descs);
+                descs = nullptr;
+                if (cudaMalloc(&descs, need) != cudaSuccess) return fail(BGPU_ERR_OOM);
+                desc_bytes = need;
+            }
+            // synchronous copy: the host array is reused by the next level
+            e = cudaMemcpyAsync(descs, sd.data(), need, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) {
+                k_schoolbook_batch<<<m2, kSbThreads, 0, st>>>(static_cast<const SchoolDesc*>(descs));
+                e = cudaGetLastError();
+            }
+            nl += 1;
+        } else {
+            int ln = 0;
+            while (((uint64_t)1 << ln) < 4 * (uint64_t)w - 1) ++ln;
+            if (!shape_supported(ln, false)) return fail(BGPU_ERR_CAPACITY);
+            const size_t nn = (size_t)1 << ln;
+            const size_t per = ntt_scratch_bytes(ln, false);
+            const uint32_t bpp = carry_blocks((uint32_t)(nn / 8));
+            const size_t flag_bytes = al256((size_t)m2 * bpp * 8) + 256;
+            const size_t need_s = m2 * per + flag_bytes;
+            if (need_s > scratch_bytes) {
+                cudaStreamSynchronize(st);
+                cudaFree(scratch);
+                scratch = nullptr;
+                if (cudaMalloc(&scratch, need_s) != cudaSuccess) return fail(BGPU_ERR_OOM);
+                scratch_bytes = need_s;
+            }
+            char* sbase = static_cast<char*>(scratch);
+            uint64_t* flags = reinterpret_cast<uint64_t*>(sbase + m2 * per);
+            unsigned long long* ticket = reinterpret_cast<unsigned long long*>(sbase + m2 * per + al256((size_t)m2 * bpp * 8));
+            const size_t y_bytes = al256(2 * (size_t)kNumPrimes * nn * 4);
+            pd.resize(m2);
+            for (uint32_t i = 0; i < m2; ++i) {
+                char* sc = sbase + (size_t)i * per;
+                ProductDesc& d = pd[i];
+                d.op[0] = OperandDesc{in + (size_t)2 * i * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
+                d.op[1] = OperandDesc{in + (size_t)(2 * i + 1) * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
+                d.y = reinterpret_cast<uint32_t*>(sc);
+                d.chunks = reinterpret_cast<uint64_t*>(sc + y_bytes);
+                d.spill = reinterpret_cast<uint64_t*>(sc + y_bytes + al256(nn / 2 * 8));
+                d.flags = flags + (size_t)i * bpp;
+                d.out = out + (size_t)2 * i * w;
+                d.out_cap = 2 * w;
+            }
+            const size_t need = m2 * sizeof(ProductDesc);
+            if (need > desc_bytes) {
+                cudaStreamSynchronize(st);
+                cudaFree(descs);
+                descs = nullptr;
+                if (cudaMalloc(&descs, need) != cudaSuccess) return fail(BGPU_ERR_OOM);
+                desc_bytes = need;
+            }
+            e = cudaMemcpyAsync(descs, pd.data(), need, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            // fresh carry-scan state for this level: ticket 0, flags 0, epoch 1
+            if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, 8, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, (size_t)m2 * bpp * 8, st);
+            if (e == cudaSuccess) {
+                CarryLaunch cl;
+                cl.ticket_base = 0;
+                cl.epoch = 1;
+                cl.ticket = ticket;
+                cl.err = hooks.err;
+                if (e == cudaSuccess)
+                    e = launch_ntt_batch(kSlotEngine + prime_set_for(ln), hooks.consts[prime_set_for(ln)],
+                                         static_cast<const ProductDesc*>(descs), (int)m2, false, ln,
+                                         kFmtLimb64, cl, st);
+            }
+            nl += kNttLaunches;
+        }
+        if (e == cudaSuccess && (m & 1)) {
+            k_tree_tail<<<1, 256, 0, st>>>(in + (m - 1) * w, out + (size_t)m2 * 2 * w, (uint32_t)w);
+            e = cudaGetLastError();
+            nl += 1;
+        }
+        if (e != cudaSuccess) return fail(BGPU_ERR_CUDA);
+        m = (m + 1) / 2;
+        w *= 2;
+        cur ^= 1;
+    }
+    cudaError_t e = cudaMemcpyAsync(d_out, buf[cur], w * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (launches) *launches = nl;
+    const int rc = e == cudaSuccess ? BGPU_OK : BGPU_ERR_CUDA;
+    cudaFree(buf[0]);
+    cudaFree(buf[1]);
+    cudaFree(scratch);
+    cudaFree(descs);
+    return rc;
+}
+
+}  // namespace bgpu

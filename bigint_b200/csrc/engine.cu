@@ -609,6 +609,59 @@ int bgpu_mul_batch_device(const bgpu_product* products, size_t count, uint32_t f
     return rc;
 }
 
+int bgpu_product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
+                             void* stream) {
+    if (!d_leaves || !d_out || n == 0) return BGPU_ERR_INVALID_ARG;
+    if (n > ((size_t)1 << 26)) return BGPU_ERR_CAPACITY;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    uint32_t nl = 0;
+    int rc = product_tree_device(d_leaves, n, d_out, out_cap, hooks_locked(),
+                                 static_cast<cudaStream_t>(stream), &nl);
+    g.last_launches = nl;
+    if (rc == BGPU_OK) rc = check_device_error(BGPU_OK);
+    return rc;
+}
+
+int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_t out_cap,
+                          size_t* out_len) {
+    if (!leaves || !out_len || n == 0 || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
+    if (n > ((size_t)1 << 26)) return BGPU_ERR_CAPACITY;
+    size_t width = 1;
+    while (width < n) width <<= 1;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    int rc = ensure(&g.d_io, &g.io_bytes, align256(n * 8) + align256(width * 8));
+    if (rc != BGPU_OK) return rc;
+    uint64_t* dl = static_cast<uint64_t*>(g.d_io);
+    uint64_t* dout = reinterpret_cast<uint64_t*>(static_cast<char*>(g.d_io) + align256(n * 8));
+    cudaError_t e = cudaMemcpyAsync(dl, leaves, n * 8, cudaMemcpyHostToDevice, g.stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    uint32_t nl = 0;
+    rc = product_tree_device(dl, n, dout, width, hooks_locked(), g.stream, &nl);
+    g.last_launches = nl;
+    if (rc != BGPU_OK) return rc;
+    std::vector<uint64_t> tmp;
+    uint64_t* dst = out;
+    if (out_cap < width) {
+        tmp.resize(width);
+        dst = tmp.data();
+    }
+    e = cudaMemcpyAsync(dst, dout, width * 8, cudaMemcpyDeviceToHost, g.stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    const size_t len = strip64(dst, width);
+    *out_len = len;
+    if (dst != out) {
+        if (len > out_cap) return BGPU_ERR_OUT_CAPACITY;
+        memcpy(out, dst, len * 8);
+    }
+    return BGPU_OK;
+}
+
 int bgpu_set_split(uint32_t log2_points, uint32_t log2_column) {
     std::lock_guard<std::mutex> lk(g_mu);
     return set_split((int)log2_points, (int)log2_column) == 0 ? BGPU_OK : BGPU_ERR_INVALID_ARG;

@@ -161,6 +161,10 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
 int batch_plan_run(bgpu_batch_plan_s* p, cudaStream_t st);
 void batch_plan_destroy(bgpu_batch_plan_s* p);
 uint32_t batch_plan_launches(const bgpu_batch_plan_s* p);
+// Pairwise product tree of n single-limb values into d_out (width: the
+// smallest power of two >= n limbs, zero padded); synchronous on `st`.
+int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
+                        const EngineHooks& hooks, cudaStream_t st, uint32_t* launches);
 
 // Schoolbook product for small operands (one CTA); out has na+nb limbs.
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,

@@ -149,6 +149,17 @@ uint32_t bgpu_batch_plan_launches(bgpu_batch_plan plan);
 /* One-shot: create, run, synchronize, destroy. */
 int bgpu_mul_batch_device(const bgpu_product* products, size_t count, uint32_t flags, void* stream);
 
+/* Pairwise product tree of n u64 values (the binary-splitting pattern of
+ * examples/pi.cpp:41-80: neighbours multiplied level by level, an odd tail
+ * carried up), each level one set of launches over the whole level; values
+ * stay on the GPU.  The device form writes the product zero padded to
+ * `width` = the smallest power of two >= n limbs (out_cap >= width) and
+ * returns when it is complete; the host form strips leading zeros. */
+int bgpu_product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
+                             void* stream);
+int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_t out_cap,
+                          size_t* out_len);
+
 /* Transform split used for 2^log2_points-point products: the column pass
  * length 2^log2_column (the row pass gets the rest).  Set by the autotuner
  * (bigint_b200/autotune.py); log2_column = 0 restores the built-in choice.
