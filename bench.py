@@ -270,6 +270,197 @@ def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int):
     return reps / el, kind, cores, reps, el
 
 
+# ---- the other configurations, reported beside the headline -----------------------
+
+def _dev_limbs(torch, device, x):
+    return torch.from_numpy(np.ascontiguousarray(x).view(np.int64)).to(device)
+
+
+def _event_ms(torch, stream, fn, reps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for i in range(reps):
+            fn(i)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def sweep_form(bb, torch, device, port):
+    """Config "NTT size sweep": squares at 2^16..2^30 bits, uniform and all-ones
+    limbs, plus the 1:8 and 1:64 unbalanced pairs; device-resident products
+    back to back on one stream (operands smaller than L2 stay cached there)."""
+    stream = torch.cuda.Stream(device)
+    sp = stream.cuda_stream
+    M = (1 << 61) - 1
+    rng = np.random.default_rng(SEED + 2)
+    rows = []
+    cases = [(1 << b, 1 << b, "square") for b in range(16, 31, 2)]
+    cases += [(1 << 24, 1 << 21, "1:8"), (1 << 20, 1 << 14, "1:64")]
+    for abits, bbits, kind in cases:
+        na, nb = abits // 64, bbits // 64
+        for fill in ("uniform", "all-ones"):
+            if fill == "uniform":
+                a = rng.integers(0, 2**64, na, dtype=np.uint64, endpoint=False)
+                a[-1] |= np.uint64(1 << 63)
+                b = a if kind == "square" else rng.integers(0, 2**64, nb, dtype=np.uint64, endpoint=False)
+                if kind != "square":
+                    b[-1] |= np.uint64(1 << 63)
+            else:
+                a = np.full(na, np.uint64(0xFFFFFFFFFFFFFFFF))
+                b = a if kind == "square" else np.full(nb, np.uint64(0xFFFFFFFFFFFFFFFF))
+            da = _dev_limbs(torch, device, a)
+            db = da if kind == "square" else _dev_limbs(torch, device, b)
+            out = torch.empty(na + nb, dtype=torch.int64, device=device)
+
+            def run(i):
+                bb.mul_device(da.data_ptr(), na, db.data_ptr(), nb, out.data_ptr(), stream=sp,
+                              method=bb.BGPU_METHOD_NTT)
+            reps = 3 if abits >= 1 << 28 else 20
+            run(0)
+            bb.device_status(sp)
+            ms = _event_ms(torch, stream, run, reps)
+            bb.device_status(sp)
+            c = out.cpu().numpy().view(np.uint64)
+            ok = port.mod_m61(a) * port.mod_m61(b) % M == port.mod_m61(c)
+            if not ok:
+                raise SystemExit(f"bench sweep: residue check failed at {abits}x{bbits} {fill}")
+            model = reference_model_bytes(na, nb)
+            rows.append({"a_bits": abits, "b_bits": bbits, "kind": kind, "limbs": fill,
+                         "ms": ms, "products_per_s": 1e3 / ms,
+                         "log2_points": (2 * na + 2 * nb - 2).bit_length(),
+                         "reference_model_frac": model / (ms * 1e-3) / 1e9 / measured_peaks()[0],
+                         "verified": "residue mod 2^61-1"})
+            del da, db, out
+    return rows
+
+
+def fft_form(bb, torch, device, A, B, reps: int):
+    """Config "FP64 FFT vs NTT": the headline workload through the FFT form with
+    bits per point from the worst-case bound and from the average bound;
+    device time of the FFT kernels per product (events inside the host call),
+    fallback counts on the uniform operands and on all-ones operands."""
+    out = {}
+    ones = np.full(A.shape[1], np.uint64(0xFFFFFFFFFFFFFFFF))
+    for name, avg in (("worst_case_bound", False), ("average_bound", True)):
+        ms, errs, fb, bits, lp = [], [], 0, None, None
+        for i in range(reps + 1):
+            _, st = bb.fft_mul(A[i % A.shape[0]], B[i % B.shape[0]], average_bound=avg, stats=True)
+            if i == 0:
+                continue  # warm-up
+            ms.append(st.device_ms)
+            errs.append(st.max_round_err)
+            fb += int(st.fell_back)
+            bits, lp = st.fft_bits, st.log2_points
+        _, sto = bb.fft_mul(ones, average_bound=avg, stats=True)
+        out[name] = {"bits_per_point": bits, "log2_points": lp,
+                     "device_ms": statistics.fmean(ms), "products_per_s": 1e3 / statistics.fmean(ms),
+                     "max_round_err": max(errs), "fallbacks": fb, "products": reps,
+                     "all_ones": {"max_round_err": sto.max_round_err, "fell_back": sto.fell_back,
+                                  "method": "ntt" if sto.fell_back else "fft"}}
+    return out
+
+
+def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
+    """Config "batched uneven": 4096 products, operand lengths log-uniform in
+    [2^10, 2^22] bits, one graph launch per batch vs one plain NTT call per
+    product (same inputs, device resident, > L2 in total)."""
+    rng = np.random.default_rng(SEED + 3)
+    na = np.maximum(1, (np.exp2(rng.uniform(10, 22, nprod)) // 64).astype(np.int64))
+    nb = np.maximum(1, (np.exp2(rng.uniform(10, 22, nprod)) // 64).astype(np.int64))
+    offs_a = np.concatenate([[0], np.cumsum(na)[:-1]])
+    offs_b = np.concatenate([[0], np.cumsum(nb)[:-1]]) + na.sum()
+    big = rng.integers(0, 2**64, int(na.sum() + nb.sum()), dtype=np.uint64, endpoint=False)
+    big[offs_a + na - 1] |= np.uint64(1 << 63)
+    big[offs_b + nb - 1] |= np.uint64(1 << 63)
+    dbig = _dev_limbs(torch, device, big)
+    outn = na + nb
+    offs_o = np.concatenate([[0], np.cumsum(outn)[:-1]])
+    dout = torch.zeros(int(outn.sum()), dtype=torch.int64, device=device)
+    base_in, base_out = dbig.data_ptr(), dout.data_ptr()
+    prods = [(base_in + 8 * int(offs_a[i]), int(na[i]), base_in + 8 * int(offs_b[i]), int(nb[i]),
+              base_out + 8 * int(offs_o[i])) for i in range(nprod)]
+    t_plan = time.perf_counter()
+    plan = bb.BatchPlan(prods)
+    t_plan = time.perf_counter() - t_plan
+    stream = torch.cuda.Stream(device)
+    sp = stream.cuda_stream
+    for _ in range(2):
+        plan.run(sp)
+    bb.device_status(sp)
+    ms_batch = _event_ms(torch, stream, lambda i: plan.run(sp), runs)
+    bb.device_status(sp)
+    host = dout.cpu().numpy().view(np.uint64)
+    M = (1 << 61) - 1
+    for i in range(nprod):
+        a = big[offs_a[i]:offs_a[i] + na[i]]
+        b = big[offs_b[i]:offs_b[i] + nb[i]]
+        c = host[offs_o[i]:offs_o[i] + outn[i]]
+        if port.mod_m61(a) * port.mod_m61(b) % M != port.mod_m61(c):
+            raise SystemExit(f"bench batched: product {i} failed the residue check")
+
+    def one_by_one(_):
+        for i in range(nprod):
+            a_ptr, n_a, b_ptr, n_b, o_ptr = prods[i]
+            bb.mul_device(a_ptr, n_a, b_ptr, n_b, o_ptr, stream=sp, method=bb.BGPU_METHOD_NTT)
+    one_by_one(0)
+    bb.device_status(sp)
+    ms_single = _event_ms(torch, stream, one_by_one, 1)
+    bb.device_status(sp)
+    launches = plan.launches
+    plan.close()
+    return {"products": nprod, "operand_bits": "log-uniform [2^10, 2^22]",
+            "batched": {"ms_per_batch": ms_batch, "products_per_s": nprod / (ms_batch * 1e-3),
+                        "launches_per_batch": launches, "graph_launches": 1,
+                        "plan_build_s": t_plan},
+            "one_plain_ntt_launch_per_product": {"ms": ms_single,
+                                                 "products_per_s": nprod / (ms_single * 1e-3),
+                                                 "launches": 4 * nprod},
+            "speedup": ms_single / ms_batch, "verified": "residue mod 2^61-1, every product"}
+
+
+def tree_form(bb, torch, device, port, nleaves: int = 1 << 20, reps: int = 3, cpu: bool = True):
+    """Config "product tree": 2^20 seeded u64 leaves in [2^32, 2^64) multiplied
+    pairwise level by level (each level one set of launches) to one ~2^26-bit
+    product; the reference BigInt tree timed on the host beside it."""
+    rng = np.random.default_rng(SEED + 5)
+    leaves = rng.integers(1 << 32, 2**64, nleaves, dtype=np.uint64, endpoint=False)
+    width = 1 << max(0, (nleaves - 1).bit_length())
+    dl = _dev_limbs(torch, device, leaves)
+    dout = torch.empty(width, dtype=torch.int64, device=device)
+    bb.product_tree_device(dl.data_ptr(), nleaves, dout.data_ptr(), width)
+    times = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bb.product_tree_device(dl.data_ptr(), nleaves, dout.data_ptr(), width)
+        times.append(time.perf_counter() - t0)
+    launches = bb.last_launch_count()
+    got = dout.cpu().numpy().view(np.uint64)
+    M = (1 << 61) - 1
+    r = 1
+    for x in leaves.tolist():
+        r = r * (x % M) % M
+    if port.mod_m61(got) != r:
+        raise SystemExit("bench tree: residue check failed")
+    res = {"leaves": nleaves, "levels": (nleaves - 1).bit_length(), "launches": launches,
+           "ms": 1e3 * statistics.median(times), "products_per_s": (nleaves - 1) / statistics.median(times),
+           "result_bits": int(np.count_nonzero(got) and (len(np.trim_zeros(got, "b")) * 64)),
+           "verified": "residue mod 2^61-1 of the product of all leaves"}
+    if cpu:
+        from oracle.pyoracle import Reference, have_reference
+
+        if have_reference():
+            ref = Reference()
+            ref.init_thread_pool(host_cores())
+            t0 = time.perf_counter()
+            ref.product_tree_digits(leaves)
+            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                    "call": "BigInt::operator* pairwise tree"}
+    return res
+
+
 # ---- arms --------------------------------------------------------------------------
 
 def run_reference_arm(args) -> None:
@@ -420,6 +611,15 @@ def run_gpu_arm(args) -> None:
     if rank != 0:
         return
 
+    forms = None
+    if not args.no_forms:
+        torch.cuda.synchronize(device)
+        forms = {"ntt_size_sweep": sweep_form(bb, torch, device, port),
+                 "fp64_fft": fft_form(bb, torch, device, A, B, reps=10),
+                 "batched_4096": batched_form(bb, torch, device, port),
+                 "product_tree_2p20": tree_form(bb, torch, device, port,
+                                                cpu=(rank == 0 and not args.no_cpu_baseline))}
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, reps, el = cpu_reference_rate(A[0], B[0], args.cpu_seconds, 50,
@@ -452,6 +652,7 @@ def run_gpu_arm(args) -> None:
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches_per_step * args.steps,
+        "forms": forms,
     }
     print(json.dumps(line))
 
@@ -465,6 +666,8 @@ def main(argv=None) -> None:
     ap.add_argument("--bits", type=int, default=OPERAND_BITS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the other configurations (size sweep, FFT form, batch, tree)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -7,6 +7,7 @@
 //   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -242,7 +243,8 @@ size_t strip32(const uint32_t* x, size_t n) {
 // two-pass twiddle and a one-bit margin.  Average mode (BGPU_FFT_AVERAGE_BOUND):
 //   2b <= 50 - L/2 - log2(L + 1),
 // the random-walk growth of the error; products whose measured error exceeds
-// 1/4 are recomputed on the NTT.
+// 1/4 are recomputed on the NTT.  Both modes also keep every coefficient below
+// 2^49 so its rounding distance is meaningful.
 int fft_pick(size_t na, size_t nb, uint32_t flags, int* bits, int* log_n) {
     const int forced = (int)((flags >> 8) & 0x1Fu);
     const bool avg = (flags & BGPU_FFT_AVERAGE_BOUND) != 0;
@@ -254,6 +256,9 @@ int fft_pick(size_t na, size_t nb, uint32_t flags, int* bits, int* log_n) {
         if (!fft_shape_supported(L)) continue;
         const double lim = avg ? 50.0 - L / 2.0 - std::log2(L + 1.0) : 46.0 - L - std::log2(L + 1.0);
         if (!forced && 2.0 * b > lim) continue;
+        // coefficients (< min(npa, npb) * 2^2b) must stay below 2^49, where the
+        // rounding distance can still certify them (doubles are 1/16 apart)
+        if (!forced && 2.0 * b + std::log2((double)std::min(npa, npb)) > 49.0) continue;
         *bits = b;
         *log_n = L;
         return BGPU_OK;
