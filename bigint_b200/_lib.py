@@ -67,7 +67,7 @@ def _load() -> C.CDLL:
     if not os.path.exists(library_path):
         raise ImportError(
             f"bigint_b200: CUDA library not found at {library_path}; build it with "
-            "`python -m bigint_b200.build` (there is no CPU fallback)")
+            "`python bigint_b200/build.py` (there is no CPU fallback)")
     L = C.CDLL(library_path)
     u64p, u32p, szp = C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_size_t)
     L.bgpu_init.argtypes = [C.c_int]

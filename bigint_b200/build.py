@@ -4,7 +4,8 @@ Compiles every ``csrc/*.cu`` for sm_100a with nvcc into one in-tree shared
 library next to this file, with the CUDA runtime linked statically so the
 library needs nothing beyond the driver at run time.
 
-Usage: ``python -m bigint_b200.build`` or ``python bigint_b200/build.py``.
+Usage: ``python bigint_b200/build.py`` (not ``-m``: the package's ``__init__``
+loads the library this recipe builds).
 """
 from __future__ import annotations
 

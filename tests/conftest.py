@@ -15,6 +15,22 @@ if ROOT not in sys.path:
 SEED = 0x9E3779B97F4A7C15  # the reference's regression seed (tests/measure_digit_bits.cpp:140)
 
 
+def load_recipe(relpath: str):
+    """Load a build recipe from its file.  Importing bigint_b200.build through
+    the package would run the package's __init__, which needs the library the
+    recipe builds."""
+    import importlib.util
+
+    name = "_recipe_" + relpath.replace("/", "_").replace(".", "_")
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, relpath))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    sys.modules[name] = mod
+    return mod
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
 

@@ -12,7 +12,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, load_recipe
 
 LIB = os.path.join(ROOT, "bigint_b200", "libbigint_b200.so")
 
@@ -28,9 +28,7 @@ def declared_functions() -> list[str]:
 
 @pytest.fixture(scope="module")
 def lib():
-    from bigint_b200.build import build
-
-    build()
+    load_recipe("bigint_b200/build.py").build()
     import bigint_b200
 
     return bigint_b200.lib
