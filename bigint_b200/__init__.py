@@ -29,6 +29,10 @@ from ._lib import (  # noqa: F401
     BGPU_METHOD_FFT,
     BGPU_METHOD_NTT,
     BGPU_METHOD_SCHOOLBOOK,
+    BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS,
+    BGPU_TUNE_FFT_MAX_LIMBS,
+    BGPU_TUNE_FFT_MIN_LIMBS,
+    BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS,
     BatchPlan,
     BigIntGPUError,
     Stats,
@@ -36,10 +40,12 @@ from ._lib import (  # noqa: F401
     device_status,
     fft_mul,
     get_split,
+    get_tuning,
     init,
     kernel_times,
     last_launch_count,
     lib,
+    load_tuning,
     library_path,
     mul,
     mul_batch_device,
@@ -50,5 +56,6 @@ from ._lib import (  # noqa: F401
     product_tree_device,
     set_split,
     set_kernel_timing,
+    set_tuning,
     shutdown,
 )

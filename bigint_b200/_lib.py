@@ -17,6 +17,11 @@ BGPU_METHOD_NTT = 1
 BGPU_METHOD_SCHOOLBOOK = 2
 BGPU_METHOD_FFT = 3
 BGPU_FFT_AVERAGE_BOUND = 0x10
+BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS = 1
+BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS = 2
+BGPU_TUNE_FFT_MIN_LIMBS = 3
+BGPU_TUNE_FFT_MAX_LIMBS = 4
+DEFAULT_TUNING = os.path.join(_HERE, "tuning_b200.txt")
 
 ERRORS = {
     -1: "BGPU_ERR_INVALID_ARG",
@@ -109,6 +114,12 @@ def _load() -> C.CDLL:
     L.bgpu_set_split.restype = C.c_int
     L.bgpu_get_split.argtypes = [C.c_uint32]
     L.bgpu_get_split.restype = C.c_int
+    L.bgpu_set_tuning.argtypes = [C.c_uint32, C.c_uint64]
+    L.bgpu_set_tuning.restype = C.c_int
+    L.bgpu_get_tuning.argtypes = [C.c_uint32, C.POINTER(C.c_uint64)]
+    L.bgpu_get_tuning.restype = C.c_int
+    L.bgpu_load_tuning.argtypes = [C.c_char_p]
+    L.bgpu_load_tuning.restype = C.c_int
     L.bgpu_set_kernel_timing.argtypes = [C.c_int]
     L.bgpu_set_kernel_timing.restype = C.c_int
     L.bgpu_kernel_times.argtypes = [C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int,
@@ -128,11 +139,48 @@ def _check(rc: int, what: str) -> None:
 
 
 def init(device: int = 0) -> None:
-    """Select the CUDA device and build the twiddle tables (idempotent)."""
+    """Select the CUDA device and build the twiddle tables (idempotent).
+
+    On first use applies a tuning table: the one named by the environment
+    variable BIGINT_B200_TUNING, else the autotuner's table shipped with the
+    package (``tuning_b200.txt``, measured on a B200) when the device is a
+    B200; BIGINT_B200_TUNING set to the empty string keeps the built-in
+    choices."""
     global _initialized_device
     with _init_lock:
+        first = _initialized_device is None
         _check(lib.bgpu_init(int(device)), "bgpu_init")
         _initialized_device = int(device)
+        if first:
+            path = os.environ.get("BIGINT_B200_TUNING")
+            if path is None and os.path.exists(DEFAULT_TUNING) and _device_is_b200():
+                path = DEFAULT_TUNING
+            if path:
+                load_tuning(path)
+
+
+def _device_is_b200() -> bool:
+    try:
+        import torch
+
+        return "B200" in torch.cuda.get_device_name(_initialized_device or 0)
+    except Exception:
+        return False
+
+
+def load_tuning(path: str) -> None:
+    """Apply a tuning table written by ``bigint_b200.autotune`` (bgpu_load_tuning)."""
+    _check(lib.bgpu_load_tuning(os.fsencode(path)), f"bgpu_load_tuning({path})")
+
+
+def set_tuning(key: int, value: int) -> None:
+    _check(lib.bgpu_set_tuning(int(key), int(value)), "bgpu_set_tuning")
+
+
+def get_tuning(key: int) -> int:
+    v = C.c_uint64(0)
+    _check(lib.bgpu_get_tuning(int(key), C.byref(v)), "bgpu_get_tuning")
+    return int(v.value)
 
 
 def shutdown() -> None:

@@ -195,7 +195,7 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
             return BGPU_ERR_INVALID_ARG;
         }
         const bool square = q.a == q.b && q.na == q.nb;
-        if (q.na + q.nb <= kSchoolbookMaxLimbs) {
+        if (q.na + q.nb <= tuning().batch_schoolbook_max_limbs) {
             p->school.push_back(SchoolDesc{q.a, q.b, q.out, (uint32_t)q.na, (uint32_t)q.nb});
             continue;
         }
@@ -411,7 +411,7 @@ int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, siz
             else k_tree_small<4><<<blocks, 256, 0, st>>>(in, out, m2);
             e = cudaGetLastError();
             nl += 1;
-        } else if (2 * w <= kSchoolbookMaxLimbs) {
+        } else if (2 * w <= tuning().batch_schoolbook_max_limbs) {
             sd.resize(m2);
             for (uint32_t i = 0; i < m2; ++i)
                 sd[i] = SchoolDesc{in + (size_t)2 * i * w, in + (size_t)(2 * i + 1) * w, out + (size_t)2 * i * w,

@@ -51,6 +51,7 @@ constexpr uint64_t kTimingRing = 1024;  // products whose kernel times are kept
 
 Engine g;
 std::mutex g_mu;
+Tuning g_tuning;
 
 int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return BGPU_OK;
@@ -206,7 +207,14 @@ bool use_schoolbook(uint32_t flags, size_t na, size_t nb) {
     const uint32_t m = flags & BGPU_METHOD_MASK;
     if (m == BGPU_METHOD_SCHOOLBOOK) return true;
     if (m == BGPU_METHOD_NTT || m == BGPU_METHOD_FFT) return false;
-    return na + nb <= kSchoolbookMaxLimbs;
+    return na + nb <= tuning().schoolbook_max_limbs;
+}
+
+// AUTO picks the FFT form only inside the tuned limb range.
+bool auto_fft(uint32_t flags, size_t na, size_t nb) {
+    if ((flags & BGPU_METHOD_MASK) != BGPU_METHOD_AUTO) return false;
+    const Tuning& t = tuning();
+    return t.fft_max_limbs != 0 && na + nb >= t.fft_min_limbs && na + nb <= t.fft_max_limbs;
 }
 
 constexpr double kFftMaxErr = 0.25;  // larger rounding distances are recomputed on the NTT
@@ -218,8 +226,13 @@ int check_device_error(int rc) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
     if (e != cudaSuccess) return cuda_status(e);
     if (err) {
+        // Clear the error and restart the carry-scan tickets from zero, so a
+        // launch that failed part-way cannot leave the counter and the host's
+        // ticket base out of step for the next product.
         cudaMemsetAsync(g.d_err, 0, sizeof(uint32_t), g.stream);
+        cudaMemsetAsync(g.d_ticket, 0, sizeof(unsigned long long), g.stream);
         cudaStreamSynchronize(g.stream);
+        g.ticket_base = 0;
         return BGPU_ERR_DEVICE_TIMEOUT;
     }
     return BGPU_OK;
@@ -331,7 +344,7 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
     if (e != cudaSuccess) return cuda_status(e);
     if (stats) cudaEventRecord(g.ev0, st);
     int fbits = 0, flog = 0;
-    const bool want_fft = (flags & BGPU_METHOD_MASK) == BGPU_METHOD_FFT &&
+    const bool want_fft = ((flags & BGPU_METHOD_MASK) == BGPU_METHOD_FFT || auto_fft(flags, na, nb)) &&
                           fft_pick(na, nb, flags, &fbits, &flog) == BGPU_OK;
     if (want_fft) {
         double err = 0;
@@ -483,6 +496,9 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
 }
 
 }  // namespace
+
+Tuning& tuning() { return g_tuning; }
+
 }  // namespace bgpu
 
 using namespace bgpu;
@@ -675,6 +691,84 @@ int bgpu_set_split(uint32_t log2_points, uint32_t log2_column) {
 int bgpu_get_split(uint32_t log2_points) {
     if (log2_points < 5 || log2_points > kMaxLogN) return BGPU_ERR_INVALID_ARG;
     return choose_shape((int)log2_points).log_n2;
+}
+
+int bgpu_set_tuning(uint32_t key, uint64_t value) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Tuning& t = g_tuning;
+    switch (key) {
+        case BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS:
+            if (value > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+            t.schoolbook_max_limbs = (uint32_t)value;
+            return BGPU_OK;
+        case BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS:
+            if (value > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+            t.batch_schoolbook_max_limbs = (uint32_t)value;
+            return BGPU_OK;
+        case BGPU_TUNE_FFT_MIN_LIMBS: t.fft_min_limbs = value; return BGPU_OK;
+        case BGPU_TUNE_FFT_MAX_LIMBS: t.fft_max_limbs = value; return BGPU_OK;
+        default: return BGPU_ERR_INVALID_ARG;
+    }
+}
+
+int bgpu_get_tuning(uint32_t key, uint64_t* value) {
+    if (!value) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    const Tuning& t = g_tuning;
+    switch (key) {
+        case BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS: *value = t.schoolbook_max_limbs; return BGPU_OK;
+        case BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS: *value = t.batch_schoolbook_max_limbs; return BGPU_OK;
+        case BGPU_TUNE_FFT_MIN_LIMBS: *value = t.fft_min_limbs; return BGPU_OK;
+        case BGPU_TUNE_FFT_MAX_LIMBS: *value = t.fft_max_limbs; return BGPU_OK;
+        default: return BGPU_ERR_INVALID_ARG;
+    }
+}
+
+int bgpu_load_tuning(const char* path) {
+    if (!path) return BGPU_ERR_INVALID_ARG;
+    FILE* f = fopen(path, "r");
+    if (!f) return BGPU_ERR_INVALID_ARG;
+    // Parse everything first, apply only a fully valid table.
+    struct Split { unsigned ln, l2; };
+    std::vector<Split> splits;
+    std::vector<std::pair<uint32_t, unsigned long long>> vals;
+    char line[256];
+    int rc = BGPU_OK;
+    while (rc == BGPU_OK && fgets(line, sizeof line, f)) {
+        char key[64];
+        unsigned long long a = 0, b = 0;
+        const char* p = line;
+        while (*p == ' ' || *p == '\t') ++p;
+        if (*p == '#' || *p == '\n' || *p == '\0') continue;
+        const int n = sscanf(p, "%63s %llu %llu", key, &a, &b);
+        if (n >= 3 && strcmp(key, "split") == 0) {
+            splits.push_back({(unsigned)a, (unsigned)b});
+        } else if (n == 2 && strcmp(key, "schoolbook_max_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS, a});
+        } else if (n == 2 && strcmp(key, "batch_schoolbook_max_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, a});
+        } else if (n == 2 && strcmp(key, "fft_min_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_FFT_MIN_LIMBS, a});
+        } else if (n == 2 && strcmp(key, "fft_max_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_FFT_MAX_LIMBS, a});
+        } else {
+            rc = BGPU_ERR_INVALID_ARG;
+        }
+    }
+    fclose(f);
+    if (rc != BGPU_OK) return rc;
+    for (const Split& sp : splits) {
+        const int l1 = (int)sp.ln - (int)sp.l2;
+        if (sp.ln < 5 || sp.ln > (unsigned)kMaxLogN || sp.l2 < 2 || sp.l2 > 11 || l1 < 3 || l1 > 15)
+            return BGPU_ERR_INVALID_ARG;
+    }
+    for (auto& kv : vals)
+        if ((kv.first == BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS || kv.first == BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS) &&
+            kv.second > kSchoolbookMaxLimbs)
+            return BGPU_ERR_INVALID_ARG;
+    for (const Split& sp : splits) bgpu_set_split(sp.ln, sp.l2);
+    for (auto& kv : vals) bgpu_set_tuning(kv.first, kv.second);
+    return BGPU_OK;
 }
 
 int bgpu_set_kernel_timing(int on) {

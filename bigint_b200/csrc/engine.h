@@ -20,6 +20,7 @@ enum DigitFormat : int {
 struct NttConsts {
     PrimeInfo pr[kNumPrimes];
     uint32_t one_w[kNumPrimes], one_wp[kNumPrimes];  // Montgomery form of 1 (reduces any u32 mod p)
+    uint32_t red[kNumPrimes];  // floor(2^32 / p): Shoup form of 1, reduces any u32 into [0, 2p)
     const uint2* stage[kNumPrimes][2];  // [prime][dir] Shoup pairs: entry h+m = omega_{2h}^{+-m}
     const uint2* th[kNumPrimes][2];     // Montgomery pairs: omega_{2^log_max}^{+-(i << split)}
     const uint2* tl[kNumPrimes][2];     // Montgomery pairs: omega_{2^log_max}^{+-i}
@@ -170,6 +171,16 @@ int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, siz
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
                               uint64_t* out, cudaStream_t stream);
 constexpr uint32_t kSchoolbookMaxLimbs = 256;  // na + nb
+
+// Method crossovers, set by the autotuner through bgpu_set_tuning /
+// bgpu_load_tuning (defaults below are the built-in choice).
+struct Tuning {
+    uint32_t schoolbook_max_limbs = kSchoolbookMaxLimbs;        // AUTO single products
+    uint32_t batch_schoolbook_max_limbs = kSchoolbookMaxLimbs;  // batch plans and product-tree levels
+    uint64_t fft_min_limbs = 0, fft_max_limbs = 0;              // AUTO host API: FFT form for na+nb in
+                                                                // [min, max]; max 0 = never
+};
+Tuning& tuning();
 
 // Digit-format conversion kernels (used around the schoolbook path).
 cudaError_t launch_digits28_to_limbs(const uint32_t* d, uint32_t nd, uint64_t* limbs,

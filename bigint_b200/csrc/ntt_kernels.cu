@@ -29,6 +29,15 @@
 
 namespace bgpu {
 
+// Row-pass CTAs of rows up to 2^11 points are capped at 48 registers a thread
+// (1280 threads' worth per SM): the pass then fits one more CTA per SM, which
+// shortens the hand-over from the column pass under programmatic dependent
+// launch (measured at 2^20 points: the isolated kernel time is unchanged, the
+// product 7 us shorter).  Longer rows need more registers and keep the default.
+__host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
+    return (l1 <= 11 && threads >= 64) ? 1280 / threads : 1;
+}
+
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
 
 __constant__ NttConsts c_consts[kConstSlots];
@@ -184,8 +193,10 @@ struct FwdColsArgs {
     int nops, log_n, log_n1, slot;
 };
 
-__device__ __forceinline__ const ProductDesc& product(const ProductDesc* descs, const ProductDesc& one,
-                                                      uint32_t p) {
+// Returned by value: binding a reference to the kernel parameter would force
+// a copy of it into local memory.
+__device__ __forceinline__ ProductDesc product(const ProductDesc* descs, const ProductDesc& one,
+                                              uint32_t p) {
     return descs ? descs[p] : one;
 }
 
@@ -197,30 +208,32 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     constexpr int NR = P2::nr;
     const NttConsts& c = c_consts[a.slot];
     const int q = blockIdx.y, opi = blockIdx.z % a.nops;
-    const ProductDesc& pd = product(a.descs, a.one, blockIdx.z / a.nops);
+    const ProductDesc pd = product(a.descs, a.one, blockIdx.z / a.nops);
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
     const OperandDesc in = opi == 0 ? pd.op[0] : pd.op[1];
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     uint32_t* y = pd.y + ((size_t)opi * kNumPrimes + q) * nn;
-    const uint32_t one_w = c.one_w[q], one_wp = c.one_wp[q];
+    const uint32_t red = c.red[q];
 
     // The last round's groups hold slots base + j (LO = 0) of one column n1;
     // k2 = bitrev(base) + bitrev_RL(j) << (L2-RL), so the inter-pass twiddle
     // omega_N^(n1*k2) = B(group) * S_col^bitrev_RL(j).  sS[col][m] holds the
-    // column powers S_col^m = omega_N^(n1 * m << (L2-RL)).
+    // column powers S_col^m = omega_N^(n1 * m << (L2-RL)).  Rows are padded to
+    // 2^RL + 1 entries so the 8 columns a warp reads at one m sit in distinct
+    // banks (an unpadded 2^RL-entry row puts all of them in one bank).
     constexpr int RL = P2::r(NR - 1);
+    constexpr int SROW = (1 << RL) + 1;
     uint2* sS = reinterpret_cast<uint2*>(sm + (kCols << L2));
     for (int t = threadIdx.x; t < (kCols << RL); t += T) {
         const uint32_t col = (uint32_t)t >> RL, m = (uint32_t)t & ((1u << RL) - 1u);
         const uint32_t e = (((c0 + col) * m) << (L2 - RL)) & (uint32_t)(nn - 1);
         const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p);
-        sS[t] = make_uint2(w, w * pinv);
+        sS[col * SROW + m] = make_uint2(w, w * pinv);
     }
     if constexpr (NR == 1) __syncthreads();
     pdl_wait();
-    pdl_trigger();
 
     // Round 0: rows n2 = base + (j << LO) read from the caller's digits.
     {
@@ -237,8 +250,11 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
                 any |= v[j];
             }
 #pragma unroll
-            for (int j = 0; j < (1 << R); ++j)
-                x[j] = LAZY ? mont_lazy(v[j], one_w, one_wp, p) : mont_mul_pre(v[j], one_w, one_wp, p);
+            for (int j = 0; j < (1 << R); ++j) {
+                // v - floor(v * red / 2^32) * p lies in [0, 2p) for any 32-bit v
+                const uint32_t r = v[j] - __umulhi(v[j], red) * p;
+                x[j] = LAZY ? r : csub(r, p);
+            }
             if (any) {
                 dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
             } else {
@@ -250,7 +266,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
                 const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & (uint32_t)(nn - 1),
                                                   a.log_n, p);
                 const uint32_t bwp = bw * pinv;
-                const uint2* srow = sS + (gr.col << RL);
+                const uint2* srow = sS + gr.col * SROW;
 #pragma unroll
                 for (int j = 0; j < (1 << R); ++j)
                     y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
@@ -277,12 +293,15 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
             const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & (uint32_t)(nn - 1),
                                               a.log_n, p);
             const uint32_t bwp = bw * pinv;
-            const uint2* srow = sS + (gr.col << RL);
+            const uint2* srow = sS + gr.col * SROW;
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j)
                 y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
         }
     }
+    // Let the row pass launch only once this CTA's work is done: an early
+    // trigger parks row-pass CTAs on SMs the column pass still fills.
+    pdl_trigger();
 }
 
 // ---- kernel 2: middle row pass ----------------------------------------------
@@ -375,7 +394,7 @@ __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, co
 }
 
 template <int PS, int L1, int T, bool SQR>
-__global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
+__global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const MidRowsArgs a) {
     constexpr bool LAZY = PS == 0;
     extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1])
     using P1 = Plan<L1>;
@@ -384,7 +403,7 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
     uint32_t* sa = sm;
     uint32_t* sb = sm + (1u << L1);
     const int q = blockIdx.y % kNumPrimes;
-    const ProductDesc& pd = product(a.descs, a.one, blockIdx.y / kNumPrimes);
+    const ProductDesc pd = product(a.descs, a.one, blockIdx.y / kNumPrimes);
     const uint32_t slot = blockIdx.x;
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* twf = c.stage[q][0];
@@ -406,7 +425,6 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
     }
     __syncthreads();
     pdl_wait();
-    pdl_trigger();
 
     if constexpr (NR == 1) {
         if constexpr (!SQR) {
@@ -450,6 +468,7 @@ __global__ void __launch_bounds__(T) k_mid_rows(const MidRowsArgs a) {
             for (int j = 0; j < (1 << R); ++j) row_a[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
         }
     }
+    pdl_trigger();  // late, as in the column pass
 }
 
 // ---- kernel 3: inverse column pass + CRT + chunk sums -------------------------
@@ -493,7 +512,7 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     const int q = threadIdx.x / TP, tq = threadIdx.x % TP;
-    const ProductDesc& pd = product(a.descs, a.one, blockIdx.y);
+    const ProductDesc pd = product(a.descs, a.one, blockIdx.y);
     uint32_t* s = sm + q * TILE;
     const uint32_t p = c.pr[q].p;
     const uint2* twi = c.stage[q][1];
@@ -604,9 +623,14 @@ __device__ __forceinline__ uint64_t make_flag(uint64_t epoch, uint32_t status, u
 // Carry resolution over chunks of 8 coefficients.  Chunk c's final value is
 // (D_c + spill_{c-1} + carry_c) mod 2^256 with carry_{c+1} = G_c | (P_c & carry_c),
 // G_c = "D_c + spill_{c-1} >= 2^256", P_c = "D_c + spill_{c-1} == 2^256 - 1".
-// Each thread owns kCarryPer consecutive chunks and folds their (G, P); the
-// threads' pairs are scanned by warp ballots, a fold over warps, and a
-// decoupled look-back over blocks taken in ticket order.
+// A block covers kCarryThreads * kCarryPer consecutive chunks; warp w of the
+// block owns 32 * kCarryPer of them as kCarryPer segments of 32, lane l
+// holding chunk (segment base + l), so every load and store of a segment is
+// one contiguous run over the warp.  All loads are issued before any carry
+// logic (one memory round trip).  Carries inside a segment come from one
+// 64-bit add of the (G, P) ballots; segments are chained inside the warp,
+// warps by a fold in shared memory, and blocks by a decoupled look-back in
+// ticket order.
 __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     __shared__ uint32_t s_bid, s_cin;
     __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
@@ -614,37 +638,48 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     __syncthreads();
     pdl_wait();
     pdl_trigger();
+    // A ticket outside this launch means the host's ticket base and the
+    // counter disagree (an earlier launch that never ran): report, touch nothing.
+    if (s_bid >= gridDim.x) {
+        if (threadIdx.x == 0) atomicOr(a.err, 2u);
+        return;
+    }
     // tickets enumerate (product, block) in order, so a block's predecessor
     // within its product always holds a smaller ticket
-    const ProductDesc& pd = product(a.descs, a.one, s_bid / a.bpp);
+    const ProductDesc pd = product(a.descs, a.one, s_bid / a.bpp);
     const uint32_t bid = s_bid % a.bpp;
     const uint64_t* chunks = pd.chunks;
     const uint64_t* spill = pd.spill;
     uint64_t* flags = pd.flags;
     const size_t out_cap = pd.out_cap;
-    const uint32_t c0 = (bid * kCarryThreads + threadIdx.x) * kCarryPer;
     const uint32_t ntot = a.nchunks + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t wbase = (bid * kCarryThreads + (uint32_t)warp * 32) * kCarryPer;
 
-    uint64_t S[kCarryPer][4];
-    uint32_t Gc[kCarryPer], Pc[kCarryPer];
-    uint64_t sp = (c0 > 0 && c0 - 1 < a.nchunks) ? spill[c0 - 1] : 0;
+    // every load first: chunk words and the spill of the chunk before
+    uint64_t S[kCarryPer][4], sp[kCarryPer];
 #pragma unroll
     for (int i = 0; i < kCarryPer; ++i) {
-        const uint32_t cc = c0 + i;
-        S[i][0] = S[i][1] = S[i][2] = S[i][3] = 0;
-        Gc[i] = 0;
-        Pc[i] = 1;  // chunks past the end pass carries through untouched
+        const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
+        if (cc < a.nchunks) {
+            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)cc * 4);
+            const ulonglong2 u = src[0], v = src[1];
+            S[i][0] = u.x, S[i][1] = u.y, S[i][2] = v.x, S[i][3] = v.y;
+        } else {
+            S[i][0] = S[i][1] = S[i][2] = S[i][3] = 0;
+        }
+        sp[i] = (cc >= 1 && cc - 1 < a.nchunks) ? spill[cc - 1] : 0;
+    }
+    // per-chunk (G, P) and per-segment ballots
+    uint32_t gm[kCarryPer], bm[kCarryPer];
+    uint32_t G = 0, P = 1;  // warp aggregate over its segments
+#pragma unroll
+    for (int i = 0; i < kCarryPer; ++i) {
+        const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
+        uint32_t g = 0, pbit = 1;  // chunks past the end pass carries through untouched
         if (cc < ntot) {
-            uint64_t nsp = 0;
-            if (cc < a.nchunks) {
-                const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)cc * 4);
-                const ulonglong2 u = src[0], v = src[1];
-                S[i][0] = u.x, S[i][1] = u.y, S[i][2] = v.x, S[i][3] = v.y;
-                nsp = spill[cc];
-            }
-            uint64_t t = S[i][0] + sp;
-            uint32_t cy = t < sp;
+            uint64_t t = S[i][0] + sp[i];
+            uint32_t cy = t < sp[i];
             S[i][0] = t;
 #pragma unroll
             for (int k = 1; k < 4; ++k) {
@@ -652,23 +687,20 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
                 cy = cy & (t == 0);
                 S[i][k] = t;
             }
-            Gc[i] = cy;
-            Pc[i] = (!cy) && ((S[i][0] & S[i][1] & S[i][2] & S[i][3]) == ~0ull);
-            sp = nsp;
+            g = cy;
+            pbit = (!cy) && ((S[i][0] & S[i][1] & S[i][2] & S[i][3]) == ~0ull);
         }
+        const uint32_t gmi = __ballot_sync(0xffffffffu, g);
+        const uint32_t pmi = __ballot_sync(0xffffffffu, pbit);
+        gm[i] = gmi;
+        bm[i] = gmi | pmi;
+        const uint32_t segG = (uint32_t)((((uint64_t)gmi + bm[i]) >> 32) & 1u);
+        G = segG | ((pmi == 0xffffffffu) & G);
+        P = P & (pmi == 0xffffffffu);
     }
-    uint32_t G = 0, P = 1;
-#pragma unroll
-    for (int i = 0; i < kCarryPer; ++i) {
-        G = Gc[i] | (Pc[i] & G);
-        P = P & Pc[i];
-    }
-    const uint32_t gm = __ballot_sync(0xffffffffu, G);
-    const uint32_t pm = __ballot_sync(0xffffffffu, P);
-    const uint32_t bm = gm | pm;
     if (lane == 0) {
-        s_wg[warp] = (uint32_t)((((uint64_t)gm + bm) >> 32) & 1u);
-        s_wp[warp] = (pm == 0xffffffffu);
+        s_wg[warp] = G;
+        s_wp[warp] = P;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -719,15 +751,17 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         s_cin = cin;
     }
     __syncthreads();
-    uint32_t cw = s_cin;
+    uint32_t cw = s_cin;  // carry into this warp's first segment
     for (int w = 0; w < warp; ++w) cw = s_wg[w] | (s_wp[w] & cw);
-    const uint64_t sum = (uint64_t)gm + bm + cw;
-    const uint32_t carries = (uint32_t)sum ^ gm ^ bm;
-    uint32_t cin = (carries >> lane) & 1u;
-    if (c0 >= ntot) return;
+    uint32_t cout[kCarryPer];  // carry out of each of this lane's chunks
 #pragma unroll
     for (int i = 0; i < kCarryPer; ++i) {
-        const uint32_t nxt = Gc[i] | (Pc[i] & cin);
+        const uint64_t sum = (uint64_t)gm[i] + bm[i] + cw;
+        const uint32_t carries = (uint32_t)sum ^ gm[i] ^ bm[i];
+        const uint32_t cin = (carries >> lane) & 1u;
+        // carry out of lane l is the carry into lane l+1 (bit 32 for lane 31)
+        cout[i] = lane == 31 ? (uint32_t)(sum >> 32) & 1u : (carries >> (lane + 1)) & 1u;
+        cw = (uint32_t)(sum >> 32) & 1u;
         uint32_t cy = cin;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -735,48 +769,55 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
             cy = cy & (t == 0);
             S[i][k] = t;
         }
-        cin = nxt;  // carry into chunk c0 + i + 1
     }
-    const uint32_t nvalid = min((uint32_t)kCarryPer, ntot - c0);
     if (a.out_fmt == kFmtLimb64) {
         uint64_t* o = static_cast<uint64_t*>(pd.out);
 #pragma unroll
         for (int i = 0; i < kCarryPer; ++i) {
-            const size_t base = (size_t)(c0 + i) * 4;
-            if ((uint32_t)i < nvalid) {
+            const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
+            if (cc >= ntot) continue;
+            const size_t base = (size_t)cc * 4;
+            if (base + 4 <= out_cap) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) o[base + k] = S[i][k];
+            } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
                     if (base + k < out_cap) o[base + k] = S[i][k];
             }
         }
     } else {
-        // 28-bit digits starting in this thread's chunks; the last one may
-        // reach into chunk c0+kCarryPer, whose final low limb is its raw limb
-        // plus the spill and carry this thread passes on.
-        uint64_t nl = 0;
-        if (c0 + kCarryPer < a.nchunks) nl = chunks[(size_t)(c0 + kCarryPer) * 4];
-        nl += sp + cin;
+        // 28-bit digits starting in each chunk; the last one may reach into
+        // chunk cc+1, whose final low limb is its raw limb plus this chunk's
+        // spill plus the carry out of this chunk (mod 2^64 suffices).
         uint32_t* o = static_cast<uint32_t*>(pd.out);
-        const uint64_t bit0 = (uint64_t)c0 * 256;
-        uint64_t k = (bit0 + 27) / 28;
-        const uint64_t kend = min(((uint64_t)(c0 + nvalid) * 256 + 27) / 28, (uint64_t)out_cap);
-        const uint32_t off0 = (uint32_t)(k * 28 - bit0);  // < 28
-        uint64_t cur = S[0][0] >> off0;
-        int have = 64 - (int)off0;
         const uint64_t mask = (1u << 28) - 1u;
 #pragma unroll
-        for (int w = 1; w <= kCarryPer * 4; ++w) {
-            const uint64_t nxtw = (w < kCarryPer * 4) ? S[w / 4][w % 4] : nl;
-            while (have >= 28) {
-                if (k < kend) o[k] = (uint32_t)(cur & mask);
+        for (int i = 0; i < kCarryPer; ++i) {
+            const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
+            if (cc >= ntot) continue;
+            uint64_t nl = (cc + 1 < a.nchunks) ? chunks[(size_t)(cc + 1) * 4] : 0;
+            nl += (cc < a.nchunks ? spill[cc] : 0) + cout[i];
+            const uint64_t bit0 = (uint64_t)cc * 256;
+            uint64_t k = (bit0 + 27) / 28;
+            const uint64_t kend = min((bit0 + 256 + 27) / 28, (uint64_t)out_cap);
+            const uint32_t off0 = (uint32_t)(k * 28 - bit0);  // < 28
+            uint64_t cur = S[i][0] >> off0;
+            int have = 64 - (int)off0;
+#pragma unroll
+            for (int w = 1; w <= 4; ++w) {
+                const uint64_t nxtw = w < 4 ? S[i][w] : nl;
+                while (have >= 28) {
+                    if (k < kend) o[k] = (uint32_t)(cur & mask);
+                    ++k;
+                    cur >>= 28;
+                    have -= 28;
+                }
+                if (k < kend) o[k] = (uint32_t)((cur | (nxtw << have)) & mask);
                 ++k;
-                cur >>= 28;
-                have -= 28;
+                cur = nxtw >> (28 - have);
+                have = 36 + have;
             }
-            if (k < kend) o[k] = (uint32_t)((cur | (nxtw << have)) & mask);
-            ++k;
-            cur = nxtw >> (28 - have);
-            have = 36 + have;
         }
     }
 }
@@ -817,7 +858,7 @@ bool shape_supported(int log_n, bool square) {
     return true;
 }
 
-size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 16 * sizeof(uint2); }
+size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 17 * sizeof(uint2); }
 size_t smem_mid_rows(int l1, bool square) {
     return (square ? 1 : 2) * ((size_t)4 << l1) + 16 * sizeof(uint2);
 }

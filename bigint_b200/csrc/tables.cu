@@ -119,6 +119,7 @@ NttConsts make_consts(int ps, int stage_log, const uint2* dev_tables) {
         const uint2 one = mont_pair(1, p);
         c.one_w[q] = one.x;
         c.one_wp[q] = one.y;
+        c.red[q] = (uint32_t)(((uint64_t)1 << 32) / p);
         for (int dir = 0; dir < 2; ++dir) {
             const uint2* base = dev_tables + (size_t)(q * 2 + dir) * blk;
             c.stage[q][dir] = base;

@@ -32,7 +32,8 @@ extern "C" {
 #define BGPU_ERR_CAPACITY -4      /* product beyond the largest supported transform */
 #define BGPU_ERR_OUT_CAPACITY -5  /* caller's output buffer too small; *out_len = needed */
 #define BGPU_ERR_CUDA -6          /* CUDA error during the multiply */
-#define BGPU_ERR_DEVICE_TIMEOUT -7/* a bounded device-side wait gave up (carry look-back) */
+#define BGPU_ERR_DEVICE_TIMEOUT -7/* a bounded device-side wait gave up (carry look-back), or the
+                                     carry scan saw a block ticket outside its launch */
 #define BGPU_ERR_NOT_INIT -8      /* bgpu_init() not called / failed */
 
 /* Method selection (flags & BGPU_METHOD_MASK). */
@@ -168,6 +169,26 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
 int bgpu_set_split(uint32_t log2_points, uint32_t log2_column);
 /* The column length exponent currently used for 2^log2_points points. */
 int bgpu_get_split(uint32_t log2_points);
+
+/* Method crossovers used by BGPU_METHOD_AUTO.  They replace the reference's
+ * fixed dispatch thresholds (_mul, include/bigint/mul.h:208-220: brute up to
+ * 16384 total bits, FFT up to fft::MAX_TOTAL_BITS, NTT above) with values the
+ * autotuner measures on the device. */
+#define BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS 1u       /* single products: schoolbook for na+nb <= v (<= 256) */
+#define BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS 2u /* batch plans and tree levels: same, per product */
+#define BGPU_TUNE_FFT_MIN_LIMBS 3u              /* host API: FFT form for na+nb in [min, max] ... */
+#define BGPU_TUNE_FFT_MAX_LIMBS 4u              /* ... max = 0 disables the FFT form under AUTO */
+int bgpu_set_tuning(uint32_t key, uint64_t value);
+int bgpu_get_tuning(uint32_t key, uint64_t* value);
+
+/* Apply a tuning table written by the autotuner: a text file, one setting
+ * per line ('#' starts a comment):
+ *     split <log2_points> <log2_column>
+ *     schoolbook_max_limbs <n>      batch_schoolbook_max_limbs <n>
+ *     fft_min_limbs <n>             fft_max_limbs <n>
+ * The whole file is checked before anything is applied; an unknown key or an
+ * out-of-range value gives BGPU_ERR_INVALID_ARG and changes nothing. */
+int bgpu_load_tuning(const char* path);
 
 /* Largest product of bgpu_mul_u64_device_noalloc: na + nb u64 limbs. */
 #define BGPU_NOALLOC_MAX_LIMBS 65536u
