@@ -66,7 +66,8 @@ struct TransformShape {
     int log_n2;  // column length (outer passes)
 };
 
-TransformShape choose_shape(int log_n);
+TransformShape choose_shape(int log_n);   // the tuned split (bgpu_set_split), else the built-in one
+TransformShape builtin_shape(int log_n);  // the built-in split only
 int set_split(int log_n, int log_n2);  // 0 on success; log_n2 == 0 restores the default
 bool shape_supported(int log_n, bool square);
 size_t smem_fwd_cols(int log_n2);
@@ -94,12 +95,13 @@ struct CarryLaunch {
 // out: device buffer in `out_fmt` with `out_cap` elements.
 // `slot` selects the constants (kSlotEngine/kSlotNoAlloc + prime_set_for(log_n));
 // `host` is the same constants on the host (for per-call scale factors).
-// `ev` (optional) holds 5 events recorded around the 4 launches.
+// `ev` (optional) holds 5 events recorded around the 4 launches.  `shape`
+// (optional) fixes the split; by default the tuned choice for log_n is used.
 cudaError_t launch_ntt_product(int slot, const NttConsts& host, const OperandDesc& a,
                                const OperandDesc& b, bool square, int log_n,
                                const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
                                const CarryLaunch& cl, cudaStream_t stream,
-                               cudaEvent_t* ev = nullptr);
+                               cudaEvent_t* ev = nullptr, const TransformShape* shape = nullptr);
 constexpr int kNttLaunches = 4;
 extern const char* const kNttKernelNames[kNttLaunches];
 

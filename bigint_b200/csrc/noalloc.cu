@@ -139,8 +139,13 @@ extern "C" int bgpu_mul_u64_device_noalloc(const uint64_t* d_a, size_t na, const
     cl.epoch = 1;
     OperandDesc oa{d_a, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
     OperandDesc ob{d_b, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
+    // The static stage tables cover rows and columns up to 2^kNaStageLog
+    // points, which the built-in split keeps to for every length here; a
+    // tuned split (bgpu_set_split) may not, so it is not used.
+    const TransformShape shape = builtin_shape(log_n);
+    if (shape.log_n1 > kNaStageLog || shape.log_n2 > kNaStageLog) return BGPU_ERR_CAPACITY;
     cudaError_t e = launch_ntt_product(kSlotNoAlloc + kNaSet, s.consts, oa, ob, square, log_n, ps,
-                                       d_out, kFmtLimb64, na + nb, cl, st, nullptr);
+                                       d_out, kFmtLimb64, na + nb, cl, st, nullptr, &shape);
     if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? BGPU_ERR_OOM : BGPU_ERR_CUDA;
     // Synchronous completion: wait for the product and report a bounded
     // device-side wait that gave up (the error word is part of the scratch).

@@ -837,26 +837,35 @@ int set_split(int log_n, int log_n2) {
     return 0;
 }
 
-TransformShape choose_shape(int log_n) {
+TransformShape builtin_shape(int log_n) {
     TransformShape s;
     s.log_n = log_n;
     int l2 = (log_n - 1) / 2;
     if (l2 > 11) l2 = 11;
     if (l2 < 2) l2 = 2;
-    if (log_n >= 0 && log_n <= kMaxLogN && g_split[log_n]) l2 = g_split[log_n];
     s.log_n2 = l2;
     s.log_n1 = log_n - l2;
     return s;
 }
 
-bool shape_supported(int log_n, bool square) {
-    if (log_n < 5 || log_n > kMaxLogN) return false;
-    TransformShape s = choose_shape(log_n);
-    if (s.log_n1 < 3) return false;
-    if (s.log_n1 > 15) return false;
+TransformShape choose_shape(int log_n) {
+    TransformShape s = builtin_shape(log_n);
+    if (log_n >= 0 && log_n <= kMaxLogN && g_split[log_n]) {
+        s.log_n2 = g_split[log_n];
+        s.log_n1 = log_n - s.log_n2;
+    }
+    return s;
+}
+
+static bool shape_ok(const TransformShape& s, bool square) {
+    if (s.log_n < 5 || s.log_n > kMaxLogN) return false;
+    if (s.log_n2 < 2 || s.log_n2 > 11) return false;
+    if (s.log_n1 < 3 || s.log_n1 > 15) return false;
     if (s.log_n1 == 15 && !square) return false;
     return true;
 }
+
+bool shape_supported(int log_n, bool square) { return shape_ok(choose_shape(log_n), square); }
 
 size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 17 * sizeof(uint2); }
 size_t smem_mid_rows(int l1, bool square) {
@@ -953,12 +962,12 @@ static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32
 
 // The four launches of `count` products (descs on the device, or `one`).
 static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDesc* descs,
-                                   const ProductDesc& one, int count, bool square, int log_n,
-                                   int out_fmt, const CarryLaunch& cl, cudaStream_t st,
-                                   cudaEvent_t* ev) {
-    if (!shape_supported(log_n, square) || log_n > c.log_max || count < 1) return cudaErrorInvalidValue;
+                                   const ProductDesc& one, int count, bool square,
+                                   const TransformShape& sh, int out_fmt, const CarryLaunch& cl,
+                                   cudaStream_t st, cudaEvent_t* ev) {
+    const int log_n = sh.log_n;
+    if (!shape_ok(sh, square) || log_n > c.log_max || count < 1) return cudaErrorInvalidValue;
     const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
-    const TransformShape sh = choose_shape(log_n);
     const size_t nn = (size_t)1 << log_n;
     const uint32_t tiles = (1u << sh.log_n1) / kCols;
     if (ev) cudaEventRecord(ev[0], st);
@@ -1026,7 +1035,8 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
 cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& a,
                                const OperandDesc& b, bool square, int log_n,
                                const ProductScratch& s, void* out, int out_fmt, size_t out_cap,
-                               const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev) {
+                               const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev,
+                               const TransformShape* shape) {
     ProductDesc one{};
     one.op[0] = a;
     one.op[1] = square ? a : b;
@@ -1039,14 +1049,26 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& c, const OperandDesc& 
     CarryLaunch c2 = cl;
     c2.ticket = s.ticket;
     c2.err = s.err;
-    return launch_ntt_core(slot, c, nullptr, one, 1, square, log_n, out_fmt, c2, st, ev);
+    return launch_ntt_core(slot, c, nullptr, one, 1, square, shape ? *shape : choose_shape(log_n),
+                           out_fmt, c2, st, ev);
 }
 
 cudaError_t launch_ntt_batch(int slot, const NttConsts& c, const ProductDesc* descs, int count,
                              bool square, int log_n, int out_fmt, const CarryLaunch& cl,
                              cudaStream_t st) {
-    return launch_ntt_core(slot, c, descs, ProductDesc{}, count, square, log_n, out_fmt, cl, st,
-                           nullptr);
+    // Grid y/z limits (65535) cap the products of one launch; larger batches
+    // go in pieces, each piece's carry scan continuing the ticket sequence.
+    constexpr int kPiece = 16384;
+    const uint32_t bpp = carry_blocks((uint32_t)(((size_t)1 << log_n) / kCols));
+    for (int done = 0; done < count; done += kPiece) {
+        const int n = count - done < kPiece ? count - done : kPiece;
+        CarryLaunch piece = cl;
+        piece.ticket_base = cl.ticket_base + (uint64_t)done * bpp;
+        const cudaError_t e = launch_ntt_core(slot, c, descs + done, ProductDesc{}, n, square,
+                                              choose_shape(log_n), out_fmt, piece, st, nullptr);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,
