@@ -9,6 +9,7 @@ this package           reference                                       C-ABI
 ``mul(A, B)``          ``bigint::mul::_mul`` (mul.h:208-220)           ``bgpu_mul_u64``
 ``ntt_mul(A, B)``      ``bigint::mul::ntt::mul`` (ntt_multithread.cpp:444) ``bgpu_mul_u64`` + NTT
 ``brute_mul(A, B)``    ``bigint::mul::brute::mul`` (mul.h:82-102)      ``bgpu_mul_u64`` + schoolbook
+``karatsuba_mul(A, B)`` (none: the reference has no Karatsuba)         ``bgpu_mul_u64`` + Karatsuba
 ``fft_mul(A, B)``      ``bigint::mul::fft::mul`` (fft.cpp:281)         ``bgpu_mul_u64`` + FFT
 ``mul_digits(a, b,``   ``bigint::mul::mul_digits`` (mul.h:223-318)     ``bgpu_mul_digits``
 ``  precision, pos)``
@@ -27,11 +28,14 @@ from ._lib import (  # noqa: F401
     BGPU_FFT_AVERAGE_BOUND,
     BGPU_METHOD_AUTO,
     BGPU_METHOD_FFT,
+    BGPU_METHOD_KARATSUBA,
     BGPU_METHOD_NTT,
     BGPU_METHOD_SCHOOLBOOK,
+    BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS,
     BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS,
     BGPU_TUNE_FFT_MAX_LIMBS,
     BGPU_TUNE_FFT_MIN_LIMBS,
+    BGPU_TUNE_KARATSUBA_MAX_LIMBS,
     BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS,
     BatchPlan,
     BigIntGPUError,
@@ -39,9 +43,11 @@ from ._lib import (  # noqa: F401
     brute_mul,
     device_status,
     fft_mul,
+    get_batch_split,
     get_split,
     get_tuning,
     init,
+    karatsuba_mul,
     kernel_times,
     last_launch_count,
     lib,
@@ -54,6 +60,7 @@ from ._lib import (  # noqa: F401
     ntt_mul,
     product_tree,
     product_tree_device,
+    set_batch_split,
     set_split,
     set_kernel_timing,
     set_tuning,

@@ -16,11 +16,14 @@ BGPU_METHOD_AUTO = 0
 BGPU_METHOD_NTT = 1
 BGPU_METHOD_SCHOOLBOOK = 2
 BGPU_METHOD_FFT = 3
+BGPU_METHOD_KARATSUBA = 4
 BGPU_FFT_AVERAGE_BOUND = 0x10
 BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS = 1
 BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS = 2
 BGPU_TUNE_FFT_MIN_LIMBS = 3
 BGPU_TUNE_FFT_MAX_LIMBS = 4
+BGPU_TUNE_KARATSUBA_MAX_LIMBS = 5
+BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS = 6
 DEFAULT_TUNING = os.path.join(_HERE, "tuning_b200.txt")
 
 ERRORS = {
@@ -114,6 +117,10 @@ def _load() -> C.CDLL:
     L.bgpu_set_split.restype = C.c_int
     L.bgpu_get_split.argtypes = [C.c_uint32]
     L.bgpu_get_split.restype = C.c_int
+    L.bgpu_set_batch_split.argtypes = [C.c_uint32, C.c_uint32]
+    L.bgpu_set_batch_split.restype = C.c_int
+    L.bgpu_get_batch_split.argtypes = [C.c_uint32]
+    L.bgpu_get_batch_split.restype = C.c_int
     L.bgpu_set_tuning.argtypes = [C.c_uint32, C.c_uint64]
     L.bgpu_set_tuning.restype = C.c_int
     L.bgpu_get_tuning.argtypes = [C.c_uint32, C.POINTER(C.c_uint64)]
@@ -256,6 +263,12 @@ def brute_mul(A, B=None, *, stats: bool = False):
     return _mul_u64(A, B, BGPU_METHOD_SCHOOLBOOK, stats)
 
 
+def karatsuba_mul(A, B=None, *, stats: bool = False):
+    """A*B on the Karatsuba kernel (one level over column sums); na, nb <= 256.
+    The reference has no Karatsuba: its small products use brute::mul."""
+    return _mul_u64(A, B, BGPU_METHOD_KARATSUBA, stats)
+
+
 def fft_mul(A, B=None, *, digit_bits: int = 0, average_bound: bool = False, stats: bool = False):
     """A*B through the FP64 complex-FFT form (``fft::mul``, fft.cpp:281).
 
@@ -321,6 +334,18 @@ def last_launch_count() -> int:
 def set_split(log2_points: int, log2_column: int) -> None:
     """Column-pass length 2^log2_column for 2^log2_points-point transforms (0 = default)."""
     _check(lib.bgpu_set_split(int(log2_points), int(log2_column)), "bgpu_set_split")
+
+
+def set_batch_split(log2_points: int, log2_column: int) -> None:
+    """Column-pass length for the NTT classes of batch plans and product trees."""
+    _check(lib.bgpu_set_batch_split(int(log2_points), int(log2_column)), "bgpu_set_batch_split")
+
+
+def get_batch_split(log2_points: int) -> int:
+    r = lib.bgpu_get_batch_split(int(log2_points))
+    if r < 0:
+        _check(r, "bgpu_get_batch_split")
+    return r
 
 
 def get_split(log2_points: int) -> int:

@@ -6,10 +6,13 @@ brute up to 16384 total bits, FFT up to ``fft::MAX_TOTAL_BITS``, NTT above)
 and has one radix-2 transform schedule (src/mul/ntt_multithread.cpp:333-379).
 Here each choice is timed on the device:
 
-* transform split: for every transform length 2^L (L = 10..25) the column
-  length 2^c (row length 2^(L-c)) with the shortest device time per product;
-* schoolbook vs NTT for single products, and for products inside a batch
-  plan (one CTA per schoolbook product vs a batched NTT class);
+* transform split: for every transform length 2^L (L = 12..25) the column
+  length 2^c (row length 2^(L-c)) with the shortest device time per product,
+  and separately (L = 10..22) the one with the highest throughput for the
+  NTT classes of batch plans and product-tree levels;
+* schoolbook vs Karatsuba vs NTT for single products, and for products
+  inside a batch plan (one CTA per schoolbook or Karatsuba product vs a
+  batched NTT class);
 * the FP64 complex-FFT form vs the NTT on the host API: AUTO uses the FFT
   form only in the limb range where it was faster (never, if it never was).
 
@@ -101,6 +104,39 @@ def tune_splits(bb, torch, dev, stream, log_ns, reps_small=40, reps_large=10):
     return res
 
 
+def tune_batch_splits(bb, torch, dev, stream, log_ns):
+    """Best column-length exponent per transform length for the NTT classes of
+    batch plans: throughput of a batch large enough to fill the GPU."""
+    sp = stream.cuda_stream
+    res = {}
+    for ln in log_ns:
+        cands = valid_splits(ln)
+        if not cands:
+            continue
+        n = 1 << (ln - 2)
+        count = int(max(8, min(1024, (1 << 25) >> ln)))
+        rng = np.random.default_rng(100 + ln)
+        A = _rand_dev(torch, dev, rng, (count, n))
+        B = _rand_dev(torch, dev, rng, (count, n))
+        O = torch.empty((count, 2 * n), dtype=torch.int64, device=dev)
+        prods = [(A[i].data_ptr(), n, B[i].data_ptr(), n, O[i].data_ptr()) for i in range(count)]
+        times = {}
+        for l2 in cands:
+            bb.set_batch_split(ln, l2)
+            plan = bb.BatchPlan(prods)
+            times[l2] = _event_ms(torch, stream, lambda i: plan.run(sp), 5, warm=2)
+            bb.device_status(sp)
+            plan.close()
+        bb.set_batch_split(ln, 0)
+        default = bb.get_batch_split(ln)
+        best = min(times, key=times.get)
+        res[ln] = {"best": best, "default": default, "ms": times, "count": count}
+        print(f"batch split 2^{ln} x{count}: best column 2^{best} {times[best] * 1e3:.1f} us "
+              f"(default 2^{default} {times.get(default, float('nan')) * 1e3:.1f} us)", flush=True)
+        del A, B, O
+    return res
+
+
 def _threshold(rows):
     """Largest total limb count up to which the first method won at every
     tested size (rows: [(total_limbs, ms_first, ms_second)] ascending)."""
@@ -113,49 +149,85 @@ def _threshold(rows):
     return best
 
 
-def tune_schoolbook(bb, torch, dev, stream, sizes):
-    """Single products: schoolbook vs NTT, na = nb = s."""
+def _small_thresholds(rows):
+    """rows: [(total_limbs, t_schoolbook, t_karatsuba, t_ntt)] ascending, inf
+    where a method cannot run.  Schoolbook up to the largest total where it
+    beat both others at every size so far; Karatsuba from there up to the
+    largest total where it beat the NTT."""
+    sb = 0
+    for total, t_sb, t_ka, t_nt in rows:
+        if t_sb <= min(t_ka, t_nt):
+            sb = total
+        else:
+            break
+    ka = 0
+    for total, t_sb, t_ka, t_nt in rows:
+        if total <= sb:
+            continue
+        if t_ka <= t_nt:
+            ka = total
+        else:
+            break
+    return sb, ka
+
+
+def tune_small(bb, torch, dev, stream, sizes):
+    """Single products na = nb = s: schoolbook, Karatsuba and NTT."""
     sp = stream.cuda_stream
     rng = np.random.default_rng(7)
     rows = []
+    inf = float("inf")
     for s in sizes:
         A = _rand_dev(torch, dev, rng, (s,))
         B = _rand_dev(torch, dev, rng, (s,))
         O = torch.empty(2 * s, dtype=torch.int64, device=dev)
         t = []
-        for m in (bb.BGPU_METHOD_SCHOOLBOOK, bb.BGPU_METHOD_NTT):
+        for m, ok in ((bb.BGPU_METHOD_SCHOOLBOOK, 2 * s <= 256), (bb.BGPU_METHOD_KARATSUBA, s <= 256),
+                      (bb.BGPU_METHOD_NTT, True)):
+            if not ok:
+                t.append(inf)
+                continue
             t.append(_event_ms(torch, stream, lambda i, m=m: bb.mul_device(
                 A.data_ptr(), s, B.data_ptr(), s, O.data_ptr(), stream=sp, method=m), 50))
             bb.device_status(sp)
-        rows.append((2 * s, t[0], t[1]))
-        print(f"single {s}x{s} limbs: schoolbook {t[0] * 1e3:.1f} us, ntt {t[1] * 1e3:.1f} us", flush=True)
-    return _threshold(rows), rows
+        rows.append((2 * s, *t))
+        print(f"single {s}x{s} limbs: schoolbook {t[0] * 1e3:.1f} us, karatsuba {t[1] * 1e3:.1f} us, "
+              f"ntt {t[2] * 1e3:.1f} us", flush=True)
+    return (*_small_thresholds(rows), rows)
 
 
-def tune_batch_schoolbook(bb, torch, dev, stream, sizes, count=1024):
-    """Batches of `count` products na = nb = s: schoolbook CTAs vs one NTT class."""
+def tune_batch_small(bb, torch, dev, stream, sizes, count=1024):
+    """Batches of `count` products na = nb = s through a batch plan whose
+    crossovers force each method in turn."""
     sp = stream.cuda_stream
     rng = np.random.default_rng(11)
     rows = []
-    saved = bb.get_tuning(bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS)
+    inf = float("inf")
+    keys = (bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, bb.BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS)
+    saved = [bb.get_tuning(k) for k in keys]
     for s in sizes:
         A = _rand_dev(torch, dev, rng, (count, s))
         B = _rand_dev(torch, dev, rng, (count, s))
         O = torch.empty((count, 2 * s), dtype=torch.int64, device=dev)
         prods = [(A[i].data_ptr(), s, B[i].data_ptr(), s, O[i].data_ptr()) for i in range(count)]
         t = []
-        for limit in (2 * s, 0):  # schoolbook for every product, then none
-            bb.set_tuning(bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, limit)
+        for sb_lim, ka_lim, ok in ((2 * s, 0, 2 * s <= 256), (0, 2 * s, s <= 256), (0, 0, True)):
+            if not ok:
+                t.append(inf)
+                continue
+            bb.set_tuning(keys[0], sb_lim)
+            bb.set_tuning(keys[1], ka_lim)
             plan = bb.BatchPlan(prods)
             t.append(_event_ms(torch, stream, lambda i: plan.run(sp), 10))
             bb.device_status(sp)
             plan.close()
-        rows.append((2 * s, t[0], t[1]))
+        rows.append((2 * s, *t))
         print(f"batch {count} x ({s}x{s}) limbs: schoolbook {t[0] * 1e3:.1f} us, "
-              f"ntt {t[1] * 1e3:.1f} us", flush=True)
+              f"karatsuba {t[1] * 1e3:.1f} us, ntt {t[2] * 1e3:.1f} us", flush=True)
         del A, B, O
-    bb.set_tuning(bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, saved)
-    return _threshold(rows), rows
+    for k, v in zip(keys, saved):
+        bb.set_tuning(k, v)
+    return (*_small_thresholds(rows), rows)
 
 
 def tune_fft(bb, log_limbs):
@@ -182,7 +254,9 @@ def tune_fft(bb, log_limbs):
     return (min(wins), max(wins)), rows
 
 
-def write_table(path: str, device: str, splits, sb, sb_rows, bsb, bsb_rows, fft, fft_rows) -> None:
+def write_table(path: str, device: str, splits, bsplits, small, bsmall, fft, fft_rows) -> None:
+    sb, ka, sb_rows = small
+    bsb, bka, bsb_rows = bsmall
     lines = [f"# bigint_b200 tuning table for {device}",
              f"# written by bigint_b200/autotune.py at {datetime.datetime.now(datetime.timezone.utc).isoformat(timespec='seconds')}",
              "# split <log2 points> <log2 column length>   (device us per product: best / built-in)"]
@@ -190,12 +264,20 @@ def write_table(path: str, device: str, splits, sb, sb_rows, bsb, bsb_rows, fft,
         r = splits[ln]
         lines.append(f"split {ln} {r['best']}    # {r['ms'][r['best']] * 1e3:.1f} / "
                      f"{r['ms'].get(r['default'], float('nan')) * 1e3:.1f}")
-    lines.append("# single products: schoolbook vs NTT (us), na + nb limbs")
-    lines += [f"#   {t}: {a * 1e3:.1f} vs {b * 1e3:.1f}" for t, a, b in sb_rows]
+    lines.append("# batch_split <log2 points> <log2 column length>   (us per batch of `count` products:"
+                 " best / built-in)")
+    for ln in sorted(bsplits):
+        r = bsplits[ln]
+        lines.append(f"batch_split {ln} {r['best']}    # x{r['count']}: {r['ms'][r['best']] * 1e3:.1f} / "
+                     f"{r['ms'].get(r['default'], float('nan')) * 1e3:.1f}")
+    lines.append("# single products: schoolbook / Karatsuba / NTT (us), na + nb limbs")
+    lines += [f"#   {t}: {a * 1e3:.1f} / {b * 1e3:.1f} / {c * 1e3:.1f}" for t, a, b, c in sb_rows]
     lines.append(f"schoolbook_max_limbs {sb}")
-    lines.append("# batches of 1024 products: schoolbook vs NTT class (us per batch)")
-    lines += [f"#   {t}: {a * 1e3:.1f} vs {b * 1e3:.1f}" for t, a, b in bsb_rows]
+    lines.append(f"karatsuba_max_limbs {ka}")
+    lines.append("# batches of 1024 products: schoolbook / Karatsuba / NTT class (us per batch)")
+    lines += [f"#   {t}: {a * 1e3:.1f} / {b * 1e3:.1f} / {c * 1e3:.1f}" for t, a, b, c in bsb_rows]
     lines.append(f"batch_schoolbook_max_limbs {bsb}")
+    lines.append(f"batch_karatsuba_max_limbs {bka}")
     lines.append("# FP64 FFT form vs NTT on the host API (device us), na + nb limbs")
     lines += [f"#   {t}: {a * 1e3:.1f} vs {b * 1e3:.1f}" for t, a, b in fft_rows]
     lines.append(f"fft_min_limbs {fft[0]}")
@@ -224,12 +306,15 @@ def main(argv=None) -> int:
     splits = tune_splits(bb, torch, dev, stream, log_ns)
     for ln, r in splits.items():  # later stages measure with the tuned splits
         bb.set_split(ln, r["best"])
-    sizes = [8, 16, 32, 64, 96, 128] if not args.quick else [16, 64, 128]
-    sb, sb_rows = tune_schoolbook(bb, torch, dev, stream, sizes)
-    bsb, bsb_rows = tune_batch_schoolbook(bb, torch, dev, stream, sizes)
+    bsplits = tune_batch_splits(bb, torch, dev, stream, range(10, 23, 3 if args.quick else 1))
+    for ln, r in bsplits.items():
+        bb.set_batch_split(ln, r["best"])
+    sizes = [8, 16, 32, 48, 64, 96, 128, 192, 256, 384] if not args.quick else [16, 64, 128, 256]
+    small = tune_small(bb, torch, dev, stream, sizes)
+    bsmall = tune_batch_small(bb, torch, dev, stream, sizes)
     fft, fft_rows = tune_fft(bb, range(8, 19, 2) if not args.quick else (10, 14))
     name = torch.cuda.get_device_name(dev)
-    write_table(args.out, name, splits, sb, sb_rows, bsb, bsb_rows, fft, fft_rows)
+    write_table(args.out, name, splits, bsplits, small, bsmall, fft, fft_rows)
     print(f"wrote {args.out}")
     return 0
 

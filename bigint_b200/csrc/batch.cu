@@ -24,58 +24,6 @@
 
 namespace bgpu {
 
-// ---- batched schoolbook ------------------------------------------------------
-
-struct SchoolDesc {
-    const uint64_t* a;
-    const uint64_t* b;
-    uint64_t* out;
-    uint32_t na, nb;
-};
-
-constexpr int kSbThreads = 128;
-
-// One CTA per product (na + nb <= kSchoolbookMaxLimbs): thread k owns output
-// columns k, k + 128, ...; column sums are 192-bit, then one carry fold.
-__global__ void __launch_bounds__(kSbThreads) k_schoolbook_batch(const SchoolDesc* descs) {
-    __shared__ uint64_t sa[kSchoolbookMaxLimbs], sb[kSchoolbookMaxLimbs];
-    __shared__ uint64_t c0[kSchoolbookMaxLimbs], c1[kSchoolbookMaxLimbs], c2[kSchoolbookMaxLimbs];
-    const SchoolDesc d = descs[blockIdx.x];
-    for (uint32_t i = threadIdx.x; i < d.na; i += kSbThreads) sa[i] = d.a[i];
-    for (uint32_t i = threadIdx.x; i < d.nb; i += kSbThreads) sb[i] = d.b[i];
-    __syncthreads();
-    const uint32_t ncol = d.na + d.nb;
-    for (uint32_t k = threadIdx.x; k < ncol; k += kSbThreads) {
-        uint64_t x0 = 0, x1 = 0, x2 = 0;
-        if (k + 1 < ncol) {
-            const uint32_t i0 = k + 1 > d.nb ? k + 1 - d.nb : 0;
-            const uint32_t i1 = k < d.na - 1 ? k : d.na - 1;
-            for (uint32_t i = i0; i <= i1; ++i) {
-                const uint64_t u = sa[i], v = sb[k - i];
-                const uint64_t lo = u * v, hi = __umul64hi(u, v);
-                x0 += lo;
-                const uint64_t c = x0 < lo;
-                const uint64_t t = x1 + hi;
-                x2 += (t < x1);
-                x1 = t + c;
-                x2 += (x1 < c);
-            }
-        }
-        c0[k] = x0, c1[k] = x1, c2[k] = x2;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned __int128 carry = 0;
-        for (uint32_t k = 0; k < ncol; ++k) {
-            unsigned __int128 s = carry + c0[k];
-            if (k >= 1) s += c1[k - 1];
-            if (k >= 2) s += c2[k - 2];
-            d.out[k] = (uint64_t)s;
-            carry = s >> 64;
-        }
-    }
-}
-
 // ---- plans -------------------------------------------------------------------
 
 struct BatchClass {
@@ -93,7 +41,8 @@ struct bgpu_batch_plan_s {
     int device = -1;
     size_t count = 0;
     std::vector<bgpu::BatchClass> classes;
-    std::vector<bgpu::SchoolDesc> school;
+    std::vector<bgpu::SchoolDesc> school;  // schoolbook products
+    std::vector<bgpu::SchoolDesc> kara;    // Karatsuba products
     void* d_mem = nullptr;  // descriptors, scratch, flags, tickets
     size_t d_bytes = 0;
     cudaGraph_t graph = nullptr;
@@ -141,7 +90,8 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
         flag_words += c.flags_words;
     }
     const size_t school_off = al256(n_desc * sizeof(ProductDesc));
-    const size_t tick_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
+    const size_t kara_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
+    const size_t tick_off = kara_off + al256(p->kara.size() * sizeof(SchoolDesc));
     unsigned long long* tickets = reinterpret_cast<unsigned long long*>(base + tick_off);
     const size_t flags_base = tick_off + al256(std::max<size_t>(1, p->classes.size()) * 8);
     // Carry-scan state restarts every run: ticket counters and flag words at 0,
@@ -165,10 +115,17 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
         if (e != cudaSuccess) return BGPU_ERR_CUDA;
         launches += kNttLaunches;
     }
+    size_t bi = p->classes.size();
     if (!p->school.empty()) {
         const SchoolDesc* d_school = reinterpret_cast<const SchoolDesc*>(base + school_off);
-        k_schoolbook_batch<<<(unsigned)p->school.size(), kSbThreads, 0, branches.back()>>>(d_school);
-        if (cudaGetLastError() != cudaSuccess) return BGPU_ERR_CUDA;
+        if (launch_schoolbook_batch(d_school, (uint32_t)p->school.size(), branches[bi++]) != cudaSuccess)
+            return BGPU_ERR_CUDA;
+        launches += 1;
+    }
+    if (!p->kara.empty()) {
+        const SchoolDesc* d_kara = reinterpret_cast<const SchoolDesc*>(base + kara_off);
+        if (launch_karatsuba_batch(d_kara, (uint32_t)p->kara.size(), branches[bi++]) != cudaSuccess)
+            return BGPU_ERR_CUDA;
         launches += 1;
     }
     for (size_t i = 0; i < branches.size(); ++i) {
@@ -199,13 +156,17 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
             p->school.push_back(SchoolDesc{q.a, q.b, q.out, (uint32_t)q.na, (uint32_t)q.nb});
             continue;
         }
+        if (q.na + q.nb <= tuning().batch_karatsuba_max_limbs && karatsuba_fits(q.na, q.nb)) {
+            p->kara.push_back(SchoolDesc{q.a, q.b, q.out, (uint32_t)q.na, (uint32_t)q.nb});
+            continue;
+        }
         if (q.na + q.nb > ((size_t)1 << 31)) {
             destroy_plan(p);
             return BGPU_ERR_CAPACITY;
         }
         int ln = ceil_log2(2 * (uint64_t)(q.na + q.nb) - 1);
         if (ln < 5) ln = 5;
-        if (!shape_supported(ln, square)) {
+        if (!shape_supported_batch(ln, square)) {
             destroy_plan(p);
             return BGPU_ERR_CAPACITY;
         }
@@ -219,7 +180,8 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         }
         p->classes[it->second].members.push_back((uint32_t)i);
     }
-    // Layout: [ProductDesc...][SchoolDesc...][tickets][flags][scratch].
+    // Layout: [ProductDesc...][SchoolDesc: schoolbook...][SchoolDesc: Karatsuba...]
+    //         [tickets][flags][scratch].
     size_t n_desc = 0, flag_words = 0, scratch = 0;
     for (auto& c : p->classes) {
         c.desc_off = n_desc;
@@ -231,7 +193,8 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         scratch += c.members.size() * ntt_scratch_bytes(c.log_n, c.square);
     }
     const size_t school_off = al256(n_desc * sizeof(ProductDesc));
-    const size_t tick_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
+    const size_t kara_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
+    const size_t tick_off = kara_off + al256(p->kara.size() * sizeof(SchoolDesc));
     const size_t flags_base = tick_off + al256(std::max<size_t>(1, p->classes.size()) * 8);
     const size_t scratch_base = flags_base + al256(flag_words * 8);
     p->d_bytes = scratch_base + scratch;
@@ -265,12 +228,15 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
     if (e == cudaSuccess && !p->school.empty())
         e = cudaMemcpy(base + school_off, p->school.data(), p->school.size() * sizeof(SchoolDesc),
                        cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !p->kara.empty())
+        e = cudaMemcpy(base + kara_off, p->kara.data(), p->kara.size() * sizeof(SchoolDesc),
+                       cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         destroy_plan(p);
         return BGPU_ERR_CUDA;
     }
     // Capture the whole batch into one graph (streams and events made first).
-    const size_t nbranch = p->classes.size() + (p->school.empty() ? 0 : 1);
+    const size_t nbranch = p->classes.size() + (p->school.empty() ? 0 : 1) + (p->kara.empty() ? 0 : 1);
     std::vector<cudaStream_t> branches(nbranch, nullptr);
     std::vector<cudaEvent_t> joins(nbranch, nullptr);
     cudaStream_t cap = nullptr;
@@ -333,8 +299,9 @@ size_t batch_plan_classes(const bgpu_batch_plan_s* p) { return p ? p->classes.si
 // tree"): n values multiplied pairwise level by level until one is left, the
 // odd tail carried up unchanged.  Every level keeps its values at one width W
 // (limbs, zero-padded), so a level is one uniform batch: a thread per product
-// for W <= 4, the batched schoolbook kernel while 2W <= 256 limbs, then one
-// NTT class.  Each level is a single set of launches; values stay on the GPU.
+// for W <= 4, then the batched schoolbook or Karatsuba kernel while 2W is
+// within their tuned limits, then one NTT class.  Each level is a single set
+// of launches; values stay on the GPU.
 
 namespace bgpu {
 
@@ -368,148 +335,169 @@ __global__ void k_tree_tail(const uint64_t* __restrict__ src, uint64_t* __restri
     for (uint32_t k = threadIdx.x; k < 2 * w; k += blockDim.x) dst[k] = k < w ? src[k] : 0;
 }
 
+namespace {
+
+// One level of the tree: m values of width w become ceil(m/2) of width 2w.
+struct TreeLevel {
+    uint32_t m, m2;
+    size_t w;
+    int kind;  // 0: thread per product (w <= 4), 1: schoolbook, 2: Karatsuba, 3: NTT
+    int log_n = 0;
+    size_t desc_off = 0;  // bytes into the descriptor region
+};
+
+}  // namespace
+
 int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
-                        const EngineHooks& hooks, cudaStream_t st, uint32_t* launches) {
-    if (n == 0) return BGPU_ERR_INVALID_ARG;
+                        const EngineHooks& hooks, TreeArena* arena, cudaStream_t st, uint32_t* launches) {
+    if (n == 0 || !arena) return BGPU_ERR_INVALID_ARG;
     // Final width: smallest power of two >= n limbs.
     size_t wfin = 1;
     while (wfin < n) wfin <<= 1;
     if (out_cap < wfin) return BGPU_ERR_OUT_CAPACITY;
-    const size_t cap_limbs = 2 * wfin + 16;
-    uint64_t *buf[2] = {nullptr, nullptr};
-    void* scratch = nullptr;
-    void* descs = nullptr;
-    size_t scratch_bytes = 0, desc_bytes = 0;
-    uint32_t nl = 0;
-    auto fail = [&](int rc) {
-        cudaStreamSynchronize(st);
-        cudaFree(buf[0]);
-        cudaFree(buf[1]);
-        cudaFree(scratch);
-        cudaFree(descs);
-        return rc;
-    };
-    if (cudaMalloc(&buf[0], cap_limbs * 8) != cudaSuccess || cudaMalloc(&buf[1], cap_limbs * 8) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(BGPU_ERR_OOM);
+    // Plan every level first: method, descriptor space, NTT scratch.
+    const Tuning& tu = tuning();
+    std::vector<TreeLevel> lv;
+    size_t desc_bytes = 0, ntt_bytes = 0, flag_words = 0;
+    for (size_t m = n, w = 1; m > 1; m = (m + 1) / 2, w *= 2) {
+        TreeLevel L;
+        L.m = (uint32_t)m;
+        L.m2 = (uint32_t)(m / 2);
+        L.w = w;
+        if (w <= 4) {
+            L.kind = 0;
+        } else if (2 * w <= tu.batch_schoolbook_max_limbs) {
+            L.kind = 1;
+        } else if (2 * w <= tu.batch_karatsuba_max_limbs && karatsuba_fits(w, w)) {
+            L.kind = 2;
+        } else {
+            L.kind = 3;
+            while (((uint64_t)1 << L.log_n) < 4 * (uint64_t)w - 1) ++L.log_n;
+            if (!shape_supported_batch(L.log_n, false)) return BGPU_ERR_CAPACITY;
+            const size_t nn = (size_t)1 << L.log_n;
+            ntt_bytes = std::max(ntt_bytes, (size_t)L.m2 * ntt_scratch_bytes(L.log_n, false));
+            flag_words = std::max(flag_words, (size_t)L.m2 * carry_blocks((uint32_t)(nn / 8)));
+        }
+        if (L.kind == 1 || L.kind == 2) {
+            L.desc_off = desc_bytes;
+            desc_bytes += al256((size_t)L.m2 * sizeof(SchoolDesc));
+        } else if (L.kind == 3) {
+            L.desc_off = desc_bytes;
+            desc_bytes += al256((size_t)L.m2 * sizeof(ProductDesc));
+        }
+        lv.push_back(L);
     }
-    if (cudaMemcpyAsync(buf[0], d_leaves, n * 8, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return fail(BGPU_ERR_CUDA);
-    size_t m = n, w = 1;
+    // Arena: [value buffer 0][value buffer 1][descriptors][ticket][flags][NTT scratch],
+    // kept by the engine between calls (grow-only).
+    const size_t cap_limbs = 2 * wfin + 16;
+    const size_t buf_bytes = al256(cap_limbs * 8);
+    const size_t off_desc = 2 * buf_bytes;
+    const size_t off_ticket = off_desc + al256(desc_bytes);
+    const size_t off_flags = off_ticket + 256;
+    const size_t off_ntt = off_flags + al256(flag_words * 8);
+    const size_t need = off_ntt + ntt_bytes;
+    if (arena->bytes < need) {
+        cudaStreamSynchronize(st);
+        cudaFree(arena->ptr);
+        arena->ptr = nullptr;
+        arena->bytes = 0;
+        if (cudaMalloc(&arena->ptr, need + need / 4) != cudaSuccess) {
+            cudaGetLastError();
+            return BGPU_ERR_OOM;
+        }
+        arena->bytes = need + need / 4;
+    }
+    char* base = static_cast<char*>(arena->ptr);
+    uint64_t* buf[2] = {reinterpret_cast<uint64_t*>(base), reinterpret_cast<uint64_t*>(base + buf_bytes)};
+    unsigned long long* ticket = reinterpret_cast<unsigned long long*>(base + off_ticket);
+    uint64_t* flags = reinterpret_cast<uint64_t*>(base + off_flags);
+    // Every level's descriptors, built on the host and copied in one go.
+    std::vector<char> hd(desc_bytes);
+    {
+        int cur = 0;
+        for (const TreeLevel& L : lv) {
+            const uint64_t* in = buf[cur];
+            uint64_t* out = buf[cur ^ 1];
+            const size_t w = L.w;
+            if (L.kind == 1 || L.kind == 2) {
+                SchoolDesc* sd = reinterpret_cast<SchoolDesc*>(hd.data() + L.desc_off);
+                for (uint32_t i = 0; i < L.m2; ++i)
+                    sd[i] = SchoolDesc{in + (size_t)2 * i * w, in + (size_t)(2 * i + 1) * w,
+                                       out + (size_t)2 * i * w, (uint32_t)w, (uint32_t)w};
+            } else if (L.kind == 3) {
+                ProductDesc* pd = reinterpret_cast<ProductDesc*>(hd.data() + L.desc_off);
+                const size_t nn = (size_t)1 << L.log_n;
+                const size_t per = ntt_scratch_bytes(L.log_n, false);
+                const uint32_t bpp = carry_blocks((uint32_t)(nn / 8));
+                const size_t y_bytes = al256(2 * (size_t)kNumPrimes * nn * 4);
+                for (uint32_t i = 0; i < L.m2; ++i) {
+                    char* sc = base + off_ntt + (size_t)i * per;
+                    ProductDesc& d = pd[i];
+                    d.op[0] = OperandDesc{in + (size_t)2 * i * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
+                    d.op[1] = OperandDesc{in + (size_t)(2 * i + 1) * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
+                    d.y = reinterpret_cast<uint32_t*>(sc);
+                    d.chunks = reinterpret_cast<uint64_t*>(sc + y_bytes);
+                    d.spill = reinterpret_cast<uint64_t*>(sc + y_bytes + al256(nn / 2 * 8));
+                    d.flags = flags + (size_t)i * bpp;
+                    d.out = out + (size_t)2 * i * w;
+                    d.out_cap = 2 * w;
+                }
+            }
+            cur ^= 1;
+        }
+    }
+    cudaError_t e = cudaMemcpyAsync(buf[0], d_leaves, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && desc_bytes)
+        e = cudaMemcpyAsync(base + off_desc, hd.data(), desc_bytes, cudaMemcpyHostToDevice, st);
+    uint32_t nl = 0;
     int cur = 0;
-    std::vector<SchoolDesc> sd;
-    std::vector<ProductDesc> pd;
-    while (m > 1) {
-        const uint32_t m2 = (uint32_t)(m / 2);
+    for (const TreeLevel& L : lv) {
+        if (e != cudaSuccess) break;
         const uint64_t* in = buf[cur];
         uint64_t* out = buf[cur ^ 1];
-        cudaError_t e = cudaSuccess;
-        if (w <= 4) {
-            const unsigned blocks = (m2 + 255) / 256;
-            if (w == 1) k_tree_small<1><<<blocks, 256, 0, st>>>(in, out, m2);
-            else if (w == 2) k_tree_small<2><<<blocks, 256, 0, st>>>(in, out, m2);
-            else k_tree_small<4><<<blocks, 256, 0, st>>>(in, out, m2);
+        const size_t w = L.w;
+        if (L.kind == 0) {
+            const unsigned blocks = (L.m2 + 255) / 256;
+            if (w == 1) k_tree_small<1><<<blocks, 256, 0, st>>>(in, out, L.m2);
+            else if (w == 2) k_tree_small<2><<<blocks, 256, 0, st>>>(in, out, L.m2);
+            else k_tree_small<4><<<blocks, 256, 0, st>>>(in, out, L.m2);
             e = cudaGetLastError();
             nl += 1;
-        } else if (2 * w <= tuning().batch_schoolbook_max_limbs) {
-            sd.resize(m2);
-            for (uint32_t i = 0; i < m2; ++i)
-                sd[i] = SchoolDesc{in + (size_t)2 * i * w, in + (size_t)(2 * i + 1) * w, out + (size_t)2 * i * w,
-                                   (uint32_t)w, (uint32_t)w};
-            const size_t need = m2 * sizeof(SchoolDesc);
-            if (need > desc_bytes) {
-                cudaStreamSynchronize(st);
-                cudaFree(descs);
-                descs = nullptr;
-                if (cudaMalloc(&descs, need) != cudaSuccess) return fail(BGPU_ERR_OOM);
-                desc_bytes = need;
-            }
-            // synchronous copy: the host array is reused by the next level
-            e = cudaMemcpyAsync(descs, sd.data(), need, cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e == cudaSuccess) {
-                k_schoolbook_batch<<<m2, kSbThreads, 0, st>>>(static_cast<const SchoolDesc*>(descs));
-                e = cudaGetLastError();
-            }
+        } else if (L.kind == 1 || L.kind == 2) {
+            const SchoolDesc* d = reinterpret_cast<const SchoolDesc*>(base + off_desc + L.desc_off);
+            e = L.kind == 2 ? launch_karatsuba_batch(d, L.m2, st) : launch_schoolbook_batch(d, L.m2, st);
             nl += 1;
         } else {
-            int ln = 0;
-            while (((uint64_t)1 << ln) < 4 * (uint64_t)w - 1) ++ln;
-            if (!shape_supported(ln, false)) return fail(BGPU_ERR_CAPACITY);
-            const size_t nn = (size_t)1 << ln;
-            const size_t per = ntt_scratch_bytes(ln, false);
-            const uint32_t bpp = carry_blocks((uint32_t)(nn / 8));
-            const size_t flag_bytes = al256((size_t)m2 * bpp * 8) + 256;
-            const size_t need_s = m2 * per + flag_bytes;
-            if (need_s > scratch_bytes) {
-                cudaStreamSynchronize(st);
-                cudaFree(scratch);
-                scratch = nullptr;
-                if (cudaMalloc(&scratch, need_s) != cudaSuccess) return fail(BGPU_ERR_OOM);
-                scratch_bytes = need_s;
-            }
-            char* sbase = static_cast<char*>(scratch);
-            uint64_t* flags = reinterpret_cast<uint64_t*>(sbase + m2 * per);
-            unsigned long long* ticket = reinterpret_cast<unsigned long long*>(sbase + m2 * per + al256((size_t)m2 * bpp * 8));
-            const size_t y_bytes = al256(2 * (size_t)kNumPrimes * nn * 4);
-            pd.resize(m2);
-            for (uint32_t i = 0; i < m2; ++i) {
-                char* sc = sbase + (size_t)i * per;
-                ProductDesc& d = pd[i];
-                d.op[0] = OperandDesc{in + (size_t)2 * i * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
-                d.op[1] = OperandDesc{in + (size_t)(2 * i + 1) * w, (uint32_t)w, (uint32_t)(2 * w), kFmtLimb64};
-                d.y = reinterpret_cast<uint32_t*>(sc);
-                d.chunks = reinterpret_cast<uint64_t*>(sc + y_bytes);
-                d.spill = reinterpret_cast<uint64_t*>(sc + y_bytes + al256(nn / 2 * 8));
-                d.flags = flags + (size_t)i * bpp;
-                d.out = out + (size_t)2 * i * w;
-                d.out_cap = 2 * w;
-            }
-            const size_t need = m2 * sizeof(ProductDesc);
-            if (need > desc_bytes) {
-                cudaStreamSynchronize(st);
-                cudaFree(descs);
-                descs = nullptr;
-                if (cudaMalloc(&descs, need) != cudaSuccess) return fail(BGPU_ERR_OOM);
-                desc_bytes = need;
-            }
-            e = cudaMemcpyAsync(descs, pd.data(), need, cudaMemcpyHostToDevice, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             // fresh carry-scan state for this level: ticket 0, flags 0, epoch 1
-            if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, 8, st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, (size_t)m2 * bpp * 8, st);
+            const size_t nn = (size_t)1 << L.log_n;
+            e = cudaMemsetAsync(ticket, 0, 8, st);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(flags, 0, (size_t)L.m2 * carry_blocks((uint32_t)(nn / 8)) * 8, st);
             if (e == cudaSuccess) {
                 CarryLaunch cl;
                 cl.ticket_base = 0;
                 cl.epoch = 1;
                 cl.ticket = ticket;
                 cl.err = hooks.err;
-                if (e == cudaSuccess)
-                    e = launch_ntt_batch(kSlotEngine + prime_set_for(ln), hooks.consts[prime_set_for(ln)],
-                                         static_cast<const ProductDesc*>(descs), (int)m2, false, ln,
-                                         kFmtLimb64, cl, st);
+                const int ps = prime_set_for(L.log_n);
+                e = launch_ntt_batch(kSlotEngine + ps, hooks.consts[ps],
+                                     reinterpret_cast<const ProductDesc*>(base + off_desc + L.desc_off),
+                                     (int)L.m2, false, L.log_n, kFmtLimb64, cl, st);
             }
             nl += kNttLaunches;
         }
-        if (e == cudaSuccess && (m & 1)) {
-            k_tree_tail<<<1, 256, 0, st>>>(in + (m - 1) * w, out + (size_t)m2 * 2 * w, (uint32_t)w);
+        if (e == cudaSuccess && (L.m & 1)) {
+            k_tree_tail<<<1, 256, 0, st>>>(in + (size_t)(L.m - 1) * w, out + (size_t)L.m2 * 2 * w, (uint32_t)w);
             e = cudaGetLastError();
             nl += 1;
         }
-        if (e != cudaSuccess) return fail(BGPU_ERR_CUDA);
-        m = (m + 1) / 2;
-        w *= 2;
         cur ^= 1;
     }
-    cudaError_t e = cudaMemcpyAsync(d_out, buf[cur], w * 8, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const size_t wlast = lv.empty() ? 1 : lv.back().w * 2;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, buf[cur], wlast * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host descriptors live until here
     if (launches) *launches = nl;
-    const int rc = e == cudaSuccess ? BGPU_OK : BGPU_ERR_CUDA;
-    cudaFree(buf[0]);
-    cudaFree(buf[1]);
-    cudaFree(scratch);
-    cudaFree(descs);
-    return rc;
+    return e == cudaSuccess ? BGPU_OK : BGPU_ERR_CUDA;
 }
 
 }  // namespace bgpu

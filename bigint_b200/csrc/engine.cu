@@ -38,6 +38,7 @@ struct Engine {
     // device I/O buffers of the host API
     void* d_io = nullptr;
     size_t io_bytes = 0;
+    TreeArena tree;  // product-tree values, descriptors and scratch
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t last_launches = 0;
     // optional per-kernel timing of NTT products: a ring of event sets, one
@@ -70,6 +71,7 @@ void release_locked() {
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
+    cudaFree(g.tree.ptr);
     if (g.ev0) cudaEventDestroy(g.ev0);
     if (g.ev1) cudaEventDestroy(g.ev1);
     for (auto e : g.kev) cudaEventDestroy(e);
@@ -203,11 +205,34 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
     return cuda_status(e);
 }
 
-bool use_schoolbook(uint32_t flags, size_t na, size_t nb) {
+// The small-product kernel a call uses (BGPU_METHOD_AUTO: by the tuned
+// crossovers), or 0 for the transform methods.
+uint32_t small_method(uint32_t flags, size_t na, size_t nb) {
     const uint32_t m = flags & BGPU_METHOD_MASK;
-    if (m == BGPU_METHOD_SCHOOLBOOK) return true;
-    if (m == BGPU_METHOD_NTT || m == BGPU_METHOD_FFT) return false;
-    return na + nb <= tuning().schoolbook_max_limbs;
+    if (m == BGPU_METHOD_SCHOOLBOOK || m == BGPU_METHOD_KARATSUBA) return m;
+    if (m != BGPU_METHOD_AUTO) return 0;
+    const Tuning& t = tuning();
+    if (na + nb <= t.schoolbook_max_limbs) return BGPU_METHOD_SCHOOLBOOK;
+    if (na + nb <= t.karatsuba_max_limbs && karatsuba_fits(na, nb)) return BGPU_METHOD_KARATSUBA;
+    return 0;
+}
+
+// Launch the small-product kernel `m` (schoolbook or Karatsuba); operands
+// beyond the kernel's limits are an invalid argument.
+int launch_small(uint32_t m, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                 cudaStream_t st) {
+    if (m == BGPU_METHOD_SCHOOLBOOK) {
+        if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+        return cuda_status(launch_schoolbook(a, (uint32_t)na, b, (uint32_t)nb, out, st));
+    }
+    if (!karatsuba_fits(na, nb)) return BGPU_ERR_INVALID_ARG;
+    return cuda_status(launch_karatsuba(a, (uint32_t)na, b, (uint32_t)nb, out, st));
+}
+
+bool valid_method(uint32_t flags, bool allow_fft) {
+    const uint32_t m = flags & BGPU_METHOD_MASK;
+    return m == BGPU_METHOD_AUTO || m == BGPU_METHOD_NTT || m == BGPU_METHOD_SCHOOLBOOK ||
+           m == BGPU_METHOD_KARATSUBA || (allow_fft && m == BGPU_METHOD_FFT);
 }
 
 // AUTO picks the FFT form only inside the tuned limb range.
@@ -362,11 +387,10 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
             rc = multiply_device(oa, ob, square, dout, kFmtLimb64, nout, flags, st, nullptr);
             if (stats) stats->fell_back = 1;
         }
-    } else if (use_schoolbook(flags, na, nb)) {
-        if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
-        rc = cuda_status(launch_schoolbook(da, (uint32_t)na, db, (uint32_t)nb, dout, st));
+    } else if (const uint32_t sm = small_method(flags, na, nb)) {
+        rc = launch_small(sm, da, na, db, nb, dout, st);
         g.last_launches = 1;
-        if (stats) stats->method = BGPU_METHOD_SCHOOLBOOK;
+        if (stats) stats->method = (int32_t)sm;
     } else {
         OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
         OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
@@ -440,8 +464,7 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, pb, lb * 4, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_status(e);
     if (stats) cudaEventRecord(g.ev0, st);
-    if (use_schoolbook(flags, la64, lb64)) {
-        if (la64 + lb64 > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+    if (const uint32_t sm = small_method(flags, la64, lb64)) {
         uint64_t* la_d = reinterpret_cast<uint64_t*>(io + l_off);
         uint64_t* lb_d = square ? la_d : la_d + align256((la64 + 1) * 8) / 8;
         uint64_t* lo_d = reinterpret_cast<uint64_t*>(io + l_off + align256((la64 + 1) * 8) +
@@ -449,13 +472,12 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
         e = launch_digits28_to_limbs(da, (uint32_t)la, la_d, (uint32_t)la64, st);
         if (e == cudaSuccess && !square)
             e = launch_digits28_to_limbs(db, (uint32_t)lb, lb_d, (uint32_t)lb64, st);
-        if (e == cudaSuccess)
-            e = launch_schoolbook(la_d, (uint32_t)la64, lb_d, (uint32_t)lb64, lo_d, st);
-        if (e == cudaSuccess)
-            e = launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st);
         rc = cuda_status(e);
+        if (rc == BGPU_OK) rc = launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st);
+        if (rc == BGPU_OK)
+            rc = cuda_status(launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st));
         g.last_launches = square ? 3 : 4;
-        if (stats) stats->method = BGPU_METHOD_SCHOOLBOOK;
+        if (stats) stats->method = (int32_t)sm;
     } else {
         OperandDesc oa{da, (uint32_t)la, (uint32_t)((la * 28 + 31) / 32), kFmtDigit28};
         OperandDesc ob{db, (uint32_t)lb, (uint32_t)((lb * 28 + 31) / 32), kFmtDigit28};
@@ -534,7 +556,7 @@ const char* bgpu_strerror(int code) {
 int bgpu_mul_u64(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
                  size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats) {
     if (!a || !b || !out_len || (!out && out_cap) || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
-    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_FFT) return BGPU_ERR_INVALID_ARG;
+    if (!valid_method(flags, true)) return BGPU_ERR_INVALID_ARG;
     const uint32_t fb = (flags >> 8) & 0x1Fu;
     if (fb && (fb < 8 || fb > 20)) return BGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_mu);
@@ -547,7 +569,7 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
                     size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
                     size_t* out_len, uint32_t flags, bgpu_stats* stats) {
     if (!a || !b || !out_len || (!out && out_cap) || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
-    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    if (!valid_method(flags, false)) return BGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
@@ -558,16 +580,15 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
 int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
                         uint64_t* d_out, uint32_t flags, void* stream) {
     if (!d_a || !d_b || !d_out || na == 0 || nb == 0) return BGPU_ERR_INVALID_ARG;
-    if ((flags & BGPU_METHOD_MASK) > BGPU_METHOD_SCHOOLBOOK) return BGPU_ERR_INVALID_ARG;
+    if (!valid_method(flags, false)) return BGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);  // 0 = the legacy default stream
     const bool square = (d_a == d_b && na == nb);
-    if (use_schoolbook(flags, na, nb)) {
-        if (na + nb > kSchoolbookMaxLimbs) return BGPU_ERR_INVALID_ARG;
+    if (const uint32_t sm = small_method(flags, na, nb)) {
         g.last_launches = 1;
-        return cuda_status(launch_schoolbook(d_a, (uint32_t)na, d_b, (uint32_t)nb, d_out, st));
+        return launch_small(sm, d_a, na, d_b, nb, d_out, st);
     }
     if (na + nb > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
     OperandDesc oa{d_a, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
@@ -638,7 +659,7 @@ int bgpu_product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
     uint32_t nl = 0;
-    int rc = product_tree_device(d_leaves, n, d_out, out_cap, hooks_locked(),
+    int rc = product_tree_device(d_leaves, n, d_out, out_cap, hooks_locked(), &g.tree,
                                  static_cast<cudaStream_t>(stream), &nl);
     g.last_launches = nl;
     if (rc == BGPU_OK) rc = check_device_error(BGPU_OK);
@@ -661,7 +682,7 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
     cudaError_t e = cudaMemcpyAsync(dl, leaves, n * 8, cudaMemcpyHostToDevice, g.stream);
     if (e != cudaSuccess) return cuda_status(e);
     uint32_t nl = 0;
-    rc = product_tree_device(dl, n, dout, width, hooks_locked(), g.stream, &nl);
+    rc = product_tree_device(dl, n, dout, width, hooks_locked(), &g.tree, g.stream, &nl);
     g.last_launches = nl;
     if (rc != BGPU_OK) return rc;
     std::vector<uint64_t> tmp;
@@ -693,6 +714,16 @@ int bgpu_get_split(uint32_t log2_points) {
     return choose_shape((int)log2_points).log_n2;
 }
 
+int bgpu_set_batch_split(uint32_t log2_points, uint32_t log2_column) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return set_batch_split((int)log2_points, (int)log2_column) == 0 ? BGPU_OK : BGPU_ERR_INVALID_ARG;
+}
+
+int bgpu_get_batch_split(uint32_t log2_points) {
+    if (log2_points < 5 || log2_points > kMaxLogN) return BGPU_ERR_INVALID_ARG;
+    return choose_shape_batch((int)log2_points).log_n2;
+}
+
 int bgpu_set_tuning(uint32_t key, uint64_t value) {
     std::lock_guard<std::mutex> lk(g_mu);
     Tuning& t = g_tuning;
@@ -707,6 +738,14 @@ int bgpu_set_tuning(uint32_t key, uint64_t value) {
             return BGPU_OK;
         case BGPU_TUNE_FFT_MIN_LIMBS: t.fft_min_limbs = value; return BGPU_OK;
         case BGPU_TUNE_FFT_MAX_LIMBS: t.fft_max_limbs = value; return BGPU_OK;
+        case BGPU_TUNE_KARATSUBA_MAX_LIMBS:
+            if (value > 2 * kKaratsubaMaxLimbs) return BGPU_ERR_INVALID_ARG;
+            t.karatsuba_max_limbs = (uint32_t)value;
+            return BGPU_OK;
+        case BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS:
+            if (value > 2 * kKaratsubaMaxLimbs) return BGPU_ERR_INVALID_ARG;
+            t.batch_karatsuba_max_limbs = (uint32_t)value;
+            return BGPU_OK;
         default: return BGPU_ERR_INVALID_ARG;
     }
 }
@@ -720,6 +759,8 @@ int bgpu_get_tuning(uint32_t key, uint64_t* value) {
         case BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS: *value = t.batch_schoolbook_max_limbs; return BGPU_OK;
         case BGPU_TUNE_FFT_MIN_LIMBS: *value = t.fft_min_limbs; return BGPU_OK;
         case BGPU_TUNE_FFT_MAX_LIMBS: *value = t.fft_max_limbs; return BGPU_OK;
+        case BGPU_TUNE_KARATSUBA_MAX_LIMBS: *value = t.karatsuba_max_limbs; return BGPU_OK;
+        case BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS: *value = t.batch_karatsuba_max_limbs; return BGPU_OK;
         default: return BGPU_ERR_INVALID_ARG;
     }
 }
@@ -729,7 +770,7 @@ int bgpu_load_tuning(const char* path) {
     FILE* f = fopen(path, "r");
     if (!f) return BGPU_ERR_INVALID_ARG;
     // Parse everything first, apply only a fully valid table.
-    struct Split { unsigned ln, l2; };
+    struct Split { unsigned ln, l2; bool batch; };
     std::vector<Split> splits;
     std::vector<std::pair<uint32_t, unsigned long long>> vals;
     char line[256];
@@ -742,7 +783,9 @@ int bgpu_load_tuning(const char* path) {
         if (*p == '#' || *p == '\n' || *p == '\0') continue;
         const int n = sscanf(p, "%63s %llu %llu", key, &a, &b);
         if (n >= 3 && strcmp(key, "split") == 0) {
-            splits.push_back({(unsigned)a, (unsigned)b});
+            splits.push_back({(unsigned)a, (unsigned)b, false});
+        } else if (n >= 3 && strcmp(key, "batch_split") == 0) {
+            splits.push_back({(unsigned)a, (unsigned)b, true});
         } else if (n == 2 && strcmp(key, "schoolbook_max_limbs") == 0) {
             vals.push_back({BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS, a});
         } else if (n == 2 && strcmp(key, "batch_schoolbook_max_limbs") == 0) {
@@ -751,6 +794,10 @@ int bgpu_load_tuning(const char* path) {
             vals.push_back({BGPU_TUNE_FFT_MIN_LIMBS, a});
         } else if (n == 2 && strcmp(key, "fft_max_limbs") == 0) {
             vals.push_back({BGPU_TUNE_FFT_MAX_LIMBS, a});
+        } else if (n == 2 && strcmp(key, "karatsuba_max_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_KARATSUBA_MAX_LIMBS, a});
+        } else if (n == 2 && strcmp(key, "batch_karatsuba_max_limbs") == 0) {
+            vals.push_back({BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS, a});
         } else {
             rc = BGPU_ERR_INVALID_ARG;
         }
@@ -762,11 +809,18 @@ int bgpu_load_tuning(const char* path) {
         if (sp.ln < 5 || sp.ln > (unsigned)kMaxLogN || sp.l2 < 2 || sp.l2 > 11 || l1 < 3 || l1 > 15)
             return BGPU_ERR_INVALID_ARG;
     }
-    for (auto& kv : vals)
+    for (auto& kv : vals) {
         if ((kv.first == BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS || kv.first == BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS) &&
             kv.second > kSchoolbookMaxLimbs)
             return BGPU_ERR_INVALID_ARG;
-    for (const Split& sp : splits) bgpu_set_split(sp.ln, sp.l2);
+        if ((kv.first == BGPU_TUNE_KARATSUBA_MAX_LIMBS || kv.first == BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS) &&
+            kv.second > 2 * kKaratsubaMaxLimbs)
+            return BGPU_ERR_INVALID_ARG;
+    }
+    for (const Split& sp : splits) {
+        if (sp.batch) bgpu_set_batch_split(sp.ln, sp.l2);
+        else bgpu_set_split(sp.ln, sp.l2);
+    }
     for (auto& kv : vals) bgpu_set_tuning(kv.first, kv.second);
     return BGPU_OK;
 }

@@ -66,10 +66,13 @@ struct TransformShape {
     int log_n2;  // column length (outer passes)
 };
 
-TransformShape choose_shape(int log_n);   // the tuned split (bgpu_set_split), else the built-in one
-TransformShape builtin_shape(int log_n);  // the built-in split only
+TransformShape choose_shape(int log_n);        // the tuned split (bgpu_set_split), else the built-in one
+TransformShape choose_shape_batch(int log_n);  // batch classes (bgpu_set_batch_split), else built-in
+TransformShape builtin_shape(int log_n);       // the built-in split only
 int set_split(int log_n, int log_n2);  // 0 on success; log_n2 == 0 restores the default
+int set_batch_split(int log_n, int log_n2);
 bool shape_supported(int log_n, bool square);
+bool shape_supported_batch(int log_n, bool square);
 size_t smem_fwd_cols(int log_n2);
 size_t smem_mid_rows(int log_n1, bool square);
 size_t smem_inv_cols(int log_n2);
@@ -164,21 +167,41 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
 int batch_plan_run(bgpu_batch_plan_s* p, cudaStream_t st);
 void batch_plan_destroy(bgpu_batch_plan_s* p);
 uint32_t batch_plan_launches(const bgpu_batch_plan_s* p);
+// Device memory the product tree keeps between calls (grow-only).
+struct TreeArena {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
 // Pairwise product tree of n single-limb values into d_out (width: the
 // smallest power of two >= n limbs, zero padded); synchronous on `st`.
 int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, size_t out_cap,
-                        const EngineHooks& hooks, cudaStream_t st, uint32_t* launches);
+                        const EngineHooks& hooks, TreeArena* arena, cudaStream_t st,
+                        uint32_t* launches);
 
-// Schoolbook product for small operands (one CTA); out has na+nb limbs.
+// Small products, one CTA each (small_kernels.cu); out has na+nb limbs.
+struct SchoolDesc {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* out;
+    uint32_t na, nb;
+};
+constexpr uint32_t kSchoolbookMaxLimbs = 256;  // schoolbook: na + nb
+constexpr uint32_t kKaratsubaMaxLimbs = 256;   // Karatsuba: na and nb each
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
                               uint64_t* out, cudaStream_t stream);
-constexpr uint32_t kSchoolbookMaxLimbs = 256;  // na + nb
+cudaError_t launch_schoolbook_batch(const SchoolDesc* d_descs, uint32_t count, cudaStream_t stream);
+cudaError_t launch_karatsuba(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
+                             uint64_t* out, cudaStream_t stream);
+cudaError_t launch_karatsuba_batch(const SchoolDesc* d_descs, uint32_t count, cudaStream_t stream);
+inline bool karatsuba_fits(size_t na, size_t nb) { return na <= kKaratsubaMaxLimbs && nb <= kKaratsubaMaxLimbs; }
 
 // Method crossovers, set by the autotuner through bgpu_set_tuning /
 // bgpu_load_tuning (defaults below are the built-in choice).
 struct Tuning {
     uint32_t schoolbook_max_limbs = kSchoolbookMaxLimbs;        // AUTO single products
     uint32_t batch_schoolbook_max_limbs = kSchoolbookMaxLimbs;  // batch plans and product-tree levels
+    uint32_t karatsuba_max_limbs = 0;        // AUTO single products: Karatsuba for na+nb <= this (0 = off)
+    uint32_t batch_karatsuba_max_limbs = 0;  // batch plans and product-tree levels (0 = off)
     uint64_t fft_min_limbs = 0, fft_max_limbs = 0;              // AUTO host API: FFT form for na+nb in
                                                                 // [min, max]; max 0 = never
 };

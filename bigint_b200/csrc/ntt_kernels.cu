@@ -824,18 +824,24 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
 
 // ---- host launchers -------------------------------------------------------------
 
-// Column length per transform length, as set by the tuner (0 = default split).
+// Column length per transform length, as set by the tuner (0 = default
+// split): one table for single products (latency) and one for the NTT
+// classes of batch plans and product-tree levels (throughput).
 static int g_split[kMaxLogN + 1] = {};
+static int g_batch_split[kMaxLogN + 1] = {};
 
-int set_split(int log_n, int log_n2) {
+static int set_split_in(int* table, int log_n, int log_n2) {
     if (log_n < 5 || log_n > kMaxLogN) return -1;
     if (log_n2 != 0) {
         const int l1 = log_n - log_n2;
         if (log_n2 < 2 || log_n2 > 11 || l1 < 3 || l1 > 15) return -1;
     }
-    g_split[log_n] = log_n2;
+    table[log_n] = log_n2;
     return 0;
 }
+
+int set_split(int log_n, int log_n2) { return set_split_in(g_split, log_n, log_n2); }
+int set_batch_split(int log_n, int log_n2) { return set_split_in(g_batch_split, log_n, log_n2); }
 
 TransformShape builtin_shape(int log_n) {
     TransformShape s;
@@ -848,14 +854,17 @@ TransformShape builtin_shape(int log_n) {
     return s;
 }
 
-TransformShape choose_shape(int log_n) {
+static TransformShape shape_from(const int* table, int log_n) {
     TransformShape s = builtin_shape(log_n);
-    if (log_n >= 0 && log_n <= kMaxLogN && g_split[log_n]) {
-        s.log_n2 = g_split[log_n];
+    if (log_n >= 0 && log_n <= kMaxLogN && table[log_n]) {
+        s.log_n2 = table[log_n];
         s.log_n1 = log_n - s.log_n2;
     }
     return s;
 }
+
+TransformShape choose_shape(int log_n) { return shape_from(g_split, log_n); }
+TransformShape choose_shape_batch(int log_n) { return shape_from(g_batch_split, log_n); }
 
 static bool shape_ok(const TransformShape& s, bool square) {
     if (s.log_n < 5 || s.log_n > kMaxLogN) return false;
@@ -866,6 +875,7 @@ static bool shape_ok(const TransformShape& s, bool square) {
 }
 
 bool shape_supported(int log_n, bool square) { return shape_ok(choose_shape(log_n), square); }
+bool shape_supported_batch(int log_n, bool square) { return shape_ok(choose_shape_batch(log_n), square); }
 
 size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 17 * sizeof(uint2); }
 size_t smem_mid_rows(int l1, bool square) {
@@ -1065,7 +1075,7 @@ cudaError_t launch_ntt_batch(int slot, const NttConsts& c, const ProductDesc* de
         CarryLaunch piece = cl;
         piece.ticket_base = cl.ticket_base + (uint64_t)done * bpp;
         const cudaError_t e = launch_ntt_core(slot, c, descs + done, ProductDesc{}, n, square,
-                                              choose_shape(log_n), out_fmt, piece, st, nullptr);
+                                              choose_shape_batch(log_n), out_fmt, piece, st, nullptr);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

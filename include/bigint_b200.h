@@ -42,6 +42,9 @@ extern "C" {
 #define BGPU_METHOD_SCHOOLBOOK 2u /* O(n*m) kernel; na + nb <= BGPU_SCHOOLBOOK_MAX_LIMBS */
 #define BGPU_METHOD_FFT 3u        /* FP64 complex FFT (bgpu_mul_u64 only); products whose
                                      max |x - round(x)| exceeds 1/4 are redone on the NTT */
+#define BGPU_METHOD_KARATSUBA 4u  /* one Karatsuba level over column sums; na, nb each
+                                     <= BGPU_KARATSUBA_MAX_LIMBS (no counterpart in the
+                                     reference, whose brute::mul is plain schoolbook) */
 #define BGPU_METHOD_MASK 0xFu
 /* FFT form: choose bits per point from the average-case error growth instead
  * of the worst-case bound (more bits, runtime check + NTT fallback). */
@@ -50,6 +53,7 @@ extern "C" {
 #define BGPU_FFT_BITS(b) ((uint32_t)(b) << 8)
 
 #define BGPU_SCHOOLBOOK_MAX_LIMBS 256u
+#define BGPU_KARATSUBA_MAX_LIMBS 256u
 #define BGPU_MAX_LOG2_POINTS 26u  /* transform points are 32-bit digits */
 
 typedef struct bgpu_stats {
@@ -169,6 +173,10 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
 int bgpu_set_split(uint32_t log2_points, uint32_t log2_column);
 /* The column length exponent currently used for 2^log2_points points. */
 int bgpu_get_split(uint32_t log2_points);
+/* The same for the NTT classes of batch plans and product-tree levels, which
+ * the autotuner sets for throughput rather than single-product latency. */
+int bgpu_set_batch_split(uint32_t log2_points, uint32_t log2_column);
+int bgpu_get_batch_split(uint32_t log2_points);
 
 /* Method crossovers used by BGPU_METHOD_AUTO.  They replace the reference's
  * fixed dispatch thresholds (_mul, include/bigint/mul.h:208-220: brute up to
@@ -178,13 +186,17 @@ int bgpu_get_split(uint32_t log2_points);
 #define BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS 2u /* batch plans and tree levels: same, per product */
 #define BGPU_TUNE_FFT_MIN_LIMBS 3u              /* host API: FFT form for na+nb in [min, max] ... */
 #define BGPU_TUNE_FFT_MAX_LIMBS 4u              /* ... max = 0 disables the FFT form under AUTO */
+#define BGPU_TUNE_KARATSUBA_MAX_LIMBS 5u        /* single products: Karatsuba for na+nb <= v (<= 512;
+                                                   0 = off), above the schoolbook limit */
+#define BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS 6u  /* batch plans and tree levels: same */
 int bgpu_set_tuning(uint32_t key, uint64_t value);
 int bgpu_get_tuning(uint32_t key, uint64_t* value);
 
 /* Apply a tuning table written by the autotuner: a text file, one setting
  * per line ('#' starts a comment):
- *     split <log2_points> <log2_column>
+ *     split <log2_points> <log2_column>    batch_split <log2_points> <log2_column>
  *     schoolbook_max_limbs <n>      batch_schoolbook_max_limbs <n>
+ *     karatsuba_max_limbs <n>       batch_karatsuba_max_limbs <n>
  *     fft_min_limbs <n>             fft_max_limbs <n>
  * The whole file is checked before anything is applied; an unknown key or an
  * out-of-range value gives BGPU_ERR_INVALID_ARG and changes nothing. */

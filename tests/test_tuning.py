@@ -35,21 +35,29 @@ def test_set_get_roundtrip_and_limits(bb):
 
 def test_load_valid_table(bb, tmp_path):
     p = tmp_path / "t.txt"
-    p.write_text("# comment\nsplit 20 8   # trailing comment\nschoolbook_max_limbs 64\n"
-                 "batch_schoolbook_max_limbs 128\nfft_min_limbs 0\nfft_max_limbs 0\n\n")
-    old_split = bb.get_split(20)
+    p.write_text("# comment\nsplit 20 8   # trailing comment\nbatch_split 18 7\nschoolbook_max_limbs 64\n"
+                 "batch_schoolbook_max_limbs 128\nkaratsuba_max_limbs 300\nbatch_karatsuba_max_limbs 512\n"
+                 "fft_min_limbs 0\nfft_max_limbs 0\n\n")
+    old_split, old_bsplit = bb.get_split(20), bb.get_batch_split(18)
     assert bb.lib.bgpu_load_tuning(os.fsencode(str(p))) == 0
     assert bb.get_split(20) == 8
+    assert bb.get_batch_split(18) == 7
+    assert bb.get_split(18) != 7 or old_split == 7  # separate tables
     assert _get(bb, bb.BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS) == 64
     assert _get(bb, bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS) == 128
+    assert _get(bb, bb.BGPU_TUNE_KARATSUBA_MAX_LIMBS) == 300
+    assert _get(bb, bb.BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS) == 512
     bb.set_split(20, 0)
-    assert bb.get_split(20) == old_split
-    bb.set_tuning(bb.BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS, 256)
-    bb.set_tuning(bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, 256)
+    bb.set_batch_split(18, 0)
+    assert bb.get_split(20) == old_split and bb.get_batch_split(18) == old_bsplit
+    for k, v in ((bb.BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS, 256), (bb.BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS, 256),
+                 (bb.BGPU_TUNE_KARATSUBA_MAX_LIMBS, 0), (bb.BGPU_TUNE_BATCH_KARATSUBA_MAX_LIMBS, 0)):
+        bb.set_tuning(k, v)
 
 
 @pytest.mark.parametrize("body", ["bogus_key 3\n", "split 20 1\n", "split 30 9\n",
-                                  "schoolbook_max_limbs 1000\n", "split 20\n"])
+                                  "schoolbook_max_limbs 1000\n", "split 20\n", "batch_split 22 1\n",
+                                  "karatsuba_max_limbs 513\n"])
 def test_invalid_table_changes_nothing(bb, tmp_path, body):
     p = tmp_path / "bad.txt"
     p.write_text("schoolbook_max_limbs 32\n" + body)
@@ -66,7 +74,7 @@ def test_shipped_table_parses(bb):
     path = os.path.join(ROOT, "bigint_b200", "tuning_b200.txt")
     if not os.path.exists(path):
         pytest.skip("no shipped tuning table")
-    saved = {ln: bb.get_split(ln) for ln in range(10, 27)}
     assert bb.lib.bgpu_load_tuning(os.fsencode(path)) == 0
-    for ln, l2 in saved.items():
+    for ln in range(10, 27):
         bb.lib.bgpu_set_split(ln, 0)
+        bb.lib.bgpu_set_batch_split(ln, 0)
