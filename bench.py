@@ -336,30 +336,69 @@ def sweep_form(bb, torch, device, port):
     return rows
 
 
-def fft_form(bb, torch, device, A, B, reps: int):
-    """Config "FP64 FFT vs NTT": the headline workload through the FFT form with
-    bits per point from the worst-case bound and from the average bound;
-    device time of the FFT kernels per product (events inside the host call),
-    fallback counts on the uniform operands and on all-ones operands."""
-    out = {}
-    ones = np.full(A.shape[1], np.uint64(0xFFFFFFFFFFFFFFFF))
-    for name, avg in (("worst_case_bound", False), ("average_bound", True)):
-        ms, errs, fb, bits, lp = [], [], 0, None, None
-        for i in range(reps + 1):
-            _, st = bb.fft_mul(A[i % A.shape[0]], B[i % B.shape[0]], average_bound=avg, stats=True)
-            if i == 0:
-                continue  # warm-up
-            ms.append(st.device_ms)
-            errs.append(st.max_round_err)
-            fb += int(st.fell_back)
-            bits, lp = st.fft_bits, st.log2_points
-        _, sto = bb.fft_mul(ones, average_bound=avg, stats=True)
-        out[name] = {"bits_per_point": bits, "log2_points": lp,
-                     "device_ms": statistics.fmean(ms), "products_per_s": 1e3 / statistics.fmean(ms),
-                     "max_round_err": max(errs), "fallbacks": fb, "products": reps,
-                     "all_ones": {"max_round_err": sto.max_round_err, "fell_back": sto.fell_back,
-                                  "method": "ntt" if sto.fell_back else "fft"}}
-    return out
+def fft_form(bb, torch, device, reps: int = 3):
+    """Config "FP64 FFT vs NTT": the FFT form at 2^20..2^28-bit operands,
+    uniform products and all-ones squares, bits per point from the worst-case
+    and from the average error bound; device time of the FFT kernels per
+    product (events inside the host call), the measured max rounding distance,
+    whether the product was recomputed on the NTT, and the NTT's device time
+    for the same operands.  Sizes beyond the FFT's capacity (its transform
+    length or the FP64 coefficient limit) run on the NTT and say so."""
+    rng = np.random.default_rng(SEED + 4)
+    rows = []
+    for k in (20, 22, 24, 26, 28):
+        n = (1 << k) // 64
+        a = rng.integers(0, 2**64, n, dtype=np.uint64, endpoint=False)
+        b = rng.integers(0, 2**64, n, dtype=np.uint64, endpoint=False)
+        a[-1] |= np.uint64(1 << 63)
+        b[-1] |= np.uint64(1 << 63)
+        ones = np.full(n, np.uint64(0xFFFFFFFFFFFFFFFF))
+        for fill, x, y in (("uniform", a, b), ("all-ones", ones, None)):
+            args = (x,) if y is None else (x, y)
+            nt = [bb.ntt_mul(*args, stats=True)[1].device_ms for _ in range(reps + 1)][1:]
+            for bound, avg in (("worst_case", False), ("average", True)):
+                sts = [bb.fft_mul(*args, average_bound=avg, stats=True)[1] for _ in range(reps + 1)][1:]
+                st = sts[-1]
+                used = "ntt (fallback)" if st.fell_back else (
+                    "fft" if st.method == bb.BGPU_METHOD_FFT else "ntt (beyond fft capacity)")
+                rows.append({"operand_bits": 1 << k, "limbs": fill, "bound": bound,
+                             "bits_per_point": st.fft_bits or None, "log2_points": st.log2_points,
+                             "method": used, "max_round_err": st.max_round_err,
+                             "fell_back": bool(st.fell_back),
+                             "device_ms": statistics.fmean(s_.device_ms for s_ in sts),
+                             "ntt_device_ms": statistics.fmean(nt)})
+    return rows
+
+
+def fast_pow_form(bb, port, cpu: bool = True):
+    """The reference's benchmark call fast_pow(1234567, 7654321)
+    (examples/benchmark.cpp:22): the whole squaring chain on the GPU through
+    the host API, wall clock, residue-checked; the reference's own fast_pow on
+    the host cores beside it (one run)."""
+    base, e = 1234567, 7654321
+    bb.fast_pow(base, 1001)  # warm-up
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        got = bb.fast_pow(base, e)
+        times.append(time.perf_counter() - t0)
+    m = (1 << 61) - 1
+    if port.mod_m61(got) != pow(base, e, m):
+        raise SystemExit("bench fast_pow: residue check failed")
+    res = {"call": "fast_pow(1234567, 7654321)", "result_bits": int(got.size * 64),
+           "s": statistics.median(times), "launches": bb.last_launch_count(),
+           "verified": "residue mod 2^61-1"}
+    if cpu:
+        from oracle.pyoracle import Reference, have_reference
+
+        if have_reference() and Reference().has_fast_pow:
+            ref = Reference()
+            ref.init_thread_pool(host_cores())
+            t0 = time.perf_counter()
+            ref.fast_pow_digits(base, e)
+            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                    "call": "bigint::fast_pow<BigInt>"}
+    return res
 
 
 def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
@@ -615,7 +654,8 @@ def run_gpu_arm(args) -> None:
     if not args.no_forms:
         torch.cuda.synchronize(device)
         forms = {"ntt_size_sweep": sweep_form(bb, torch, device, port),
-                 "fp64_fft": fft_form(bb, torch, device, A, B, reps=10),
+                 "fp64_fft": fft_form(bb, torch, device),
+                 "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
                                                 cpu=(rank == 0 and not args.no_cpu_baseline))}

@@ -13,6 +13,7 @@ this package           reference                                       C-ABI
 ``fft_mul(A, B)``      ``bigint::mul::fft::mul`` (fft.cpp:281)         ``bgpu_mul_u64`` + FFT
 ``mul_digits(a, b,``   ``bigint::mul::mul_digits`` (mul.h:223-318)     ``bgpu_mul_digits``
 ``  precision, pos)``
+``fast_pow(base, e)``  ``fast_pow<BigInt>`` (bigint_base.h:60-69)      ``bgpu_pow_u64``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
 =====================  ==============================================  =========================
 
@@ -58,6 +59,7 @@ from ._lib import (  # noqa: F401
     mul_device,
     mul_digits,
     ntt_mul,
+    fast_pow,
     product_tree,
     product_tree_device,
     set_batch_split,

@@ -91,6 +91,8 @@ def _load() -> C.CDLL:
                                   C.POINTER(C.c_int64), u32p, C.c_size_t, szp, C.c_uint32,
                                   C.POINTER(_Stats)]
     L.bgpu_mul_digits.restype = C.c_int
+    L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]
+    L.bgpu_pow_u64.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_uint32, C.c_void_p]
     L.bgpu_mul_u64_device.restype = C.c_int
@@ -277,6 +279,35 @@ def fft_mul(A, B=None, *, digit_bits: int = 0, average_bound: bool = False, stat
     exceeds 1/4 is recomputed on the NTT (reported in ``stats``)."""
     flags = BGPU_METHOD_FFT | (int(digit_bits) << 8) | (BGPU_FFT_AVERAGE_BOUND if average_bound else 0)
     return _mul_u64(A, B, flags, stats)
+
+
+def fast_pow(base, exponent: int) -> np.ndarray:
+    """base**exponent (``fast_pow``, include/bigint/bigint_base.h:60-69) with
+    every product of the squaring chain on the GPU.  ``base`` is a Python int
+    >= 0 or a u64 limb array; returns little-endian u64 limbs."""
+    _ensure_init()
+    if isinstance(base, (int, np.integer)):
+        v = int(base)
+        if v < 0:
+            raise ValueError("base must be non-negative")
+        limbs = []
+        while v:
+            limbs.append(v & 0xFFFFFFFFFFFFFFFF)
+            v >>= 64
+        a = np.array(limbs or [0], dtype=np.uint64)
+    else:
+        a = _as_limbs(base)
+    e = int(exponent)
+    if not 0 <= e < 2**32:
+        raise ValueError("exponent must fit in 32 bits (the reference's uint32_t)")
+    bits = max(1, int(a.size) * 64)
+    cap = max(1, (bits * max(e, 1) + 63) // 64 + 1)
+    out = np.empty(cap, dtype=np.uint64)
+    n = C.c_size_t(0)
+    u64p = C.POINTER(C.c_uint64)
+    _check(lib.bgpu_pow_u64(a.ctypes.data_as(u64p), a.size, e, out.ctypes.data_as(u64p), cap,
+                            C.byref(n)), "bgpu_pow_u64")
+    return out[: n.value]
 
 
 def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = None, *,

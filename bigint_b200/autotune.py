@@ -57,12 +57,13 @@ def _rand_dev(torch, dev, rng, shape):
     return torch.from_numpy(rng.integers(0, 2**63, shape, dtype=np.int64)).to(dev)
 
 
-def valid_splits(log_n: int, square: bool = False) -> list[int]:
-    """Column-length exponents the engine accepts for 2^log_n points."""
+def valid_splits(log_n: int) -> list[int]:
+    """Column-length exponents the engine accepts for 2^log_n points (rows of
+    2^15 points exist for transforms above 2^23 points only)."""
     out = []
     for l2 in range(2, 12):
         l1 = log_n - l2
-        if 3 <= l1 <= (15 if square else 14):
+        if 3 <= l1 <= (15 if log_n > 23 else 14):
             out.append(l2)
     return out
 

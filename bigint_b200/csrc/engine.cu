@@ -419,6 +419,129 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
     return BGPU_OK;
 }
 
+// Product of device operands into dout (na + nb limbs, zero padded) with the
+// method AUTO picks: a small-product kernel or the NTT.
+int device_product(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, uint64_t* dout,
+                   cudaStream_t st, uint32_t* launches) {
+    const bool square = da == db && na == nb;
+    if (const uint32_t sm = small_method(BGPU_METHOD_AUTO, na, nb)) {
+        *launches += 1;
+        return launch_small(sm, da, na, db, nb, dout, st);
+    }
+    OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
+    OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
+    *launches += kNttLaunches;
+    return multiply_device(oa, ob, square, dout, kFmtLimb64, na + nb, BGPU_METHOD_AUTO, st, nullptr);
+}
+
+uint64_t bit_length(const uint64_t* x, size_t n) {  // n > 0, x[n-1] != 0
+    return 64 * (uint64_t)(n - 1) + (64 - (uint64_t)__builtin_clzll(x[n - 1]));
+}
+
+// base^exponent by the reference's square-and-multiply (fast_pow<T>,
+// include/bigint/bigint_base.h:60-69: res *= base on a set bit, then
+// base *= base), every product on the device.  Operand lengths come from the
+// exact bound bits(x y) <= bits(x) + bits(y), so the chain needs no host
+// synchronisation; the final squaring the reference performs after the last
+// set bit does not change the result and is skipped.
+int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
+                   size_t out_cap, size_t* out_len) {
+    nbase = strip64(base, nbase);
+    if (exponent == 0 || (nbase == 1 && base[0] == 1)) {  // x^0 = 1 (the reference's res = 1)
+        *out_len = 1;
+        if (out_cap < 1) return BGPU_ERR_OUT_CAPACITY;
+        out[0] = 1;
+        return BGPU_OK;
+    }
+    if (nbase == 0) {
+        *out_len = 0;
+        return BGPU_OK;
+    }
+    const uint64_t bbits = bit_length(base, nbase);
+    const uint64_t rbits = bbits * exponent;
+    auto limbs = [](uint64_t bits) { return (size_t)((bits + 63) / 64); };
+    const size_t rlimbs = limbs(rbits);
+    if (rlimbs > ((size_t)1 << 30)) return BGPU_ERR_CAPACITY;
+    // Plan the chain: operand sizes of every product, the largest transform.
+    int max_ln = 0;
+    size_t max_base = limbs(bbits);
+    {
+        uint64_t bb = bbits, rb = 0;
+        for (uint32_t e = exponent; e; e >>= 1) {
+            if (e & 1) {
+                if (rb) {
+                    const uint64_t t32 = 2 * (uint64_t)(limbs(rb) + limbs(bb));
+                    if (t32 > ((uint64_t)1 << kMaxLogN)) return BGPU_ERR_CAPACITY;
+                    max_ln = std::max(max_ln, ceil_log2(t32 - 1));
+                }
+                rb += bb;
+            }
+            if (e > 1) {
+                const uint64_t t32 = 4 * (uint64_t)limbs(bb);
+                if (t32 > ((uint64_t)1 << kMaxLogN)) return BGPU_ERR_CAPACITY;
+                max_ln = std::max(max_ln, ceil_log2(t32 - 1));
+                bb *= 2;
+                max_base = std::max(max_base, limbs(bb));
+            }
+        }
+    }
+    // Device buffers: two for the running base, two for the running result.
+    const size_t bsz = align256((2 * max_base + 2) * 8), rsz = align256((rlimbs + max_base + 2) * 8);
+    int rc = ensure(&g.d_io, &g.io_bytes, 2 * bsz + 2 * rsz);
+    if (rc != BGPU_OK) return rc;
+    if (max_ln >= 5) {  // size the transform scratch once for the whole chain
+        ProductScratch s{};
+        rc = prepare_scratch(max_ln, false, &s);
+        if (rc != BGPU_OK) return rc;
+    }
+    char* io = static_cast<char*>(g.d_io);
+    uint64_t* bufb[2] = {reinterpret_cast<uint64_t*>(io), reinterpret_cast<uint64_t*>(io + bsz)};
+    uint64_t* bufr[2] = {reinterpret_cast<uint64_t*>(io + 2 * bsz), reinterpret_cast<uint64_t*>(io + 2 * bsz + rsz)};
+    cudaStream_t st = g.stream;
+    cudaError_t e = cudaMemcpyAsync(bufb[0], base, nbase * 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    int cb = 0, cr = 0;
+    uint64_t bb = bbits, rb = 0;
+    uint32_t nl = 0;
+    for (uint32_t ex = exponent; ex; ex >>= 1) {
+        if (ex & 1) {
+            if (rb == 0) {
+                e = cudaMemcpyAsync(bufr[cr], bufb[cb], limbs(bb) * 8, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            } else {
+                rc = device_product(bufr[cr], limbs(rb), bufb[cb], limbs(bb), bufr[cr ^ 1], st, &nl);
+                if (rc != BGPU_OK) return rc;
+                cr ^= 1;
+            }
+            rb += bb;
+        }
+        if (ex > 1) {
+            rc = device_product(bufb[cb], limbs(bb), bufb[cb], limbs(bb), bufb[cb ^ 1], st, &nl);
+            if (rc != BGPU_OK) return rc;
+            cb ^= 1;
+            bb *= 2;
+        }
+    }
+    g.last_launches = nl;
+    std::vector<uint64_t> tmp;
+    uint64_t* dst = out;
+    if (out_cap < rlimbs) {
+        tmp.resize(rlimbs);
+        dst = tmp.data();
+    }
+    e = cudaMemcpyAsync(dst, bufr[cr], rlimbs * 8, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    const size_t n = strip64(dst, rlimbs);
+    *out_len = n;
+    if (dst != out) {
+        if (n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+        memcpy(out, dst, n * 8);
+    }
+    return BGPU_OK;
+}
+
 int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb, size_t prec,
                       int64_t* point_pos, uint32_t* out, size_t out_cap, size_t* out_len,
                       uint32_t flags, bgpu_stats* stats) {
@@ -575,6 +698,15 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
     cudaSetDevice(g.device);
     return mul_digits_locked(a, na, b, nb, output_precision, point_pos, out, out_cap, out_len,
                              flags, stats);
+}
+
+int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
+                 size_t out_cap, size_t* out_len) {
+    if (!base || !out_len || (!out && out_cap) || nbase == 0) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return pow_u64_locked(base, nbase, exponent, out, out_cap, out_len);
 }
 
 int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,

@@ -325,12 +325,20 @@ __device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t s
     }
 }
 
+// Rows too long for two row buffers in shared memory (2^15 points of a
+// non-square product): A's transformed row is parked in its own global plane
+// and read back there by the pointwise product, while B's row uses the one
+// shared buffer.
+template <int L1, bool SQR>
+constexpr bool kOneRowBuffer = !SQR && L1 >= 15;
+
 // Last DIF round of B (or A when squaring) fused with the pointwise product
 // and the first DIT round; with a single round also the inverse twiddle.
 template <bool LAZY, int L1, int T, bool SQR, bool SINGLE>
 __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& c, uint32_t* sa,
                                          uint32_t* sb, const uint32_t* row_a, const uint32_t* row_b,
                                          uint32_t* row_out, int q, uint32_t k2, const uint2* sT) {
+    constexpr bool ONE = kOneRowBuffer<L1, SQR>;
     using P1 = Plan<L1>;
     constexpr int K = P1::nr - 1;
     using Gr = Group<L1, 1, K>;
@@ -340,7 +348,7 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
     const uint2* twi = c.stage[q][1];
     const uint32_t sw = q == 0 ? a.scale_w[0] : (q == 1 ? a.scale_w[1] : a.scale_w[2]);
     const uint32_t swp = q == 0 ? a.scale_wp[0] : (q == 1 ? a.scale_wp[1] : a.scale_wp[2]);
-    const uint32_t* src = SQR ? sa : sb;
+    const uint32_t* src = (SQR || ONE) ? sa : sb;
 #pragma unroll 1
     for (int g = threadIdx.x; g < Gr::G; g += T) {
         const Gr gr(g);
@@ -355,7 +363,7 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
         dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twf, p);
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
-            const uint32_t other = SQR ? x[j] : sa[gr.at(j)];
+            const uint32_t other = SQR ? x[j] : (ONE ? row_a[gr.idx(j)] : sa[gr.at(j)]);
             x[j] = pointwise<LAZY>(x[j], other, sw, swp, p, pinv);
         }
         dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
@@ -396,9 +404,11 @@ __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, co
 template <int PS, int L1, int T, bool SQR>
 __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const MidRowsArgs a) {
     constexpr bool LAZY = PS == 0;
-    extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1])
+    constexpr bool ONE = kOneRowBuffer<L1, SQR>;
+    extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1] unless SQR or ONE)
     using P1 = Plan<L1>;
     constexpr int NR = P1::nr;
+    static_assert(!ONE || NR > 1, "the one-buffer row pass needs several rounds");
     const NttConsts& c = c_consts[a.slot];
     uint32_t* sa = sm;
     uint32_t* sb = sm + (1u << L1);
@@ -417,7 +427,7 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
     // inter-pass twiddle omega_N^-(k2 n1) = B(q) * T^j with the row-constant
     // powers sT[j] = omega_N^-(k2 j << LO0).
     constexpr int R0 = P1::r(0), LO0 = P1::lo(0);
-    uint2* sT = reinterpret_cast<uint2*>(sm + ((SQR ? 1u : 2u) << L1));
+    uint2* sT = reinterpret_cast<uint2*>(sm + ((SQR || ONE ? 1u : 2u) << L1));
     for (int t = threadIdx.x; t < (1 << R0); t += T) {
         const uint32_t w = inter_twiddle(c, q, 1, ((k2 * (uint32_t)t) << LO0) & (uint32_t)(nn - 1),
                                          a.log_n, p);
@@ -445,7 +455,15 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
         mid_turn<LAZY, L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
     } else {
         mid_dif_row<LAZY, L1, T>(row_a, sa, twf, p);
-        if constexpr (!SQR) {
+        if constexpr (ONE) {
+            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, threadIdx.x);  // A's last DIF round
+            __syncthreads();
+            // park A's transform in its plane (element i at row_a[i]) ...
+            for (uint32_t i = threadIdx.x; i < (1u << L1); i += T) row_a[i] = sa[sidx<1>(i, 0)];
+            __syncthreads();
+            // ... and transform B in the same buffer
+            mid_dif_row<LAZY, L1, T>(row_b, sa, twf, p);
+        } else if constexpr (!SQR) {
             smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, threadIdx.x);  // A's last DIF round
             mid_dif_row<LAZY, L1, T>(row_b, sb, twf, p);
         }
@@ -870,7 +888,10 @@ static bool shape_ok(const TransformShape& s, bool square) {
     if (s.log_n < 5 || s.log_n > kMaxLogN) return false;
     if (s.log_n2 < 2 || s.log_n2 > 11) return false;
     if (s.log_n1 < 3 || s.log_n1 > 15) return false;
-    if (s.log_n1 == 15 && !square) return false;
+    // Rows of 2^15 points are built for the strict prime set only (transforms
+    // above 2^23 points); non-square products use the one-buffer row pass.
+    if (s.log_n1 == 15 && prime_set_for(s.log_n) == 0) return false;
+    (void)square;
     return true;
 }
 
@@ -879,7 +900,7 @@ bool shape_supported_batch(int log_n, bool square) { return shape_ok(choose_shap
 
 size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 17 * sizeof(uint2); }
 size_t smem_mid_rows(int l1, bool square) {
-    return (square ? 1 : 2) * ((size_t)4 << l1) + 16 * sizeof(uint2);
+    return (square || l1 >= 15 ? 1 : 2) * ((size_t)4 << l1) + 16 * sizeof(uint2);
 }
 size_t smem_inv_cols(int l2) { return (size_t)kNumPrimes * kCols * 4 << l2; }
 
@@ -931,13 +952,9 @@ static cudaError_t launch_mid(const MidRowsArgs& m, bool square, uint32_t rows, 
         allow_smem(k, sm);
         return launch_k(k, grid, dim3(T), sm, st, m);
     }
-    if constexpr (L1 <= 14) {
-        auto k = k_mid_rows<PS, L1, T, false>;
-        allow_smem(k, sm);
-        return launch_k(k, grid, dim3(T), sm, st, m);
-    } else {
-        return cudaErrorInvalidValue;
-    }
+    auto k = k_mid_rows<PS, L1, T, false>;
+    allow_smem(k, sm);
+    return launch_k(k, grid, dim3(T), sm, st, m);
 }
 
 template <int PS>

@@ -96,6 +96,15 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
                     size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
                     size_t* out_len, uint32_t flags, bgpu_stats* stats);
 
+/* base^exponent for a u64-limb base: the reference's fast_pow<BigInt>
+ * (include/bigint/bigint_base.h:60-69, the squaring chain its benchmark
+ * example times, examples/benchmark.cpp:22), every product on the GPU with no
+ * host round trip between them.  Writes the power without leading zeros;
+ * 0^0 = 1 like the reference's res = 1.  BGPU_ERR_CAPACITY when a product of
+ * the chain exceeds the largest transform. */
+int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
+                 size_t out_cap, size_t* out_len);
+
 /* Device-resident product (no host copies, asynchronous on `stream`, a
  * cudaStream_t; 0 is the legacy default stream): d_out receives exactly
  * na + nb limbs (zero padded).  d_a == d_b with na == nb squares.  Errors

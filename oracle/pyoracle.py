@@ -147,6 +147,10 @@ class Reference(_Lib):
         L.ref_product_tree.restype = C.c_int
         L.ref_init_thread_pool.argtypes = [C.c_uint32]
         L.ref_init_thread_pool.restype = None
+        self.has_fast_pow = hasattr(L, "ref_fast_pow")
+        if self.has_fast_pow:
+            L.ref_fast_pow.argtypes = [C.c_uint64, C.c_uint32, _u32p, C.c_size_t, _szp]
+            L.ref_fast_pow.restype = C.c_int
 
     def init_thread_pool(self, n: int) -> None:
         """First call wins (ntt_multithread.cpp:287-290); 0/1 disables threads."""
@@ -169,6 +173,16 @@ class Reference(_Lib):
 
     def mul_digits(self, a, b=None, output_precision: int = 0, point_pos: int | None = None):
         return _mul_digits(self.lib.ref_mul_digits, a, b, output_precision, point_pos)
+
+    def fast_pow_digits(self, base: int, exponent: int) -> np.ndarray:
+        """fast_pow(BigInt(base), exponent) as reference 28-bit Digits."""
+        cap = (int(exponent) * 64) // 28 + 8
+        out = np.zeros(cap, dtype=np.uint32)
+        n = C.c_size_t(0)
+        rc = self.lib.ref_fast_pow(int(base), int(exponent), _p32(out), cap, C.byref(n))
+        if rc != 0:
+            raise OracleError(f"ref_fast_pow returned {rc}")
+        return out[: n.value].copy()
 
     def product_tree_digits(self, leaves) -> np.ndarray:
         leaves = _limbs(leaves)

@@ -12,6 +12,7 @@
 //   ref_mul         -> bigint::mul::_mul          include/bigint/mul.h:208
 //   ref_mul_digits  -> bigint::mul::mul_digits    include/bigint/mul.h:223
 //   ref_product_tree-> BigInt::operator* (bigint.h:284) over a pairwise tree
+//   ref_fast_pow    -> bigint::fast_pow<BigInt>   include/bigint/bigint_base.h:60
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -119,6 +120,14 @@ int ref_product_tree(const uint64_t* leaves, size_t n, uint32_t* out, size_t cap
         return 0;
     }
     return copy_out32(level[0].get_data(), out, cap, out_len);
+}
+
+// fast_pow over BigInt, as the reference's benchmark example calls it
+// (examples/benchmark.cpp:22); the power is returned as 28-bit Digits.
+int ref_fast_pow(uint64_t base, uint32_t exponent, uint32_t* out, size_t cap, size_t* out_len) {
+    bigint::BigInt a(base);
+    a = bigint::fast_pow(a, exponent);
+    return copy_out32(a.get_data(), out, cap, out_len);
 }
 
 }  // extern "C"

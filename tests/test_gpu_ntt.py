@@ -157,6 +157,23 @@ def test_largest_square_residue(bb, port):
     assert ra * ra % M61 == port.mod_m61(c)
 
 
+def test_largest_general_product_residue(bb, port):
+    """2^30 x 2^30-bit product (2^26 points, rows of 2^15 points through the
+    one-buffer row pass): residue identity, commutativity through the other
+    plane assignment, and the all-ones closed form."""
+    rng = np.random.default_rng(SEED + 31)
+    n = (1 << 30) // 64
+    a, b = rand_limbs(rng, n), rand_limbs(rng, n)
+    c, st = bb.ntt_mul(a, b, stats=True)
+    assert st.log2_points == 26 and c.size == 2 * n
+    assert port.mod_m61(a) * port.mod_m61(b) % M61 == port.mod_m61(c)
+    assert np.array_equal(bb.ntt_mul(b, a), c)
+    ones = np.full(n, ONES)
+    c1 = bb.ntt_mul(ones, ones.copy())  # distinct buffers: a general product, not a square
+    assert c1[0] == 1 and np.all(c1[1:n] == 0) and c1[n] == np.uint64(0xFFFFFFFFFFFFFFFE)
+    assert np.all(c1[n + 1:] == ONES)
+
+
 def test_device_resident_entry_point(bb, port):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(SEED + 16)
