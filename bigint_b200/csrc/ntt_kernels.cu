@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     {
         using Gr = Group<L2, kCols, 0>;
         constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
         for (int g = threadIdx.x; g < Gr::G; g += T) {
             const Gr gr(g);
             uint32_t v[1 << R], x[1 << R];
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
         // Last round: butterflies, inter-pass twiddle, store to global.
         using Gr = Group<L2, kCols, NR - 1>;
         constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
         for (int g = threadIdx.x; g < Gr::G; g += T) {
             const Gr gr(g);
             uint32_t x[1 << R];
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     {
         using Gr = Group<L2, kCols, NR - 1>;
         constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
         for (int g = tq; g < Gr::G; g += TP) {
             const Gr gr(g);
             uint32_t x[1 << R];
@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
         // Round 0: DIT then reduce to [0, p) for the CRT.
         using Gr = Group<L2, kCols, 0>;
         constexpr int R = Gr::R;
-#pragma unroll 1
+#pragma unroll 2
         for (int g = tq; g < Gr::G; g += TP) {
             const Gr gr(g);
             uint32_t x[1 << R];
@@ -577,7 +577,7 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     }
 
     // CRT and chunk sums: row n2 of the tile is chunk (c0 + N1*n2)/8.
-#pragma unroll 1
+#pragma unroll 2
     for (uint32_t n2 = threadIdx.x; n2 < (1u << L2); n2 += T) {
         uint32_t w0[kCols], w1[kCols], w2[kCols];
         const uint32_t row = sidx<kCols>(n2, 0);
