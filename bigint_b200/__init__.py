@@ -58,6 +58,7 @@ from ._lib import (  # noqa: F401
     mul_batch_device,
     mul_device,
     mul_digits,
+    mul_many,
     ntt_mul,
     fast_pow,
     product_tree,

@@ -66,6 +66,11 @@ class Stats:
     fft_bits: int
 
 
+class HostProduct(C.Structure):
+    _fields_ = [("a", C.c_void_p), ("na", C.c_size_t), ("b", C.c_void_p), ("nb", C.c_size_t),
+                ("out", C.c_void_p), ("out_cap", C.c_size_t), ("out_len", C.POINTER(C.c_size_t))]
+
+
 class Product(C.Structure):
     _fields_ = [("a", C.c_void_p), ("na", C.c_size_t), ("b", C.c_void_p), ("nb", C.c_size_t),
                 ("out", C.c_void_p)]
@@ -91,6 +96,8 @@ def _load() -> C.CDLL:
                                   C.POINTER(C.c_int64), u32p, C.c_size_t, szp, C.c_uint32,
                                   C.POINTER(_Stats)]
     L.bgpu_mul_digits.restype = C.c_int
+    L.bgpu_mul_u64_many.argtypes = [C.POINTER(HostProduct), C.c_size_t, C.c_uint32]
+    L.bgpu_mul_u64_many.restype = C.c_int
     L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]
     L.bgpu_pow_u64.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
@@ -253,6 +260,34 @@ def mul(A, B=None, *, stats: bool = False, out=None):
     zero limbs (an empty array for a zero operand).  ``out`` may supply the
     destination (e.g. pinned host memory); the result is a view of it."""
     return _mul_u64(A, B, BGPU_METHOD_AUTO, stats, out)
+
+
+def mul_many(pairs, outs=None, method: int = BGPU_METHOD_AUTO) -> list:
+    """Products of many host-resident pairs in one pipelined call
+    (``bgpu_mul_u64_many``): copies of neighbouring products overlap the
+    multiplies.  ``pairs`` is a list of (A, B) limb arrays (B None or A
+    itself squares); ``outs`` optionally gives each destination (>= na + nb
+    limbs, page-locked for overlap).  Returns the products as views without
+    leading zeros."""
+    _ensure_init()
+    n = len(pairs)
+    arr = (HostProduct * max(1, n))()
+    lens = (C.c_size_t * max(1, n))()
+    keep, res = [], []
+    for i, (A, B) in enumerate(pairs):
+        a = _as_limbs(A)
+        b = a if (B is None or B is A) else _as_limbs(B)
+        if a.size == 0 or b.size == 0:
+            raise BigIntGPUError(-1, "bgpu_mul_u64_many (empty operand)")
+        o = outs[i] if outs is not None else np.empty(a.size + b.size, dtype=np.uint64)
+        if o.dtype != np.uint64 or not o.flags.c_contiguous or o.size < a.size + b.size:
+            raise ValueError("each out must be a contiguous uint64 array of >= na + nb limbs")
+        keep += [a, b, o]
+        res.append(o)
+        len_ptr = C.cast(C.addressof(lens) + i * C.sizeof(C.c_size_t), C.POINTER(C.c_size_t))
+        arr[i] = HostProduct(a.ctypes.data, a.size, b.ctypes.data, b.size, o.ctypes.data, o.size, len_ptr)
+    _check(lib.bgpu_mul_u64_many(arr, n, method), "bgpu_mul_u64_many")
+    return [res[i][: lens[i]] for i in range(n)]
 
 
 def ntt_mul(A, B=None, *, stats: bool = False):

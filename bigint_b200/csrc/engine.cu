@@ -24,6 +24,11 @@ namespace {
 struct Engine {
     int device = -1;
     cudaStream_t stream = nullptr;
+    // copy streams, slot buffers and events of the pipelined host API
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    void* d_many = nullptr;
+    size_t many_bytes = 0;
+    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
     NttConsts consts[kNumSets]{};
     void* d_tables[kNumSets] = {};
     void* d_fft_tables = nullptr;
@@ -75,6 +80,14 @@ void release_locked() {
     if (g.ev0) cudaEventDestroy(g.ev0);
     if (g.ev1) cudaEventDestroy(g.ev1);
     for (auto e : g.kev) cudaEventDestroy(e);
+    cudaFree(g.d_many);
+    for (int i = 0; i < 2; ++i) {
+        if (g.ev_in[i]) cudaEventDestroy(g.ev_in[i]);
+        if (g.ev_comp[i]) cudaEventDestroy(g.ev_comp[i]);
+        if (g.ev_out[i]) cudaEventDestroy(g.ev_out[i]);
+    }
+    if (g.h2d) cudaStreamDestroy(g.h2d);
+    if (g.d2h) cudaStreamDestroy(g.d2h);
     if (g.stream) cudaStreamDestroy(g.stream);
     g = Engine{};
 }
@@ -111,6 +124,13 @@ int init_locked(int device) {
     g.device = device;
     int rc = build_tables_locked();
     if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.h2d, cudaStreamNonBlocking));
+    if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.d2h, cudaStreamNonBlocking));
+    for (int i = 0; i < 2 && rc == BGPU_OK; ++i) {
+        rc = cuda_status(cudaEventCreateWithFlags(&g.ev_in[i], cudaEventDisableTiming));
+        if (rc == BGPU_OK) rc = cuda_status(cudaEventCreateWithFlags(&g.ev_comp[i], cudaEventDisableTiming));
+        if (rc == BGPU_OK) rc = cuda_status(cudaEventCreateWithFlags(&g.ev_out[i], cudaEventDisableTiming));
+    }
     if (rc == BGPU_OK) rc = cuda_status(cudaMalloc(&g.d_err, sizeof(uint32_t)));
     if (rc == BGPU_OK) rc = cuda_status(cudaMemset(g.d_err, 0, sizeof(uint32_t)));
     if (rc == BGPU_OK) rc = cuda_status(cudaMalloc(&g.d_ticket, sizeof(unsigned long long)));
@@ -542,6 +562,89 @@ int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64
     return BGPU_OK;
 }
 
+// Many host-resident products, pipelined: two device slots; product i's
+// operands go up on the H2D stream while product i-1 computes and product
+// i-2's result comes back on the D2H stream.  Every product still makes its
+// own host->device and device->host copies.
+int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags) {
+    struct Item { size_t na, nb; bool square; };
+    std::vector<Item> it(count);
+    size_t slot_in = 0, slot_out = 0;
+    int max_ln = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const bgpu_host_product& q = p[i];
+        if (!q.a || !q.b || !q.out || !q.out_len || q.na == 0 || q.nb == 0) return BGPU_ERR_INVALID_ARG;
+        const bool square = q.a == q.b && q.na == q.nb;
+        const size_t na = strip64(q.a, q.na), nb = square ? na : strip64(q.b, q.nb);
+        if (q.out_cap < q.na + q.nb) return BGPU_ERR_OUT_CAPACITY;
+        if (na + nb > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+        it[i] = {na, nb, square};
+        slot_in = std::max(slot_in, align256(na * 8) + align256(nb * 8));
+        slot_out = std::max(slot_out, align256((na + nb) * 8));
+        if (na && nb && !small_method(flags, na, nb)) {
+            const int ln = ceil_log2(2 * (uint64_t)(na + nb) - 1);
+            if (ln > kMaxLogN) return BGPU_ERR_CAPACITY;
+            max_ln = std::max(max_ln, ln < 5 ? 5 : ln);
+        }
+    }
+    const size_t slot = slot_in + slot_out;
+    int rc = ensure(&g.d_many, &g.many_bytes, 2 * slot);
+    if (rc != BGPU_OK) return rc;
+    if (max_ln) {  // size the transform scratch once, before anything is in flight
+        ProductScratch s{};
+        rc = prepare_scratch(max_ln, false, &s);
+        if (rc != BGPU_OK) return rc;
+    }
+    cudaStream_t st = g.stream;
+    uint32_t nl = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const bgpu_host_product& q = p[i];
+        const Item& m = it[i];
+        const int k = (int)(i & 1);
+        char* base = static_cast<char*>(g.d_many) + k * slot;
+        uint64_t* da = reinterpret_cast<uint64_t*>(base);
+        uint64_t* db = m.square ? da : reinterpret_cast<uint64_t*>(base + align256(m.na * 8));
+        uint64_t* dout = reinterpret_cast<uint64_t*>(base + slot_in);
+        const size_t nout = q.na + q.nb;
+        cudaError_t e = cudaSuccess;
+        if (i >= 2) e = cudaStreamWaitEvent(g.h2d, g.ev_out[k], 0);  // slot k's last result is out
+        if (m.na == 0 || m.nb == 0) {  // a zero operand: the product is zero
+            if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, nout * 8, g.h2d);
+            if (e == cudaSuccess) e = cudaEventRecord(g.ev_comp[k], g.h2d);
+        } else {
+            if (e == cudaSuccess) e = cudaMemcpyAsync(da, q.a, m.na * 8, cudaMemcpyHostToDevice, g.h2d);
+            if (e == cudaSuccess && !m.square)
+                e = cudaMemcpyAsync(db, q.b, m.nb * 8, cudaMemcpyHostToDevice, g.h2d);
+            if (e == cudaSuccess) e = cudaEventRecord(g.ev_in[k], g.h2d);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, g.ev_in[k], 0);
+            if (e != cudaSuccess) return cuda_status(e);
+            if (const uint32_t sm = small_method(flags, m.na, m.nb)) {
+                rc = launch_small(sm, da, m.na, db, m.nb, dout, st);
+                nl += 1;
+            } else {
+                OperandDesc oa{da, (uint32_t)m.na, (uint32_t)(2 * m.na), kFmtLimb64};
+                OperandDesc ob{db, (uint32_t)m.nb, (uint32_t)(2 * m.nb), kFmtLimb64};
+                rc = multiply_device(oa, ob, m.square, dout, kFmtLimb64, m.na + m.nb, flags, st, nullptr);
+                nl += kNttLaunches;
+            }
+            if (rc != BGPU_OK) return rc;
+            if (m.na + m.nb < nout) e = cudaMemsetAsync(dout + m.na + m.nb, 0, (nout - m.na - m.nb) * 8, st);
+            if (e == cudaSuccess) e = cudaEventRecord(g.ev_comp[k], st);
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(g.d2h, g.ev_comp[k], 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(q.out, dout, nout * 8, cudaMemcpyDeviceToHost, g.d2h);
+        if (e == cudaSuccess) e = cudaEventRecord(g.ev_out[k], g.d2h);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    g.last_launches = nl;
+    cudaError_t e = cudaStreamSynchronize(g.d2h);
+    if (e != cudaSuccess) return cuda_status(e);
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    for (size_t i = 0; i < count; ++i) *p[i].out_len = strip64(p[i].out, p[i].na + p[i].nb);
+    return BGPU_OK;
+}
+
 int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb, size_t prec,
                       int64_t* point_pos, uint32_t* out, size_t out_cap, size_t* out_len,
                       uint32_t flags, bgpu_stats* stats) {
@@ -698,6 +801,15 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
     cudaSetDevice(g.device);
     return mul_digits_locked(a, na, b, nb, output_precision, point_pos, out, out_cap, out_len,
                              flags, stats);
+}
+
+int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t flags) {
+    if (!products && count) return BGPU_ERR_INVALID_ARG;
+    if (!valid_method(flags, false)) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return mul_u64_many_locked(products, count, flags);
 }
 
 int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,

@@ -96,6 +96,27 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
                     size_t output_precision, int64_t* point_pos, uint32_t* out, size_t out_cap,
                     size_t* out_len, uint32_t flags, bgpu_stats* stats);
 
+/* Many independent products of host-resident operands, pipelined: each
+ * product's operands are copied to the GPU, multiplied and the product copied
+ * back, with the copies of neighbouring products overlapping the multiply
+ * (two device slots, separate copy streams).  The reference multiplies one
+ * pair per call (_mul, include/bigint/mul.h:208-220); this is that call over a
+ * list, for callers with many products at hand (binary splitting,
+ * examples/pi.cpp:41-80).  out receives na + nb limbs (out_cap >= na + nb;
+ * zero padded) and *out_len the length without leading zeros.  a == b with
+ * na == nb squares.  Overlap needs page-locked host buffers; pageable ones
+ * work but copy synchronously.  Returns after every product is back. */
+typedef struct bgpu_host_product {
+    const uint64_t* a;
+    size_t na;
+    const uint64_t* b;
+    size_t nb;
+    uint64_t* out;
+    size_t out_cap;
+    size_t* out_len;
+} bgpu_host_product;
+int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t flags);
+
 /* base^exponent for a u64-limb base: the reference's fast_pow<BigInt>
  * (include/bigint/bigint_base.h:60-69, the squaring chain its benchmark
  * example times, examples/benchmark.cpp:22), every product on the GPU with no

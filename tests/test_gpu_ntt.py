@@ -198,3 +198,25 @@ def test_product_tree_matches_reference_tree(bb, golden):
                 nxt.append(leaves[-1])
             leaves = nxt
         assert np.array_equal(leaves[0], digits28_to_limbs(golden[f"tree_{k:03d}_digits"]))
+
+
+def test_mul_many_pipelined(bb, port):
+    """bgpu_mul_u64_many: many host-resident products in one pipelined call
+    (copies overlapping the multiplies), mixed sizes, squares and zeros."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 33)
+    pairs, want = [], []
+    for i, (na, nb) in enumerate([(262144, 262144), (5000, 3000), (3, 2), (100, 100), (40000, 1),
+                                  (262144, 262144), (70000, 65000), (1, 1)]):
+        a = rand_limbs(rng, na)
+        b = a if i == 3 else rand_limbs(rng, nb)
+        if i == 7:
+            b = np.zeros(1, dtype=np.uint64)  # a zero operand
+        pairs.append((a, b))
+        want.append(port.mul(a) if i == 3 else port.mul(a, b))
+    outs = [torch.empty(a.size + b.size, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+            for a, b in pairs]
+    got = bb.mul_many(pairs, outs)
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert np.array_equal(g, w), i
+    assert all(np.array_equal(x, y) for x, y in zip(bb.mul_many(pairs), want))  # pageable buffers
