@@ -96,6 +96,8 @@ def _load() -> C.CDLL:
                                   C.POINTER(C.c_int64), u32p, C.c_size_t, szp, C.c_uint32,
                                   C.POINTER(_Stats)]
     L.bgpu_mul_digits.restype = C.c_int
+    L.bgpu_selftest_wait.argtypes = [C.c_uint32, C.c_int]
+    L.bgpu_selftest_wait.restype = C.c_int
     L.bgpu_mul_u64_many.argtypes = [C.POINTER(HostProduct), C.c_size_t, C.c_uint32]
     L.bgpu_mul_u64_many.restype = C.c_int
     L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]

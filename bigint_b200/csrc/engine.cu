@@ -803,6 +803,21 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
                              flags, stats);
 }
 
+int bgpu_selftest_wait(uint32_t spin_limit, int set_flag) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    // one flag word in the grow-only I/O buffer: 0 (no epoch) or epoch 1 set
+    int rc = ensure(&g.d_io, &g.io_bytes, 256);
+    if (rc != BGPU_OK) return rc;
+    uint64_t* flag = static_cast<uint64_t*>(g.d_io);
+    const uint64_t word = set_flag ? ((uint64_t)1 << 4) | (2u << 2) : 0;
+    cudaError_t e = cudaMemcpyAsync(flag, &word, sizeof(word), cudaMemcpyHostToDevice, g.stream);
+    if (e == cudaSuccess) e = launch_wait_selftest(flag, 1, spin_limit, g.d_err, g.stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    return check_device_error(BGPU_OK);
+}
+
 int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t flags) {
     if (!products && count) return BGPU_ERR_INVALID_ARG;
     if (!valid_method(flags, false)) return BGPU_ERR_INVALID_ARG;

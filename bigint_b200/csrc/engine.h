@@ -110,6 +110,10 @@ extern const char* const kNttKernelNames[kNttLaunches];
 
 uint32_t carry_blocks(uint32_t nchunks);
 
+// Diagnostic launch of the carry scan's bounded wait on one flag word.
+cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t limit, uint32_t* err,
+                                 cudaStream_t st);
+
 // Batched NTT products: `count` products of 2^log_n points described by the
 // device array `descs`, four launches in all (one per pass, a grid slice per
 // product); the carry scan takes count * carry_blocks(N/8) tickets.

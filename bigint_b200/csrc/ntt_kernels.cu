@@ -638,6 +638,36 @@ __device__ __forceinline__ uint64_t make_flag(uint64_t epoch, uint32_t status, u
     return (epoch << 4) | ((uint64_t)status << 2) | ((uint64_t)g << 1) | pbit;
 }
 
+// Bounded wait for a look-back flag word of the current epoch: returns it, or
+// 0 after `limit` polls with bit 0 of the error word set.  The only wait of
+// the carry scan; the diagnostic k_wait_selftest runs it on its own.
+__device__ __forceinline__ uint64_t wait_flag(const uint64_t* flag, uint64_t epoch, uint32_t limit,
+                                              uint32_t* err) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> w(
+        *reinterpret_cast<unsigned long long*>(const_cast<uint64_t*>(flag)));
+    for (uint32_t spins = 0;; ++spins) {
+        const uint64_t f = w.load(cuda::memory_order_acquire);
+        if ((f >> 4) == epoch) return f;
+        if (spins >= limit) {
+            atomicOr(err, 1u);
+            return 0;
+        }
+        __nanosleep(32);
+    }
+}
+
+// Diagnostic: one thread waits on `flag` for `epoch` with the carry scan's
+// wait; with a flag nothing sets it gives up after `limit` polls.
+__global__ void k_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t limit, uint32_t* err) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) wait_flag(flag, epoch, limit, err);
+}
+
+cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t limit, uint32_t* err,
+                                 cudaStream_t st) {
+    k_wait_selftest<<<1, 32, 0, st>>>(flag, epoch, limit, err);
+    return cudaGetLastError();
+}
+
 // Carry resolution over chunks of 8 coefficients.  Chunk c's final value is
 // (D_c + spill_{c-1} + carry_c) mod 2^256 with carry_{c+1} = G_c | (P_c & carry_c),
 // G_c = "D_c + spill_{c-1} >= 2^256", P_c = "D_c + spill_{c-1} == 2^256 - 1".
@@ -735,19 +765,9 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         } else {
             self.store(make_flag(a.epoch, 1, bG, bP), cuda::memory_order_release);
             int k = (int)bid - 1;
-            uint32_t spins = 0;
             while (true) {
-                cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> pred(
-                    *reinterpret_cast<unsigned long long*>(flags + k));
-                const uint64_t f = pred.load(cuda::memory_order_acquire);
-                if ((f >> 4) != a.epoch) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(a.err, 1u);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
+                const uint64_t f = wait_flag(flags + k, a.epoch, kSpinLimit, a.err);
+                if (f == 0) break;  // gave up: error recorded, carry taken as 0
                 const uint32_t st = (uint32_t)(f >> 2) & 3u, fg = (uint32_t)(f >> 1) & 1u,
                                fp = (uint32_t)f & 1u;
                 if (st == 2) {

@@ -139,6 +139,16 @@ int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, siz
  * the sticky device status. */
 int bgpu_device_status(void* stream);
 
+/* Diagnostic of failure detection, safe to run on a shared GPU: one thread
+ * runs the carry scan's bounded wait on a device flag word for at most
+ * spin_limit polls.  With set_flag = 0 nothing ever sets the flag, the wait
+ * gives up, the device error word is set and the call returns
+ * BGPU_ERR_DEVICE_TIMEOUT (the context stays usable and the error is cleared);
+ * with set_flag = 1 the flag is already set and the call returns BGPU_OK.
+ * No counterpart in the reference (its waits are on host threads,
+ * src/mul/ntt_multithread.cpp:184-203). */
+int bgpu_selftest_wait(uint32_t spin_limit, int set_flag);
+
 /* Number of kernel launches the last multiply issued (for bench accounting). */
 uint32_t bgpu_last_launch_count(void);
 

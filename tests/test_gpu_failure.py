@@ -1,0 +1,60 @@
+"""Failure detection without a GPU fault: the carry scan's only wait is
+bounded; here it runs (bgpu_selftest_wait) on a flag word that nothing sets,
+gives up after a short limit, and reports BGPU_ERR_DEVICE_TIMEOUT through the
+sticky device error word -- after which the context keeps working."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+
+from conftest import SEED, rand_limbs
+
+pytestmark = pytest.mark.gpu
+BGPU_ERR_DEVICE_TIMEOUT = -7
+
+
+def test_wait_on_unset_flag_times_out_and_context_survives(bb, port):
+    t0 = time.perf_counter()
+    assert bb.lib.bgpu_selftest_wait(20000, 0) == BGPU_ERR_DEVICE_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0  # gave up after its limit, well under a second typically
+    assert bb.lib.bgpu_selftest_wait(20000, 1) == 0  # error word cleared; a set flag passes at once
+    rng = np.random.default_rng(SEED + 80)
+    a, b = rand_limbs(rng, 70000), rand_limbs(rng, 50000)
+    assert np.array_equal(bb.mul(a, b), port.mul(a, b))  # tickets restarted, products still exact
+
+
+def test_device_status_reports_and_clears(bb):
+    assert bb.lib.bgpu_selftest_wait(1000, 0) == BGPU_ERR_DEVICE_TIMEOUT
+    bb.device_status(0)  # nothing left to report
+
+
+def test_concurrent_host_threads(bb, port):
+    """The reference claims thread safety (README.md:10); calls from several
+    host threads are serialized inside the library and each gets its own
+    exact product."""
+    import threading
+
+    rng = np.random.default_rng(SEED + 81)
+    jobs = [(rand_limbs(rng, n), rand_limbs(rng, m)) for n, m in
+            [(5000, 4000), (100, 90), (70000, 1000), (3, 3), (20000, 20000), (128, 64)] * 3]
+    want = [port.mul(a, b) for a, b in jobs]
+    got = [None] * len(jobs)
+    errors = []
+
+    def worker(idx):
+        try:
+            for i in idx:
+                got[i] = bb.mul(*jobs[i])
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(range(t, len(jobs), 4),)) for t in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert np.array_equal(g, w), i
