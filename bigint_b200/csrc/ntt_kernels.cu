@@ -313,16 +313,15 @@ struct MidRowsArgs {
     uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
 };
 
-// Pointwise product a*b*N^-1 (cancelling the Montgomery 2^-32 with the scale).
+// a*b*2^-32 mod p in [0, p); the 2^-32 and the inverse transform's N^-1 are
+// both cancelled by the scale N^-1 * 2^32 folded into the row's inverse
+// inter-pass twiddle (one multiply per group instead of one per point).
 template <bool LAZY>
-__device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t sw, uint32_t swp,
-                                              uint32_t p, uint32_t pinv) {
-    if constexpr (LAZY) {
-        const uint32_t y = csub(mont_lazy(a, b, b * pinv, p), p);  // b < 2p: result < 2p
-        return mont_lazy(y, sw, swp, p);
-    } else {
-        return mont_mul_pre(mont_mul(a, b, p, pinv), sw, swp, p);
-    }
+__device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
+    if constexpr (LAZY)
+        return csub(mont_lazy(a, b, b * pinv, p), p);  // a, b < 2p, 4p < 2^32: product term < p
+    else
+        return mont_mul(a, b, p, pinv);
 }
 
 // Rows too long for two row buffers in shared memory (2^15 points of a
@@ -364,12 +363,12 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
             const uint32_t other = SQR ? x[j] : (ONE ? row_a[gr.idx(j)] : sa[gr.at(j)]);
-            x[j] = pointwise<LAZY>(x[j], other, sw, swp, p, pinv);
+            x[j] = pointwise<LAZY>(x[j], other, p, pinv);
         }
         dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
         if constexpr (SINGLE) {
             // one round covers the row: n1 = j, twiddle omega^-(k2 j) = sT[j]
-            const uint32_t bw = c.one_w[q], bwp = c.one_wp[q];
+            const uint32_t bw = sw, bwp = swp;  // the scale N^-1 * 2^32 (no inter-pass twiddle part)
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) row_out[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
         } else {
@@ -422,6 +421,8 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
     uint32_t* row_a = pd.y + q * nn + (size_t)slot * (1u << L1);
     const uint32_t* row_b = SQR ? nullptr : pd.y + (kNumPrimes + q) * nn + (size_t)slot * (1u << L1);
     const uint32_t k2 = bitrev(slot, a.log_n2);
+    const uint32_t sw = q == 0 ? a.scale_w[0] : (q == 1 ? a.scale_w[1] : a.scale_w[2]);
+    const uint32_t swp = q == 0 ? a.scale_wp[0] : (q == 1 ? a.scale_wp[1] : a.scale_wp[2]);
 
     // The last DIT round's groups hold n1 = q + (j << LO0); the inverse
     // inter-pass twiddle omega_N^-(k2 n1) = B(q) * T^j with the row-constant
@@ -480,7 +481,9 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) x[j] = sa[gr.at(j)];
             dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
-            const uint32_t bw = inter_twiddle(c, q, 1, (k2 * gr.base) & (uint32_t)(nn - 1), a.log_n, p);
+            // inverse inter-pass twiddle of the group times the scale N^-1 * 2^32
+            const uint32_t bw = mont_mul_pre(
+                inter_twiddle(c, q, 1, (k2 * gr.base) & (uint32_t)(nn - 1), a.log_n, p), sw, swp, p);
             const uint32_t bwp = bw * pinv;
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j) row_a[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
