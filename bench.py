@@ -748,6 +748,38 @@ def run_gpu_arm(args) -> None:
     print(json.dumps(line))
 
 
+FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "batched_4096", "product_tree_2p20")
+
+
+def run_single_form(args) -> None:
+    """One of the other configurations alone (for profiling it): prints
+    {"form": name, "result": ...}."""
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    import bigint_b200 as bb
+    from oracle.pyoracle import Port
+
+    bb.init(0)
+    port = Port()
+    name = args.form
+    if name == "batched_2p24":
+        A, B = make_operands(args.bits, pairs=32)
+        res = batched_same_size_form(bb, torch, device, port, A, B)
+    elif name == "ntt_size_sweep":
+        res = sweep_form(bb, torch, device, port)
+    elif name == "fp64_fft":
+        res = fft_form(bb, torch, device)
+    elif name == "fast_pow":
+        res = fast_pow_form(bb, port, cpu=not args.no_cpu_baseline)
+    elif name == "batched_4096":
+        res = batched_form(bb, torch, device, port)
+    else:
+        res = tree_form(bb, torch, device, port, cpu=not args.no_cpu_baseline)
+    print(json.dumps({"form": name, "result": res}))
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -759,9 +791,14 @@ def main(argv=None) -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the other configurations (size sweep, FFT form, batch, tree)")
+    ap.add_argument("--form", choices=FORMS, default=None,
+                    help="run only this one of the other configurations and print its result")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.form:
+        run_single_form(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:

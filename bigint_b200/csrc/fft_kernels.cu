@@ -22,7 +22,7 @@
 
 namespace bgpu {
 
-constexpr int kFftCols = 8;
+constexpr int kFftCols = 4;  // columns per column tile: 4 x 16 B = 64 B per row segment
 constexpr int kFftMaxR = 3;  // radix-8 rounds (double2 data: 16 values per thread)
 
 __constant__ FftConsts c_fft;
@@ -35,15 +35,27 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 w) {
     return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
 }
 
-// Shared-memory placement for 16-byte elements.  Column tiles need no
-// swizzle (8 lanes of a phase read 8 consecutive columns); rows use an
-// XOR-linear, bijective swizzle that keeps 8-lane phases conflict free.
+// Shared-memory placement for 16-byte elements.  Column tiles of 4 columns
+// put row i at slots 4*swz(i) .. 4*swz(i)+3, swz(i) = i with bit 0 flipped by
+// the parity of the higher bits: the two rows an 8-lane phase touches always
+// differ by one power of two, so they land in opposite halves of a 128-byte
+// window (conflict free).  Rows use an XOR-linear, bijective swizzle that
+// keeps 8-lane phases conflict free.  Both are linear over GF(2).
+__host__ __device__ constexpr uint32_t parity32(uint32_t v) {
+    v ^= v >> 16;
+    v ^= v >> 8;
+    v ^= v >> 4;
+    v ^= v >> 2;
+    v ^= v >> 1;
+    return v & 1u;
+}
+
 template <int C>
 __host__ __device__ constexpr uint32_t fsoff(uint32_t i) {
     if constexpr (C == 1)
         return i ^ (((i >> 2) ^ (i >> 5)) & 7u);
     else
-        return i * C;
+        return (i ^ parity32(i >> 1)) * C;
 }
 
 template <int L, int C, int K>
