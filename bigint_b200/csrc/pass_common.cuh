@@ -68,9 +68,12 @@ struct Group {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Opt in to large dynamic shared memory.  The default limit (48 KB) covers
+// static plus dynamic memory, so kernels with a few KB of static tables opt in
+// a little below it too.
 template <class K>
 static void allow_smem(K k, size_t bytes) {
-    if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (bytes > 40 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // Launch with programmatic stream serialization, so the kernel's launch
