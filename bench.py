@@ -372,6 +372,20 @@ def fft_form(bb, torch, device, reps: int = 3):
     return rows
 
 
+def digits28_to_limbs_np(d) -> np.ndarray:
+    """Little-endian 28-bit digits -> u64 limbs (vectorised bit repacking)."""
+    d = np.ascontiguousarray(d, dtype=np.uint32)
+    bits = np.unpackbits(d.view(np.uint8), bitorder="little").reshape(-1, 32)[:, :28].ravel()
+    pad = (-bits.size) % 64
+    if pad:
+        bits = np.concatenate([bits, np.zeros(pad, dtype=np.uint8)])
+    limbs = np.packbits(bits, bitorder="little").view(np.uint64)
+    n = limbs.size
+    while n and limbs[n - 1] == 0:
+        n -= 1
+    return limbs[:n]
+
+
 def fast_pow_form(bb, port, cpu: bool = True):
     """The reference's benchmark call fast_pow(1234567, 7654321)
     (examples/benchmark.cpp:22): the whole squaring chain on the GPU through
@@ -390,16 +404,29 @@ def fast_pow_form(bb, port, cpu: bool = True):
     res = {"call": "fast_pow(1234567, 7654321)", "result_bits": int(got.size * 64),
            "s": statistics.median(times), "launches": bb.last_launch_count(),
            "verified": "residue mod 2^61-1"}
-    if cpu:
-        from oracle.pyoracle import Reference, have_reference
+    from oracle.pyoracle import REF_GPU_SO, Reference, have_reference, have_reference_gpu
 
-        if have_reference() and Reference().has_fast_pow:
-            ref = Reference()
-            ref.init_thread_pool(host_cores())
-            t0 = time.perf_counter()
-            ref.fast_pow_digits(base, e)
-            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
-                                    "call": "bigint::fast_pow<BigInt>"}
+    if have_reference_gpu():
+        # the reference's own fast_pow<BigInt> (unmodified C++), its products
+        # hooked to this engine (bigint_b200/hooks/reference_hook.cpp)
+        hooked = Reference(REF_GPU_SO)
+        hooked.init_thread_pool(1)
+        hooked.fast_pow_digits(base, 1001)
+        t0 = time.perf_counter()
+        d = hooked.fast_pow_digits(base, e)
+        el = time.perf_counter() - t0
+        same = np.array_equal(digits28_to_limbs_np(d), got)
+        if not same:
+            raise SystemExit("bench fast_pow: hooked reference differs from bgpu_pow_u64")
+        res["reference_code_on_gpu"] = {"s": el, "call": "bigint::fast_pow<BigInt> with ntt::mul and "
+                                        "fft::mul hooked to bgpu_mul_u64", "identical": same}
+    if cpu and have_reference() and Reference().has_fast_pow:
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        t0 = time.perf_counter()
+        ref.fast_pow_digits(base, e)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                "call": "bigint::fast_pow<BigInt>"}
     return res
 
 

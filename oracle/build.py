@@ -74,12 +74,50 @@ def build_ref(force: bool = False) -> str | None:
     return REF_SO
 
 
+HOOK_SRC = os.path.join(os.path.dirname(HERE), "bigint_b200", "hooks", "reference_hook.cpp")
+ENGINE_DIR = os.path.join(os.path.dirname(HERE), "bigint_b200")
+REF_GPU_SO = os.path.join(REF_DIR, "libbigint_ref_gpu.so")
+# The reference without its CPU NTT and FFT translation units: those two
+# functions (and init_thread_pool) come from the hook, which calls the engine.
+REF_GPU_SOURCES = ["src/mul/ssa.cpp", "src/bigint.cpp"]
+
+
+def build_ref_gpu(force: bool = False) -> str | None:
+    """The unmodified reference BigInt with its multiplies on the GPU engine
+    (bigint_b200/hooks/reference_hook.cpp), plus the same C-ABI shim as the
+    reference oracle, linked against bigint_b200/libbigint_b200.so."""
+    engine = os.path.join(ENGINE_DIR, "libbigint_b200.so")
+    if not os.path.isdir(os.path.join(REF_ROOT, "src")) or not os.path.exists(engine):
+        return REF_GPU_SO if os.path.exists(REF_GPU_SO) else None
+    os.makedirs(REF_DIR, exist_ok=True)
+    shim = os.path.join(HERE, "ref_shim.cpp")
+    compat = os.path.join(HERE, "ref_compat.h")
+    srcs = [os.path.join(REF_ROOT, s) for s in REF_GPU_SOURCES]
+    if not (force or _stale(REF_GPU_SO, srcs + [shim, compat, HOOK_SRC, engine, __file__])):
+        return REF_GPU_SO
+    flags = ["-std=c++20", "-O3", "-DNDEBUG", "-mavx", "-mavx2", "-mfma", "-fPIC", "-pthread",
+             "-include", compat, "-I", os.path.join(REF_ROOT, "include"),
+             "-I", os.path.join(os.path.dirname(HERE), "include")]
+    objs = []
+    for s in srcs + [shim, HOOK_SRC]:
+        o = os.path.join(REF_DIR, "gpu_" + os.path.basename(s).replace(".cpp", ".o"))
+        _run(["g++", *flags, "-c", s, "-o", o])
+        objs.append(o)
+    _run(["g++", "-shared", "-pthread", "-Wl,-Bsymbolic", *objs, "-o", REF_GPU_SO,
+          "-L", ENGINE_DIR, "-lbigint_b200", "-Wl,-rpath,$ORIGIN/../../bigint_b200"])
+    for o in objs:
+        os.remove(o)
+    return REF_GPU_SO
+
+
 def main(argv: list[str]) -> int:
     what = argv[1] if len(argv) > 1 else "all"
     if what in ("port", "all"):
         print("oracle port:", build_port())
     if what in ("ref", "all"):
         print("oracle reference:", build_ref())
+    if what in ("ref_gpu", "all"):
+        print("reference on the GPU engine:", build_ref_gpu())
     return 0
 
 

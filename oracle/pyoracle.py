@@ -15,6 +15,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbigint_ref.so")
+# The same reference sources with ntt::mul / fft::mul / init_thread_pool taken
+# from bigint_b200/hooks/reference_hook.cpp (products on the GPU engine).
+REF_GPU_SO = os.path.join(HERE, "_ref", "libbigint_ref_gpu.so")
 
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
@@ -197,6 +200,10 @@ class Reference(_Lib):
 
 def have_reference() -> bool:
     return os.path.exists(REF_SO)
+
+
+def have_reference_gpu() -> bool:
+    return os.path.exists(REF_GPU_SO)
 
 
 def digits28_to_limbs(d) -> np.ndarray:

@@ -56,6 +56,19 @@ def reference():
 
 
 @pytest.fixture(scope="session")
+def reference_gpu():
+    """The unmodified reference BigInt with ntt::mul / fft::mul hooked to the
+    GPU engine (bigint_b200/hooks/reference_hook.cpp)."""
+    from oracle.pyoracle import REF_GPU_SO, Reference, have_reference_gpu
+
+    if not have_reference_gpu():
+        pytest.skip("oracle/_ref/libbigint_ref_gpu.so (reference + GPU hook) is not built")
+    r = Reference(REF_GPU_SO)
+    r.init_thread_pool(1)  # the hook initializes the engine
+    return r
+
+
+@pytest.fixture(scope="session")
 def golden():
     path = os.path.join(ROOT, "tests", "golden", "golden.npz")
     return dict(np.load(path, allow_pickle=False))
