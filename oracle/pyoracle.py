@@ -150,6 +150,11 @@ class Reference(_Lib):
         L.ref_product_tree.restype = C.c_int
         L.ref_init_thread_pool.argtypes = [C.c_uint32]
         L.ref_init_thread_pool.restype = None
+        self.has_reciprocal = hasattr(L, "ref_reciprocal")
+        if self.has_reciprocal:
+            L.ref_reciprocal.argtypes = [_u64p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t, _szp,
+                                         C.POINTER(C.c_int64)]
+            L.ref_reciprocal.restype = C.c_int
         self.has_fast_pow = hasattr(L, "ref_fast_pow")
         if self.has_fast_pow:
             L.ref_fast_pow.argtypes = [C.c_uint64, C.c_uint32, _u32p, C.c_size_t, _szp]
@@ -176,6 +181,19 @@ class Reference(_Lib):
 
     def mul_digits(self, a, b=None, output_precision: int = 0, point_pos: int | None = None):
         return _mul_digits(self.lib.ref_mul_digits, a, b, output_precision, point_pos)
+
+    def reciprocal_digits(self, leaves, precision: int):
+        """BigFloat(prod(leaves)).reciprocal(precision): (digits, point_pos)."""
+        leaves = _limbs(leaves)
+        n = C.c_size_t(0)
+        pp = C.c_int64(0)
+        cap = 4 * int(precision) + 64  # Newton's last step may leave up to ~2x precision digits
+        out = np.zeros(cap, dtype=np.uint32)
+        rc = self.lib.ref_reciprocal(_p64(leaves), leaves.size, int(precision), _p32(out), cap, C.byref(n),
+                                     C.byref(pp))
+        if rc != 0:
+            raise OracleError(f"ref_reciprocal returned {rc}")
+        return out[: n.value].copy(), int(pp.value)
 
     def fast_pow_digits(self, base: int, exponent: int) -> np.ndarray:
         """fast_pow(BigInt(base), exponent) as reference 28-bit Digits."""

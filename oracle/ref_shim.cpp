@@ -13,6 +13,7 @@
 //   ref_mul_digits  -> bigint::mul::mul_digits    include/bigint/mul.h:223
 //   ref_product_tree-> BigInt::operator* (bigint.h:284) over a pairwise tree
 //   ref_fast_pow    -> bigint::fast_pow<BigInt>   include/bigint/bigint_base.h:60
+//   ref_reciprocal  -> BigFloat::reciprocal       src/bigint.cpp:1044 (Newton, BigFloat::mul)
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -120,6 +121,19 @@ int ref_product_tree(const uint64_t* leaves, size_t n, uint32_t* out, size_t cap
         return 0;
     }
     return copy_out32(level[0].get_data(), out, cap, out_len);
+}
+
+// 1 / x to `precision` digits for x = the product of `n` u64 leaves (built
+// with BigInt::operator*, as ref_product_tree): the Newton iteration of
+// BigFloat::reciprocal, whose products go through BigFloat::mul -> mul_digits.
+// Returns the digits and the point position of the reciprocal.
+int ref_reciprocal(const uint64_t* leaves, size_t n, size_t precision, uint32_t* out, size_t cap,
+                   size_t* out_len, int64_t* point_pos) {
+    bigint::BigInt x(1);
+    for (size_t i = 0; i < n; ++i) x *= bigint::BigInt(leaves[i]);
+    const bigint::BigFloat r = bigint::BigFloat(x).reciprocal(precision);
+    *point_pos = r.get_point_pos();
+    return copy_out32(r.get_data(), out, cap, out_len);
 }
 
 // fast_pow over BigInt, as the reference's benchmark example calls it

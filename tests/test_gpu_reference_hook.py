@@ -46,3 +46,16 @@ def test_fast_pow(bb, reference, reference_gpu):
         pytest.skip("reference shim without fast_pow")
     assert np.array_equal(reference_gpu.fast_pow_digits(1234567, 100003),
                           reference.fast_pow_digits(1234567, 100003))
+
+
+@pytest.mark.parametrize("nleaves,prec", [(1024, 500), (1024, 50000), (16384, 200000)])
+def test_bigfloat_reciprocal(bb, reference, reference_gpu, nleaves, prec):
+    """BigFloat::reciprocal's Newton iteration (src/bigint.cpp:1044-1071):
+    its BigFloat::mul products go through mul_digits -> _mul -> the hook."""
+    if not reference.has_reciprocal:
+        pytest.skip("reference shim without reciprocal")
+    rng = np.random.default_rng(SEED + 93 + nleaves)
+    leaves = rng.integers(1 << 32, 2**64, nleaves, dtype=np.uint64, endpoint=False)
+    dg, pg = reference_gpu.reciprocal_digits(leaves, prec)
+    dr, pr = reference.reciprocal_digits(leaves, prec)
+    assert pg == pr and np.array_equal(dg, dr)
