@@ -372,6 +372,47 @@ def fft_form(bb, torch, device, reps: int = 3):
     return rows
 
 
+def mul_digits_form(bb, port, cpu: bool = True, reps: int = 20):
+    """The reference's main seam at the headline size: mul_digits on 28-bit
+    Digits (BigInt::operator*, include/bigint/bigint.h:289) of two 2^24-bit
+    numbers (599186 digits each) through the host API bgpu_mul_digits (H2D
+    of both operands, the kernels reading and writing Digits directly, D2H of
+    the product), wall clock; the reference's own mul_digits on the host cores
+    beside it (one run)."""
+    rng = np.random.default_rng(SEED + 6)
+    nd = -(-(1 << 24) // 28)
+    a = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
+    b = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
+    a[-1] |= np.uint32(1 << 27)
+    b[-1] |= np.uint32(1 << 27)
+    bb.mul_digits(a, b)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        got = bb.mul_digits(a, b)
+    el = (time.perf_counter() - t0) / reps
+    res = {"digits_per_operand": nd, "ms": el * 1e3, "products_per_s": 1.0 / el,
+           "api": "bgpu_mul_digits (host buffers)"}
+    from oracle.pyoracle import Reference, have_reference
+
+    if cpu and have_reference():
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        t0 = time.perf_counter()
+        want = ref.mul_digits(a, b)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                "call": "bigint::mul::mul_digits"}
+        if not np.array_equal(got, want):
+            raise SystemExit("bench mul_digits: product differs from the reference")
+        res["verified"] = "identical to the reference's mul_digits"
+    else:
+        M = (1 << 61) - 1
+        if port.mod_m61(digits28_to_limbs_np(a)) * port.mod_m61(digits28_to_limbs_np(b)) % M != \
+                port.mod_m61(digits28_to_limbs_np(got)):
+            raise SystemExit("bench mul_digits: residue check failed")
+        res["verified"] = "residue mod 2^61-1"
+    return res
+
+
 def digits28_to_limbs_np(d) -> np.ndarray:
     """Little-endian 28-bit digits -> u64 limbs (vectorised bit repacking)."""
     d = np.ascontiguousarray(d, dtype=np.uint32)
@@ -731,6 +772,7 @@ def run_gpu_arm(args) -> None:
                  "ntt_size_sweep": sweep_form(bb, torch, device, port),
                  "fp64_fft": fft_form(bb, torch, device),
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
+                 "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
                                                 cpu=(rank == 0 and not args.no_cpu_baseline))}
@@ -775,7 +817,8 @@ def run_gpu_arm(args) -> None:
     print(json.dumps(line))
 
 
-FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "batched_4096", "product_tree_2p20")
+FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "batched_4096",
+         "product_tree_2p20")
 
 
 def run_single_form(args) -> None:
@@ -800,6 +843,8 @@ def run_single_form(args) -> None:
         res = fft_form(bb, torch, device)
     elif name == "fast_pow":
         res = fast_pow_form(bb, port, cpu=not args.no_cpu_baseline)
+    elif name == "mul_digits_2p24":
+        res = mul_digits_form(bb, port, cpu=not args.no_cpu_baseline)
     elif name == "batched_4096":
         res = batched_form(bb, torch, device, port)
     else:
