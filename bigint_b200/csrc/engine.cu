@@ -69,6 +69,7 @@ void release_locked() {
     if (g.device < 0) return;
     cudaSetDevice(g.device);
     if (g.stream) cudaStreamSynchronize(g.stream);
+    release_host_staging();
     for (auto t : g.d_tables) cudaFree(t);
     cudaFree(g.d_fft_tables);
     cudaFree(g.d_fft_err);
@@ -384,9 +385,9 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
     uint64_t* db = square ? da : reinterpret_cast<uint64_t*>(io + b_off);
     uint64_t* dout = reinterpret_cast<uint64_t*>(io + o_off);
     cudaStream_t st = g.stream;
-    cudaError_t e = cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, b, nb * 8, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_status(e);
+    rc = host_to_device(da, a, na * 8, st, nullptr);
+    if (rc == BGPU_OK && !square) rc = host_to_device(db, b, nb * 8, st, nullptr);
+    if (rc != BGPU_OK) return rc;
     if (stats) cudaEventRecord(g.ev0, st);
     int fbits = 0, flog = 0;
     const bool want_fft = ((flags & BGPU_METHOD_MASK) == BGPU_METHOD_FFT || auto_fft(flags, na, nb)) &&
@@ -425,9 +426,8 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
         tmp.resize(nout);
         dst = tmp.data();
     }
-    e = cudaMemcpyAsync(dst, dout, nout * 8, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_status(e);
-    rc = check_device_error(BGPU_OK);
+    rc = device_to_host(dst, dout, nout * 8, st);
+    rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
     if (stats) cudaEventElapsedTime(&stats->device_ms, g.ev0, g.ev1);
     const size_t n = strip64(dst, nout);
@@ -518,8 +518,9 @@ int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64
     uint64_t* bufb[2] = {reinterpret_cast<uint64_t*>(io), reinterpret_cast<uint64_t*>(io + bsz)};
     uint64_t* bufr[2] = {reinterpret_cast<uint64_t*>(io + 2 * bsz), reinterpret_cast<uint64_t*>(io + 2 * bsz + rsz)};
     cudaStream_t st = g.stream;
-    cudaError_t e = cudaMemcpyAsync(bufb[0], base, nbase * 8, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_status(e);
+    rc = host_to_device(bufb[0], base, nbase * 8, st, nullptr);
+    if (rc != BGPU_OK) return rc;
+    cudaError_t e = cudaSuccess;
     int cb = 0, cr = 0;
     uint64_t bb = bbits, rb = 0;
     uint32_t nl = 0;
@@ -549,9 +550,8 @@ int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64
         tmp.resize(rlimbs);
         dst = tmp.data();
     }
-    e = cudaMemcpyAsync(dst, bufr[cr], rlimbs * 8, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_status(e);
-    rc = check_device_error(BGPU_OK);
+    rc = device_to_host(dst, bufr[cr], rlimbs * 8, st);
+    rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
     const size_t n = strip64(dst, rlimbs);
     *out_len = n;
@@ -667,11 +667,6 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     const uint32_t* pa = a + off_a;
     const uint32_t* pb = b + off_b;
     size_t la = strip32(pa, na - off_a), lb = square ? la : strip32(pb, nb - off_b);
-    for (size_t i = 0; i < la; ++i)
-        if (pa[i] >> 28) return BGPU_ERR_INVALID_ARG;
-    if (!square)
-        for (size_t i = 0; i < lb; ++i)
-            if (pb[i] >> 28) return BGPU_ERR_INVALID_ARG;
     const size_t nres = la + lb + 1;  // 28-bit digits of the product, with margin
     if (nres > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
     const size_t la64 = (la * 28 + 63) / 64, lb64 = (lb * 28 + 63) / 64;
@@ -686,9 +681,16 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     uint32_t* db = square ? da : reinterpret_cast<uint32_t*>(io + b_off);
     uint32_t* dres = reinterpret_cast<uint32_t*>(io + o_off);
     cudaStream_t st = g.stream;
-    cudaError_t e = cudaMemcpyAsync(da, pa, la * 4, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess && !square) e = cudaMemcpyAsync(db, pb, lb * 4, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_status(e);
+    // the 28-bit check rides on the copies; nothing is launched before it
+    bool ok_a = true, ok_b = true;
+    rc = host_to_device(da, pa, la * 4, st, &ok_a);
+    if (rc == BGPU_OK && !square) rc = host_to_device(db, pb, lb * 4, st, &ok_b);
+    if (rc != BGPU_OK) return rc;
+    if (!ok_a || !ok_b) {
+        cudaStreamSynchronize(st);  // a page-locked source may still be in flight
+        return BGPU_ERR_INVALID_ARG;
+    }
+    cudaError_t e = cudaSuccess;
     if (stats) cudaEventRecord(g.ev0, st);
     if (const uint32_t sm = small_method(flags, la64, lb64)) {
         uint64_t* la_d = reinterpret_cast<uint64_t*>(io + l_off);
@@ -719,9 +721,8 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
         tmp.resize(nres);
         dst = tmp.data();
     }
-    e = cudaMemcpyAsync(dst, dres, nres * 4, cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_status(e);
-    rc = check_device_error(BGPU_OK);
+    rc = device_to_host(dst, dres, nres * 4, st);
+    rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
     if (stats) cudaEventElapsedTime(&stats->device_ms, g.ev0, g.ev1);
     size_t n = strip32(dst, nres);
@@ -938,8 +939,8 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
     if (rc != BGPU_OK) return rc;
     uint64_t* dl = static_cast<uint64_t*>(g.d_io);
     uint64_t* dout = reinterpret_cast<uint64_t*>(static_cast<char*>(g.d_io) + align256(n * 8));
-    cudaError_t e = cudaMemcpyAsync(dl, leaves, n * 8, cudaMemcpyHostToDevice, g.stream);
-    if (e != cudaSuccess) return cuda_status(e);
+    rc = host_to_device(dl, leaves, n * 8, g.stream, nullptr);
+    if (rc != BGPU_OK) return rc;
     uint32_t nl = 0;
     rc = product_tree_device(dl, n, dout, width, hooks_locked(), &g.tree, g.stream, &nl);
     g.last_launches = nl;
@@ -950,9 +951,8 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
         tmp.resize(width);
         dst = tmp.data();
     }
-    e = cudaMemcpyAsync(dst, dout, width * 8, cudaMemcpyDeviceToHost, g.stream);
-    if (e != cudaSuccess) return cuda_status(e);
-    rc = check_device_error(BGPU_OK);
+    rc = device_to_host(dst, dout, width * 8, g.stream);
+    rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
     const size_t len = strip64(dst, width);
     *out_len = len;

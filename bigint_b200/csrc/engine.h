@@ -217,4 +217,15 @@ cudaError_t launch_digits28_to_limbs(const uint32_t* d, uint32_t nd, uint64_t* l
 cudaError_t launch_limbs_to_digits28(const uint64_t* limbs, uint32_t nlimbs, uint32_t* d,
                                      uint32_t nd, cudaStream_t stream);
 
+// Host <-> device copies of the host API: page-locked caller memory goes
+// straight to the copy engines, pageable memory through a ring of
+// page-locked slots filled by a pool of host threads.  host_to_device may
+// return before the copy has finished: a page-locked source must stay
+// unchanged until the stream has passed the copy, a pageable one is free at
+// once.  With digits_ok it also checks that every 32-bit word is below 2^28.
+// device_to_host returns once the bytes are in dst.
+int host_to_device(void* dst, const void* src, size_t bytes, cudaStream_t st, bool* digits_ok);
+int device_to_host(void* dst, const void* src, size_t bytes, cudaStream_t st);
+void release_host_staging();
+
 }  // namespace bgpu
