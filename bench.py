@@ -375,16 +375,17 @@ def fft_form(bb, torch, device, reps: int = 3):
 def mul_digits_form(bb, port, cpu: bool = True, reps: int = 20):
     """The reference's main seam at the headline size: mul_digits on 28-bit
     Digits (BigInt::operator*, include/bigint/bigint.h:289) of two 2^24-bit
-    numbers (599186 digits each) through the host API bgpu_mul_digits (H2D
+    numbers (599187 digits each) through the host API bgpu_mul_digits (H2D
     of both operands, the kernels reading and writing Digits directly, D2H of
     the product), wall clock; the reference's own mul_digits on the host cores
     beside it (one run)."""
     rng = np.random.default_rng(SEED + 6)
     nd = -(-(1 << 24) // 28)
+    top = (1 << 24) - 28 * (nd - 1)  # bits in the top digit: exactly 2^24 bits in all
     a = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
     b = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
-    a[-1] |= np.uint32(1 << 27)
-    b[-1] |= np.uint32(1 << 27)
+    for x in (a, b):
+        x[-1] = (x[-1] & np.uint32((1 << top) - 1)) | np.uint32(1 << (top - 1))
     bb.mul_digits(a, b)
     t0 = time.perf_counter()
     for _ in range(reps):

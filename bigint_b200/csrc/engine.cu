@@ -294,6 +294,11 @@ size_t strip32(const uint32_t* x, size_t n) {
     return n;
 }
 
+// Bit length of n >= 1 28-bit digits whose top digit is nonzero.
+uint64_t bits28(const uint32_t* d, size_t n) {
+    return 28 * (uint64_t)(n - 1) + (32 - __builtin_clz(d[n - 1]));
+}
+
 // Bits per FFT point.  Worst-case mode: the largest b in [8, 20] with
 //   2b <= 46 - L - log2(L + 1),   L = log2 of the transform length,
 // which keeps the error of every coefficient below 1/4 by Percival's bound for
@@ -707,8 +712,11 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
         g.last_launches = square ? 3 : 4;
         if (stats) stats->method = (int32_t)sm;
     } else {
-        OperandDesc oa{da, (uint32_t)la, (uint32_t)((la * 28 + 31) / 32), kFmtDigit28};
-        OperandDesc ob{db, (uint32_t)lb, (uint32_t)((lb * 28 + 31) / 32), kFmtDigit28};
+        // 32-bit digit counts from the true bit lengths: a number of exactly
+        // 2^k bits has ceil(2^k / 28) digits, whose 28 * digits overshoots 2^k
+        // and would double the transform
+        OperandDesc oa{da, (uint32_t)la, (uint32_t)((bits28(pa, la) + 31) / 32), kFmtDigit28};
+        OperandDesc ob{db, (uint32_t)lb, (uint32_t)((bits28(pb, lb) + 31) / 32), kFmtDigit28};
         rc = multiply_device(oa, ob, square, dres, kFmtDigit28, nres, flags, st, stats);
     }
     if (rc != BGPU_OK) return rc;

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdint>
 #include <cstring>
@@ -35,18 +36,29 @@ constexpr size_t kSlot = 4 << 20;         // bytes of one page-locked slot
 constexpr int kSlots = 4;                 // slots in the ring
 constexpr size_t kDirectMax = 256 << 10;  // pageable copies up to this go to the driver
 constexpr unsigned kMaxWorkers = 16;
+constexpr auto kSpin = std::chrono::microseconds(200);  // idle workers poll this long before sleeping
+
+inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+    __builtin_ia32_pause();
+#else
+    std::this_thread::yield();
+#endif
+}
 
 // Fixed pool of host threads running index-parallel jobs.  The calling thread
 // takes part, so a job finishes even with no worker running (after fork()).
 // The job counter carries the job's generation in its high half: a worker
 // that picked up an older job's parameters never claims an index of a newer
-// one.
+// one.  One call of the host API runs several jobs back to back (operand
+// copies, then the result's), so an idle worker polls for the next job for a
+// short while before it sleeps on the condition variable.
 class Pool {
   public:
     ~Pool() {
         {
             std::lock_guard<std::mutex> lk(mu_);
-            stop_ = true;
+            stop_.store(true);
         }
         cv_.notify_all();
         for (auto& t : threads_) t.join();
@@ -64,6 +76,7 @@ class Pool {
             n_ = n;
             done_.store(0, std::memory_order_relaxed);
             next_.store((uint64_t)gen << 32, std::memory_order_release);
+            pub_.store(gen, std::memory_order_release);
         }
         if (n > 1) cv_.notify_all();
         work(gen, n, fn, ctx);
@@ -95,10 +108,15 @@ class Pool {
             uint32_t gen, n;
             void (*fn)(void*, uint32_t);
             void* ctx;
+            const auto t0 = std::chrono::steady_clock::now();
+            for (uint32_t i = 1; pub_.load(std::memory_order_acquire) == seen && !stop_.load(); ++i) {
+                cpu_relax();
+                if ((i & 255) == 0 && std::chrono::steady_clock::now() - t0 > kSpin) break;
+            }
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
-                if (stop_) return;
+                cv_.wait(lk, [&] { return stop_.load() || gen_ != seen; });
+                if (stop_.load()) return;
                 seen = gen = gen_;
                 fn = fn_;
                 ctx = ctx_;
@@ -112,8 +130,9 @@ class Pool {
     bool started_ = false;
     std::mutex mu_;
     std::condition_variable cv_;
-    bool stop_ = false;
-    uint32_t gen_ = 0;
+    std::atomic<bool> stop_{false};
+    uint32_t gen_ = 0;                 // written under mu_
+    std::atomic<uint32_t> pub_{0};     // gen_, for the polling workers
     void (*fn_)(void*, uint32_t) = nullptr;
     void* ctx_ = nullptr;
     uint32_t n_ = 0;

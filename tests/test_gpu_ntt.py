@@ -121,6 +121,27 @@ def test_digits_random_vs_port(bb, port):
         assert np.array_equal(bb.mul_digits(a), port.mul_digits(a))
 
 
+def test_digits_transform_sized_by_bit_length(bb, port):
+    """Digits of exactly 2^k bits (ceil(2^k / 28) digits, the top one short)
+    take the same transform as 2^k-bit u64 limbs; top digits one bit longer
+    take the next one.  Products exact either way."""
+    rng = np.random.default_rng(SEED + 16)
+    for k in (16, 20):
+        nd = -(-(1 << k) // 28)
+        top = (1 << k) - 28 * (nd - 1)
+        a, b = rand_digits(rng, nd), rand_digits(rng, nd)
+        for x in (a, b):
+            x[-1] = (x[-1] & np.uint32((1 << top) - 1)) | np.uint32(1 << (top - 1))
+        got, st = bb.mul_digits(a, b, method=bb.BGPU_METHOD_NTT, stats=True)
+        assert st.log2_points == k - 4, (k, st.log2_points)
+        assert np.array_equal(got, port.mul_digits(a, b)), k
+        a[-1] |= np.uint32(1 << top)  # both 2^k + 1 bits: 2^(k-5) + 1 words each
+        b[-1] |= np.uint32(1 << top)
+        got, st = bb.mul_digits(a, b, method=bb.BGPU_METHOD_NTT, stats=True)
+        assert st.log2_points == k - 3, (k, st.log2_points)
+        assert np.array_equal(got, port.mul_digits(a, b)), k
+
+
 def test_headline_size_vs_port(bb, port):
     """2^24 x 2^24-bit product (the bench workload) limb-exact."""
     rng = np.random.default_rng(SEED + 15)
