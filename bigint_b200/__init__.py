@@ -14,6 +14,7 @@ this package           reference                                       C-ABI
 ``mul_digits(a, b,``   ``bigint::mul::mul_digits`` (mul.h:223-318)     ``bgpu_mul_digits``
 ``  precision, pos)``
 ``fast_pow(base, e)``  ``fast_pow<BigInt>`` (bigint_base.h:60-69)      ``bgpu_pow_u64``
+``reciprocal_digits``  ``BigFloat::reciprocal`` (bigint.cpp:1044-1071) ``bgpu_reciprocal_digits``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
 =====================  ==============================================  =========================
 
@@ -63,6 +64,7 @@ from ._lib import (  # noqa: F401
     fast_pow,
     product_tree,
     product_tree_device,
+    reciprocal_digits,
     set_batch_split,
     set_split,
     set_kernel_timing,

@@ -102,6 +102,9 @@ def _load() -> C.CDLL:
     L.bgpu_mul_u64_many.restype = C.c_int
     L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]
     L.bgpu_pow_u64.restype = C.c_int
+    L.bgpu_reciprocal_digits.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, u32p,
+                                         C.c_size_t, szp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.bgpu_reciprocal_digits.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_uint32, C.c_void_p]
     L.bgpu_mul_u64_device.restype = C.c_int
@@ -375,6 +378,33 @@ def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = Non
     if stats:
         return ret, _stats(st)
     return ret
+
+
+def reciprocal_digits(digits, point_pos: int = 0, neg: bool = False, precision: int = 0):
+    """``BigFloat::reciprocal(precision)`` (src/bigint.cpp:1044-1071) on the GPU.
+
+    The input is a BigFloat's fields: 28-bit Digits without a leading zero
+    digit, the point position (value = digits * 2^(-28 point_pos)) and the
+    sign.  Returns ``(digits, point_pos, neg)`` of the reciprocal, identical to
+    the reference's.  Every step of the Newton iteration keeps its digits on
+    the device (``bgpu_reciprocal_digits``)."""
+    _ensure_init()
+    d = _as_digits(digits)
+    if d.size == 0:
+        raise BigIntGPUError(-1, "bgpu_reciprocal_digits (empty input)")
+    u32p = C.POINTER(C.c_uint32)
+    cap = 4 * max(int(precision), d.size) + 64
+    for _ in range(2):
+        out = np.empty(cap, dtype=np.uint32)
+        n, pp, ng = C.c_size_t(0), C.c_int64(0), C.c_int(0)
+        rc = lib.bgpu_reciprocal_digits(d.ctypes.data_as(u32p), d.size, int(point_pos), int(bool(neg)),
+                                        int(precision), out.ctypes.data_as(u32p), cap, C.byref(n),
+                                        C.byref(pp), C.byref(ng))
+        if rc != -5:
+            break
+        cap = n.value
+    _check(rc, "bgpu_reciprocal_digits")
+    return out[: n.value], int(pp.value), bool(ng.value)
 
 
 def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, stream: int = 0,

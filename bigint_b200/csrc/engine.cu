@@ -5,6 +5,7 @@
 //   bgpu_mul_u64     <- bigint::mul::_mul / ntt::mul   (include/bigint/mul.h:208-220,
 //                                                       src/mul/ntt_multithread.cpp:444-530)
 //   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
+//   bgpu_reciprocal_digits <- BigFloat::reciprocal      (src/bigint.cpp:1044-1071)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -44,6 +45,9 @@ struct Engine {
     void* d_io = nullptr;
     size_t io_bytes = 0;
     TreeArena tree;  // product-tree values, descriptors and scratch
+    // digit buffers of the device-resident reciprocal (one per live value)
+    uint32_t* rs[11] = {};
+    size_t rs_bytes[11] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t last_launches = 0;
     // optional per-kernel timing of NTT products: a ring of event sets, one
@@ -78,6 +82,7 @@ void release_locked() {
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
     cudaFree(g.tree.ptr);
+    for (auto p : g.rs) cudaFree(p);
     if (g.ev0) cudaEventDestroy(g.ev0);
     if (g.ev1) cudaEventDestroy(g.ev1);
     for (auto e : g.kev) cudaEventDestroy(e);
@@ -752,6 +757,431 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     return BGPU_OK;
 }
 
+
+// ---- device-resident BigFloat::reciprocal ----------------------------------
+//
+// The reference's Newton iteration (src/bigint.cpp:1044-1071):
+//   b = *this >> exponent, tail zeros removed (b in [1/2, 1));
+//   x = BigFloat(1 / b.to_double());
+//   while (cur < precision) { cur *= 2;
+//       x += mul(x, one - mul(b, x, cur + 1), cur + 1); }
+//   return x >> exponent;
+// replayed step by step with every value's digits on the device.  The host
+// keeps what the reference's control flow reads -- each value's length, point
+// position, sign, bottom zeros and top digit -- and gets it back after each
+// step from the extent kernel (four words); the digit work runs in device
+// kernels: truncated products (BigFloat::mul -> mul_digits) on the NTT or the
+// small-product kernels, frame additions and subtractions (add_or_sub) and
+// shifts.  Only the starting value 1 / b.to_double() (two or three digits)
+// is formed on the host, from b's top three digits, as the reference does.
+
+enum RecipSlot { kRsIn, kRsB, kRsX0, kRsX1, kRsT1, kRsT2, kRsT3, kRsOut, kRsScratch, kRsSmall, kRsOne };
+
+constexpr uint32_t kDigitMask = (1u << 28) - 1u;
+
+struct DVal {
+    const uint32_t* d = nullptr;  // d[0..n); the zero value is {0} and has no digits on the device
+    size_t n = 1;
+    int64_t pp = 0;               // point position: value = digits * 2^(-28 pp)
+    bool neg = false;
+    size_t tz = 0;                // zero digits at the bottom
+    uint32_t top = 0;             // d[n-1]
+    int slot = -1;                // buffer holding the digits (-1: none)
+    bool zero() const { return n == 1 && top == 0; }
+};
+
+uint32_t* rslot(int k, size_t words, int* rc) {
+    *rc = ensure(reinterpret_cast<void**>(&g.rs[k]), &g.rs_bytes[k], std::max<size_t>(words, 4) * 4);
+    return *rc == BGPU_OK ? g.rs[k] : nullptr;
+}
+
+// Runs what is queued and reads `count` words back.
+int read_back(const uint32_t* d, uint32_t* h, size_t count) {
+    cudaError_t e = cudaMemcpyAsync(h, d, count * 4, cudaMemcpyDeviceToHost, g.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+    return check_device_error(cuda_status(e));
+}
+
+// The four-word result block of the compare and extent kernels, zeroed.
+int result_block(unsigned long long** dr) {
+    int rc;
+    uint32_t* p = rslot(kRsSmall, 8, &rc);
+    if (rc != BGPU_OK) return rc;
+    *dr = reinterpret_cast<unsigned long long*>(p);
+    return cuda_status(cudaMemsetAsync(p, 0, 4 * sizeof(unsigned long long), g.stream));
+}
+
+// Queues the extent kernel into the block, runs everything queued and reads
+// the block back: r[0] = highest nonzero index + 1 (0: all zero), r[1], r[2] =
+// lowest nonzero index >= from0, from1 (0xffffffff: none), r[3] = the digit
+// at r[0] - 1; *cmp (if given) = the compare word.
+int extent(unsigned long long* dr, const uint32_t* d, size_t n, size_t from0, size_t from1, uint32_t r[4],
+           unsigned long long* cmp = nullptr) {
+    cudaError_t e = launch_extent(d, (uint32_t)n, (uint32_t)std::min<size_t>(from0, UINT32_MAX),
+                                  (uint32_t)std::min<size_t>(from1, UINT32_MAX), dr, g.stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    unsigned long long h[4];
+    e = cudaMemcpyAsync(h, dr, sizeof(h), cudaMemcpyDeviceToHost, g.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
+    const int rc = check_device_error(cuda_status(e));
+    if (rc != BGPU_OK) return rc;
+    r[0] = (uint32_t)(h[0] >> 32);
+    r[3] = (uint32_t)h[0];
+    r[1] = h[1] ? (uint32_t)((1ull << 32) - h[1]) : 0xffffffffu;
+    r[2] = h[2] ? (uint32_t)((1ull << 32) - h[2]) : 0xffffffffu;
+    if (cmp) *cmp = h[3];
+    return BGPU_OK;
+}
+
+// BigFloat::shift (src/bigint.cpp:769-789): the point moves by whole digits
+// (C++ division, truncating toward zero), the remaining bits by a right shift
+// when the bottom digit has that many zero bits, else by a left shift.
+struct ShiftPlan {
+    int64_t pp;
+    int mode;  // 0 none, 1 right by s, 2 left by s
+    uint32_t s;
+};
+
+ShiftPlan plan_shift(int64_t pp, int64_t offset, uint32_t low) {
+    pp -= offset / 28;
+    int64_t off = offset % 28;
+    if (off == 0) return {pp, 0, 0};
+    if (off > 0) {
+        off = 28 - off;
+        --pp;
+    } else {
+        off = -off;
+    }
+    const int64_t ctz = low ? __builtin_ctz(low) : 32;
+    if (ctz >= off) return {pp, 1, (uint32_t)off};
+    return {pp + 1, 2, (uint32_t)(28 - off)};
+}
+
+// The same on a short host vector (the double-derived starting value).
+void host_shift(std::vector<uint32_t>& v, int64_t* pp, bool* neg, int64_t offset) {
+    const ShiftPlan sp = plan_shift(*pp, offset, v[0]);
+    *pp = sp.pp;
+    const size_t n = v.size();
+    if (sp.mode == 1) {
+        for (size_t i = 0; i + 1 < n; ++i) v[i] = ((v[i] >> sp.s) | (v[i + 1] << (28 - sp.s))) & kDigitMask;
+        v[n - 1] >>= sp.s;
+    } else if (sp.mode == 2) {
+        v.push_back(0);
+        for (size_t i = n; i > 0; --i) v[i] = ((v[i] << sp.s) | (v[i - 1] >> (28 - sp.s))) & kDigitMask;
+        v[0] = (v[0] << sp.s) & kDigitMask;
+    }
+    size_t i = v.size();
+    while (i > 1 && v[i - 1] == 0) --i;
+    v.resize(i);
+    if (i == 1 && v[0] == 0) {  // reset()
+        *pp = 0;
+        *neg = false;
+    }
+}
+
+// BigFloat::to_double (src/bigint.cpp:717-766) from the top k <= 3 digits
+// t[0..k) of an n-digit value (t[k-1] = top); b in [1/2, 1) needs at most two
+// digits below the top.
+double to_double_top(const uint32_t* t, size_t k, size_t n, int64_t pp, bool neg, bool* ok) {
+    auto dig = [&](size_t i) { return (uint64_t)t[i - (n - k)]; };
+    auto shl = [](uint64_t x, int64_t r) { return r < 0 ? x >> (-r) : x << r; };
+    const uint32_t top = t[k - 1];
+    const int64_t hbw = 32 - __builtin_clz(top);
+    const int64_t exponent = 28 * ((int64_t)n - 1 - pp) + hbw - 1;
+    int64_t eb = exponent + 1023;
+    *ok = true;
+    if (eb >= 2047) return neg ? -HUGE_VAL : HUGE_VAL;
+    int64_t offset;
+    uint64_t mant;
+    if (eb <= 0) {
+        if (exponent < -52 - 1023 + 1) return neg ? -0.0 : 0.0;
+        eb = 0;
+        offset = exponent + 52 + 1023 - hbw;
+        mant = shl(top, offset);
+    } else {
+        offset = 52 - (hbw - 1);
+        mant = shl(top & ((1u << (hbw - 1)) - 1), offset);
+    }
+    size_t i = n - 1;
+    while (offset > 0 && i > 0) {
+        offset -= 28;
+        --i;
+        if (i < n - k) {  // needs more than the top three digits
+            *ok = false;
+            return 0.0;
+        }
+        mant |= shl(dig(i), offset);
+    }
+    const uint64_t bits = ((uint64_t)neg << 63) | ((uint64_t)eb << 52) | mant;
+    double r;
+    memcpy(&r, &bits, sizeof(r));
+    return r;
+}
+
+// BigFloat::BigFloat(double) (src/bigint.cpp:681-715) for finite nonzero v.
+void double_to_digits(double v, std::vector<uint32_t>* d, int64_t* pp, bool* neg) {
+    uint64_t raw;
+    memcpy(&raw, &v, sizeof(raw));
+    *pp = 0;
+    *neg = (raw >> 63) != 0;
+    const int64_t eb = (int64_t)((raw >> 52) & 2047);
+    uint64_t base = raw & ((1ull << 52) - 1);
+    int64_t offset = -52 - 1023;
+    if (eb == 0) {
+        offset += 1;
+    } else {
+        base |= 1ull << 52;
+        offset += eb;
+    }
+    d->clear();
+    while (base) {
+        d->push_back((uint32_t)base & kDigitMask);
+        base >>= 28;
+    }
+    host_shift(*d, pp, neg, offset);
+}
+
+// *out = in shifted as BigFloat::shift(offset) does, into `slot`.
+int shift_val(const DVal& in, int64_t offset, int slot, DVal* out) {
+    uint32_t low = 0;
+    int rc = read_back(in.d, &low, 1);
+    if (rc != BGPU_OK) return rc;
+    const ShiftPlan sp = plan_shift(in.pp, offset, low);
+    *out = in;
+    out->pp = sp.pp;
+    if (sp.mode == 0) return BGPU_OK;  // whole digits: only the point moves
+    const size_t nout = in.n + (sp.mode == 2 ? 1 : 0);
+    uint32_t* o = rslot(slot, nout, &rc);
+    if (rc != BGPU_OK) return rc;
+    unsigned long long* dr = nullptr;
+    rc = cuda_status(launch_shift_digits(in.d, (uint32_t)in.n, sp.s, sp.mode == 2, o, g.stream));
+    if (rc == BGPU_OK) rc = result_block(&dr);
+    uint32_t r[4];
+    if (rc == BGPU_OK) rc = extent(dr, o, nout, 0, 0, r);
+    if (rc != BGPU_OK) return rc;
+    if (r[0] == 0) return BGPU_ERR_CUDA;  // a nonzero value cannot shift to zero
+    out->d = o;
+    out->n = r[0];
+    out->tz = r[1];
+    out->top = r[3];
+    out->slot = slot;
+    return BGPU_OK;
+}
+
+// Product of the device digit ranges a.d[off_a..a.n) and b.d[off_b..b.n)
+// into nres digits at dres, by the method the host API would use.
+int digits_product(const DVal& a, size_t off_a, const DVal& b, size_t off_b, uint32_t* dres, size_t nres) {
+    const uint32_t* pa = a.d + off_a;
+    const uint32_t* pb = b.d + off_b;
+    const size_t la = a.n - off_a, lb = b.n - off_b;
+    const size_t la64 = (la * 28 + 63) / 64, lb64 = (lb * 28 + 63) / 64;
+    cudaStream_t st = g.stream;
+    if (const uint32_t sm = small_method(BGPU_METHOD_AUTO, la64, lb64)) {
+        int rc;
+        uint32_t* scr = rslot(kRsScratch, 2 * ((la64 + 1) + (lb64 + 1) + (la64 + lb64)), &rc);
+        if (rc != BGPU_OK) return rc;
+        uint64_t* la_d = reinterpret_cast<uint64_t*>(scr);
+        uint64_t* lb_d = la_d + la64 + 1;
+        uint64_t* lo_d = lb_d + lb64 + 1;
+        cudaError_t e = launch_digits28_to_limbs(pa, (uint32_t)la, la_d, (uint32_t)la64, st);
+        if (e == cudaSuccess) e = launch_digits28_to_limbs(pb, (uint32_t)lb, lb_d, (uint32_t)lb64, st);
+        rc = cuda_status(e);
+        if (rc == BGPU_OK) rc = launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st);
+        if (rc == BGPU_OK)
+            rc = cuda_status(launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st));
+        return rc;
+    }
+    const uint64_t bits_a = 28 * (uint64_t)(la - 1) + (32 - __builtin_clz(a.top));
+    const uint64_t bits_b = 28 * (uint64_t)(lb - 1) + (32 - __builtin_clz(b.top));
+    OperandDesc oa{pa, (uint32_t)la, (uint32_t)((bits_a + 31) / 32), kFmtDigit28};
+    OperandDesc ob{pb, (uint32_t)lb, (uint32_t)((bits_b + 31) / 32), kFmtDigit28};
+    return multiply_device(oa, ob, false, dres, kFmtDigit28, nres, BGPU_METHOD_AUTO, st, nullptr);
+}
+
+// BigFloat::mul(a, b, prec) (include/bigint/bigint.h:570-582) with the
+// truncation of mul_digits (include/bigint/mul.h:227-243, 301-312).  The
+// truncated operands keep any zero digits at their bottom: the product then
+// carries those zeros below its own digits, and the first nonzero digit at or
+// above the cut lands where the reference's cut and zero skip put it.
+int mul_trunc(const DVal& a, const DVal& b, size_t prec, int slot, DVal* out) {
+    if (a.zero() || b.zero()) {
+        *out = DVal{};
+        return BGPU_OK;
+    }
+    const size_t off_a = a.n > prec ? a.n - prec : 0, off_b = b.n > prec ? b.n - prec : 0;
+    const size_t la = a.n - off_a, lb = b.n - off_b;
+    const size_t nres = la + lb + 1;
+    if (nres > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    int rc;
+    uint32_t* dres = rslot(slot, nres, &rc);
+    if (rc != BGPU_OK) return rc;
+    unsigned long long* dr = nullptr;
+    rc = digits_product(a, off_a, b, off_b, dres, nres);
+    if (rc == BGPU_OK) rc = result_block(&dr);
+    if (rc != BGPU_OK) return rc;
+    // the product has la + lb - 1 or la + lb digits
+    const size_t n0 = la + lb - 1, n1 = la + lb;
+    uint32_t r[4];
+    rc = extent(dr, dres, nres, n0 > prec ? n0 - prec : 0, n1 > prec ? n1 - prec : 0, r);
+    if (rc != BGPU_OK) return rc;
+    const uint32_t first = r[0] == n0 ? r[1] : (r[0] == n1 ? r[2] : 0xffffffffu);
+    if (first >= r[0]) return BGPU_ERR_CUDA;
+    out->d = dres + first;
+    out->n = r[0] - first;
+    out->pp = a.pp + b.pp - (int64_t)(off_a + off_b + first);
+    out->neg = a.neg != b.neg;
+    out->tz = 0;
+    out->top = r[3];
+    out->slot = slot;
+    return BGPU_OK;
+}
+
+// BigFloat::add_or_sub (src/bigint.cpp:849-936): the exact sum or difference
+// in the reference's frame, then its leading and bottom zeros removed.
+int add_or_sub(const DVal& a, const DVal& b, bool is_sub, int slot, DVal* out) {
+    if (a.zero()) {
+        *out = b;
+        if (is_sub && !b.zero()) out->neg = !b.neg;
+        return BGPU_OK;
+    }
+    if (b.zero()) {
+        *out = a;
+        return BGPU_OK;
+    }
+    const int64_t len_a = (int64_t)a.n, len_b = (int64_t)b.n;
+    const int64_t pp_res = std::max(a.pp - (int64_t)a.tz, b.pp - (int64_t)b.tz);
+    const int64_t len_res = std::max(len_a - a.pp, len_b - b.pp) + pp_res;
+    if (len_res <= 0 || len_res >= ((int64_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    FrameOp f{a.d, pp_res - a.pp, (uint32_t)a.n, b.d, pp_res - b.pp, (uint32_t)b.n, (uint32_t)len_res, 0,
+              nullptr};
+    const bool sub = a.neg != (b.neg != is_sub);  // magnitudes subtract
+    const uint32_t L = (uint32_t)len_res, nblk = frame_blocks(L);
+    const size_t dig = (L + 1 + 63) & ~(size_t)63;
+    int rc;
+    uint32_t* o = rslot(slot, dig + 2 * (size_t)nblk, &rc);
+    unsigned long long* dr = nullptr;
+    if (rc == BGPU_OK) rc = result_block(&dr);
+    if (rc != BGPU_OK) return rc;
+    if (sub) {
+        // the compare stays on the device: the frame kernels read it and
+        // subtract the smaller magnitude from the larger (the reference's
+        // negation when B is larger); equal magnitudes give all-zero digits
+        rc = cuda_status(launch_frame_cmp(f, dr + 3, g.stream));
+        f.sub = 1;
+        f.order = dr + 3;
+    }
+    if (rc == BGPU_OK) rc = cuda_status(launch_frame_addsub(f, o + dig, o + dig + nblk, o, g.stream));
+    uint32_t r[4];
+    unsigned long long cmp = 0;
+    if (rc == BGPU_OK) rc = extent(dr, o, L + 1, 0, 0, r, &cmp);
+    if (rc != BGPU_OK) return rc;
+    if (sub && cmp == 0) {  // exactly zero: reset()
+        *out = DVal{};
+        return BGPU_OK;
+    }
+    if (r[0] == 0 || r[1] >= r[0]) return BGPU_ERR_CUDA;  // a nonzero result has a nonzero digit
+    out->d = o + r[1];
+    out->n = r[0] - r[1];
+    out->pp = pp_res - (int64_t)r[1];
+    out->neg = sub && (cmp & 3u) == 2u ? !a.neg : a.neg;
+    out->tz = 0;
+    out->top = r[3];
+    out->slot = slot;
+    return BGPU_OK;
+}
+
+int upload_digits(int slot, const std::vector<uint32_t>& v, int64_t pp, bool neg, DVal* out) {
+    int rc;
+    uint32_t* d = rslot(slot, v.size(), &rc);
+    if (rc != BGPU_OK) return rc;
+    rc = cuda_status(cudaMemcpyAsync(d, v.data(), v.size() * 4, cudaMemcpyHostToDevice, g.stream));
+    if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(g.stream));
+    if (rc != BGPU_OK) return rc;
+    size_t tz = 0;
+    while (tz < v.size() && v[tz] == 0) ++tz;
+    *out = DVal{d, v.size(), pp, neg, tz, v.back(), slot};
+    return BGPU_OK;
+}
+
+int reciprocal_locked(const uint32_t* digits, size_t n, int64_t point_pos, bool neg, size_t precision,
+                      uint32_t* out, size_t out_cap, size_t* out_len, int64_t* out_pp, int* out_neg) {
+    if (n >= ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    for (size_t i = 0; i < n; ++i)
+        if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    if (digits[n - 1] == 0) return BGPU_ERR_INVALID_ARG;  // a leading zero digit, or the value zero
+    if (precision == 0) precision = n;
+    const int64_t exponent = 28 * ((int64_t)n - 1 - point_pos) + (32 - __builtin_clz(digits[n - 1]));
+    int rc;
+    uint32_t* din = rslot(kRsIn, n, &rc);
+    if (rc != BGPU_OK) return rc;
+    rc = host_to_device(din, digits, n * 4, g.stream, nullptr);
+    if (rc != BGPU_OK) return rc;
+    size_t tz = 0;
+    while (digits[tz] == 0) ++tz;
+    const DVal in{din, n, point_pos, neg, tz, digits[n - 1], kRsIn};
+
+    // b = *this >> exponent; b.remove_tail_zero()
+    DVal b;
+    rc = shift_val(in, -exponent, kRsB, &b);
+    if (rc != BGPU_OK) return rc;
+    b.d += b.tz;
+    b.n -= b.tz;
+    b.pp -= (int64_t)b.tz;
+    b.tz = 0;
+
+    // x = BigFloat(1 / b.to_double())
+    uint32_t t[3];
+    const size_t k = std::min<size_t>(b.n, 3);
+    rc = read_back(b.d + (b.n - k), t, k);
+    if (rc != BGPU_OK) return rc;
+    bool ok;
+    const double bd = to_double_top(t, k, b.n, b.pp, b.neg, &ok);
+    if (!ok || !(std::fabs(bd) >= 0.5 && std::fabs(bd) < 1.0)) return BGPU_ERR_CUDA;
+    std::vector<uint32_t> x0;
+    int64_t x0_pp;
+    bool x0_neg;
+    double_to_digits(1 / bd, &x0, &x0_pp, &x0_neg);
+    DVal x, one;
+    rc = upload_digits(kRsX0, x0, x0_pp, x0_neg, &x);
+    if (rc == BGPU_OK) rc = upload_digits(kRsOne, std::vector<uint32_t>{1u}, 0, false, &one);
+    if (rc != BGPU_OK) return rc;
+
+    size_t cur = 52 / 28;  // DOUBLE_MANTISSA_LEN / DIGIT_BITS
+    while (cur < precision) {
+        cur *= 2;
+        DVal t1, t2, t3, xn;
+        rc = mul_trunc(b, x, cur + 1, kRsT1, &t1);
+        if (rc == BGPU_OK) rc = add_or_sub(one, t1, true, kRsT2, &t2);
+        if (rc == BGPU_OK) rc = mul_trunc(x, t2, cur + 1, kRsT3, &t3);
+        const int xs = x.slot == kRsX0 ? kRsX1 : kRsX0;
+        if (rc == BGPU_OK) rc = add_or_sub(x, t3, false, xs, &xn);
+        if (rc != BGPU_OK) return rc;
+        if (xn.slot != kRsX0 && xn.slot != kRsX1) {  // x + t3 returned t3 itself: keep x in an x buffer
+            uint32_t* d = rslot(xs, xn.n, &rc);
+            if (rc != BGPU_OK) return rc;
+            if (!xn.zero()) {
+                rc = cuda_status(cudaMemcpyAsync(d, xn.d, xn.n * 4, cudaMemcpyDeviceToDevice, g.stream));
+                if (rc != BGPU_OK) return rc;
+                xn.d = d;
+            }
+            xn.slot = xs;
+        }
+        x = xn;
+    }
+
+    // x >>= exponent
+    DVal r;
+    if (x.zero()) return BGPU_ERR_CUDA;
+    rc = shift_val(x, -exponent, kRsOut, &r);
+    if (rc != BGPU_OK) return rc;
+    *out_len = r.n;
+    *out_pp = r.pp;
+    *out_neg = r.neg ? 1 : 0;
+    if (r.n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+    rc = device_to_host(out, r.d, r.n * 4, g.stream);
+    return check_device_error(rc);
+}
+
 }  // namespace
 
 Tuning& tuning() { return g_tuning; }
@@ -810,6 +1240,18 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
     cudaSetDevice(g.device);
     return mul_digits_locked(a, na, b, nb, output_precision, point_pos, out, out_cap, out_len,
                              flags, stats);
+}
+
+int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
+                           size_t precision, uint32_t* out, size_t out_cap, size_t* out_len,
+                           int64_t* out_point_pos, int* out_is_neg) {
+    if (!digits || n == 0 || !out_len || !out_point_pos || !out_is_neg || (!out && out_cap))
+        return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return reciprocal_locked(digits, n, point_pos, is_neg != 0, precision, out, out_cap, out_len,
+                             out_point_pos, out_is_neg);
 }
 
 int bgpu_selftest_wait(uint32_t spin_limit, int set_flag) {

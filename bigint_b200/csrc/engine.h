@@ -217,6 +217,36 @@ cudaError_t launch_digits28_to_limbs(const uint32_t* d, uint32_t nd, uint64_t* l
 cudaError_t launch_limbs_to_digits28(const uint64_t* limbs, uint32_t nlimbs, uint32_t* d,
                                      uint32_t nd, cudaStream_t stream);
 
+// Digit kernels of the device-resident BigFloat steps (bigfloat_kernels.cu).
+// A frame operation places operand A at digit offset oa (frame digit j holds
+// a[j - oa] when 0 <= j - oa < na, else 0) and B likewise, and writes the L
+// frame digits of A + B, or of A - B for A >= B, plus the carry out of the
+// frame in out[L].  agg and cin hold frame_blocks(L) words each.
+struct FrameOp {
+    const uint32_t* a;
+    int64_t oa;
+    uint32_t na;
+    const uint32_t* b;
+    int64_t ob;
+    uint32_t nb;
+    uint32_t L;
+    int sub;
+    const unsigned long long* order;  // nullptr, or a compare result: B - A when B is larger
+};
+uint32_t frame_blocks(uint32_t L);
+cudaError_t launch_frame_addsub(const FrameOp& f, uint32_t* agg, uint32_t* cin, uint32_t* out,
+                                cudaStream_t st);
+// Into a zeroed word: (j + 1) << 2 | (1 if A_j > B_j else 2) for the highest
+// frame position j where A and B differ; stays 0 when they are equal.
+cudaError_t launch_frame_cmp(const FrameOp& f, unsigned long long* r, cudaStream_t st);
+// Into three zeroed words: r[0] = (j + 1) << 32 | d[j] for the highest nonzero
+// j; r[1], r[2] = 2^32 - j for the lowest nonzero j >= from0, from1 (0: none).
+cudaError_t launch_extent(const uint32_t* d, uint32_t n, uint32_t from0, uint32_t from1,
+                          unsigned long long* r, cudaStream_t st);
+// out = v >> s (n digits) or v << s (n + 1 digits), s in [1, 27], 28-bit digits
+cudaError_t launch_shift_digits(const uint32_t* v, uint32_t n, uint32_t s, bool left, uint32_t* out,
+                                cudaStream_t st);
+
 // Host <-> device copies of the host API: page-locked caller memory goes
 // straight to the copy engines, pageable memory through a ring of
 // page-locked slots filled by a pool of host threads.  host_to_device may

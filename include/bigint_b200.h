@@ -126,6 +126,22 @@ int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t 
 int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
                  size_t out_cap, size_t* out_len);
 
+/* Reciprocal of a BigFloat: BigFloat::reciprocal(precision)
+ * (src/bigint.cpp:1044-1071), its Newton iteration
+ * x += mul(x, 1 - mul(b, x, p + 1), p + 1) run with every value on the GPU
+ * (the truncated products of BigFloat::mul / mul_digits, the additions and
+ * subtractions of BigFloat::add_or_sub, the shifts), so no digit array makes a
+ * host round trip between steps.  The input is the BigFloat's fields: its
+ * Digits (28-bit, no leading zero digit), point position (value = digits *
+ * 2^(-28 point_pos)) and sign; precision 0 means the input's digit count, as
+ * in the reference.  Writes the reciprocal's Digits, point position and sign,
+ * identical to the reference's result.  Division by zero (the reference
+ * throws std::domain_error) and digits >= 2^28 give BGPU_ERR_INVALID_ARG;
+ * BGPU_ERR_OUT_CAPACITY when out_cap is too small (*out_len = needed). */
+int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
+                           size_t precision, uint32_t* out, size_t out_cap, size_t* out_len,
+                           int64_t* out_point_pos, int* out_is_neg);
+
 /* Device-resident product (no host copies, asynchronous on `stream`, a
  * cudaStream_t; 0 is the legacy default stream): d_out receives exactly
  * na + nb limbs (zero padded).  d_a == d_b with na == nb squares.  Errors

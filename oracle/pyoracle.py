@@ -150,6 +150,13 @@ class Reference(_Lib):
         L.ref_product_tree.restype = C.c_int
         L.ref_init_thread_pool.argtypes = [C.c_uint32]
         L.ref_init_thread_pool.restype = None
+        self.has_bigfloat_reciprocal = hasattr(L, "ref_bigfloat_reciprocal")
+        if self.has_bigfloat_reciprocal:
+            L.ref_bigfloat_reciprocal.argtypes = [_u64p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t,
+                                                  _u32p, C.c_size_t, _szp, C.POINTER(C.c_int64),
+                                                  _u32p, C.c_size_t, _szp, C.POINTER(C.c_int64),
+                                                  C.POINTER(C.c_int)]
+            L.ref_bigfloat_reciprocal.restype = C.c_int
         self.has_reciprocal = hasattr(L, "ref_reciprocal")
         if self.has_reciprocal:
             L.ref_reciprocal.argtypes = [_u64p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t, _szp,
@@ -194,6 +201,28 @@ class Reference(_Lib):
         if rc != 0:
             raise OracleError(f"ref_reciprocal returned {rc}")
         return out[: n.value].copy(), int(pp.value)
+
+    def bigfloat_reciprocal(self, limbs, offset: int, neg: bool, precision: int):
+        """(+-BigFloat(X, offset)).reciprocal(precision), X = the integer with
+        little-endian u64 ``limbs`` (nonzero).
+
+        Returns ((in_digits, in_point_pos, neg), (digits, point_pos, neg)): the
+        input BigFloat's fields and the reciprocal's."""
+        leaves = _limbs(limbs)
+        in_cap = (leaves.size * 64) // 28 + 8
+        cap = 4 * max(int(precision), in_cap) + 64
+        din = np.zeros(in_cap, dtype=np.uint32)
+        out = np.zeros(cap, dtype=np.uint32)
+        nin, nout = C.c_size_t(0), C.c_size_t(0)
+        ppin, pp, oneg = C.c_int64(0), C.c_int64(0), C.c_int(0)
+        rc = self.lib.ref_bigfloat_reciprocal(_p64(leaves), leaves.size, int(offset), int(bool(neg)),
+                                              int(precision), _p32(din), in_cap, C.byref(nin),
+                                              C.byref(ppin), _p32(out), cap, C.byref(nout), C.byref(pp),
+                                              C.byref(oneg))
+        if rc != 0:
+            raise OracleError(f"ref_bigfloat_reciprocal returned {rc}")
+        return ((din[: nin.value].copy(), int(ppin.value), bool(neg)),
+                (out[: nout.value].copy(), int(pp.value), bool(oneg.value)))
 
     def fast_pow_digits(self, base: int, exponent: int) -> np.ndarray:
         """fast_pow(BigInt(base), exponent) as reference 28-bit Digits."""

@@ -14,6 +14,7 @@
 //   ref_product_tree-> BigInt::operator* (bigint.h:284) over a pairwise tree
 //   ref_fast_pow    -> bigint::fast_pow<BigInt>   include/bigint/bigint_base.h:60
 //   ref_reciprocal  -> BigFloat::reciprocal       src/bigint.cpp:1044 (Newton, BigFloat::mul)
+//   ref_bigfloat_reciprocal -> the same on BigFloat(x, offset), negated on request
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -21,6 +22,7 @@
 #include <cstdint>
 #include <cstring>
 #include <span>
+#include <string>
 #include <vector>
 
 #include "bigint/bigint.h"
@@ -133,6 +135,31 @@ int ref_reciprocal(const uint64_t* leaves, size_t n, size_t precision, uint32_t*
     for (size_t i = 0; i < n; ++i) x *= bigint::BigInt(leaves[i]);
     const bigint::BigFloat r = bigint::BigFloat(x).reciprocal(precision);
     *point_pos = r.get_point_pos();
+    return copy_out32(r.get_data(), out, cap, out_len);
+}
+
+// BigFloat::reciprocal of +-BigFloat(X, offset) (the constructor of
+// include/bigint/bigint.h:382: X * 2^offset, tail zeros removed), X given by
+// its little-endian u64 limbs and built through the reference's hex-string
+// constructor (src/bigint.cpp:25).  Returns the input BigFloat's digits,
+// point position and sign as well, so a caller can hand the same BigFloat to
+// another implementation.
+int ref_bigfloat_reciprocal(const uint64_t* limbs, size_t n, int64_t offset, int neg, size_t precision,
+                            uint32_t* in_out, size_t in_cap, size_t* in_len, int64_t* in_point_pos,
+                            uint32_t* out, size_t cap, size_t* out_len, int64_t* point_pos, int* out_neg) {
+    static const char hexd[] = "0123456789abcdef";
+    std::string hex;
+    hex.reserve(16 * n);
+    for (size_t i = n; i-- > 0;)
+        for (int k = 15; k >= 0; --k) hex.push_back(hexd[(limbs[i] >> (4 * k)) & 15]);
+    bigint::BigInt x(hex, true);
+    bigint::BigFloat v(x, offset);
+    if (neg) v = -v;
+    *in_point_pos = v.get_point_pos();
+    if (copy_out32(v.get_data(), in_out, in_cap, in_len) != 0) return -1;
+    const bigint::BigFloat r = v.reciprocal(precision);
+    *point_pos = r.get_point_pos();
+    *out_neg = r.sign() < 0 ? 1 : 0;
     return copy_out32(r.get_data(), out, cap, out_len);
 }
 
