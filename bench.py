@@ -472,6 +472,68 @@ def fast_pow_form(bb, port, cpu: bool = True):
     return res
 
 
+def reciprocal_form(bb, cpu: bool = True, reps: int = 5):
+    """BigFloat::reciprocal (src/bigint.cpp:1044-1071) of a 2^24-bit value at
+    its own precision (599187 digits) through bgpu_reciprocal_digits, every
+    Newton step on the device, wall clock from host Digits to host Digits;
+    the reference's own reciprocal on the host cores beside it (one run),
+    digits, point and sign compared."""
+    rng = np.random.default_rng(SEED + 7)
+    limbs = rng.integers(0, 2**64, (1 << 24) // 64, dtype=np.uint64)
+    limbs[-1] |= np.uint64(1 << 63)
+    digits = limbs_to_digits28_np(limbs)
+    tz = int(np.argmax(digits != 0))  # BigFloat(BigInt) drops bottom zero digits
+    digits, pp_in = digits[tz:], -tz
+    bb.reciprocal_digits(digits, pp_in)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        got, pp, neg = bb.reciprocal_digits(digits, pp_in)
+        times.append(time.perf_counter() - t0)
+    res = {"input_bits": 1 << 24, "precision_digits": int(digits.size), "result_digits": int(got.size),
+           "s": statistics.median(times), "api": "bgpu_reciprocal_digits (host Digits in and out)"}
+    from oracle.pyoracle import Reference, have_reference
+
+    if cpu and have_reference() and Reference().has_bigfloat_reciprocal:
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        t0 = time.perf_counter()
+        (din, ppin, _), (want, wpp, wneg) = ref.bigfloat_reciprocal(limbs, 0, False, 0)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                "call": "BigFloat::reciprocal"}
+        if not (np.array_equal(din, digits) and ppin == pp_in and np.array_equal(got, want) and pp == wpp
+                and neg == wneg):
+            raise SystemExit("bench reciprocal: result differs from the reference's")
+        res["verified"] = "identical to the reference's reciprocal"
+    else:
+        # x * r within 2^(-28 k) of 1 for k = half the precision (Newton's
+        # previous step alone guarantees that much)
+        prod = bb.mul_digits(digits, got)  # point position pp_in + pp
+        k = digits.size // 2
+        top = prod[pp_in + pp - k:]
+        t = int.from_bytes(digits28_to_limbs_np(top).tobytes(), "little")
+        if t not in ((1 << (28 * k)) - 1, 1 << (28 * k)):
+            raise SystemExit("bench reciprocal: x * (1/x) is not close to 1")
+        res["verified"] = f"x * (1/x) = 1 to {28 * k} bits"
+    return res
+
+
+def limbs_to_digits28_np(limbs) -> np.ndarray:
+    """u64 limbs -> little-endian 28-bit digits without leading zeros."""
+    bits = np.unpackbits(np.ascontiguousarray(limbs, dtype=np.uint64).view(np.uint8), bitorder="little")
+    pad = (-bits.size) % 28
+    if pad:
+        bits = np.concatenate([bits, np.zeros(pad, dtype=np.uint8)])
+    b = bits.reshape(-1, 28)
+    d = np.zeros(b.shape[0], dtype=np.uint32)
+    for k in range(28):
+        d |= b[:, k].astype(np.uint32) << np.uint32(k)
+    n = d.size
+    while n > 1 and d[n - 1] == 0:
+        n -= 1
+    return d[:n]
+
+
 def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
     """Config "batched uneven": 4096 products, operand lengths log-uniform in
     [2^10, 2^22] bits, one graph launch per batch vs one plain NTT call per
@@ -774,6 +836,7 @@ def run_gpu_arm(args) -> None:
                  "fp64_fft": fft_form(bb, torch, device),
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
+                 "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
                                                 cpu=(rank == 0 and not args.no_cpu_baseline))}
@@ -818,7 +881,8 @@ def run_gpu_arm(args) -> None:
     print(json.dumps(line))
 
 
-FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "batched_4096",
+FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
+         "batched_4096",
          "product_tree_2p20")
 
 
@@ -846,6 +910,8 @@ def run_single_form(args) -> None:
         res = fast_pow_form(bb, port, cpu=not args.no_cpu_baseline)
     elif name == "mul_digits_2p24":
         res = mul_digits_form(bb, port, cpu=not args.no_cpu_baseline)
+    elif name == "reciprocal_2p24":
+        res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "batched_4096":
         res = batched_form(bb, torch, device, port)
     else:
