@@ -28,6 +28,7 @@ from __future__ import annotations
 
 from ._lib import (  # noqa: F401
     BGPU_FFT_AVERAGE_BOUND,
+    BGPU_INDEPENDENT,
     BGPU_METHOD_AUTO,
     BGPU_METHOD_FFT,
     BGPU_METHOD_KARATSUBA,

@@ -18,6 +18,7 @@ BGPU_METHOD_SCHOOLBOOK = 2
 BGPU_METHOD_FFT = 3
 BGPU_METHOD_KARATSUBA = 4
 BGPU_FFT_AVERAGE_BOUND = 0x10
+BGPU_INDEPENDENT = 0x20  # mul_device: operands not written by work in flight on the stream
 BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS = 1
 BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS = 2
 BGPU_TUNE_FFT_MIN_LIMBS = 3
@@ -413,7 +414,9 @@ def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, stream: i
 
     ``out_ptr`` receives na+nb limbs.  Equal pointers and lengths square.
     ``stream`` is a cudaStream_t handle (0 = legacy default stream), e.g.
-    ``torch.cuda.current_stream().cuda_stream``."""
+    ``torch.cuda.current_stream().cuda_stream``.  ``method`` may include
+    ``BGPU_INDEPENDENT`` for a stream of independent products (the next
+    product's transform starts under the previous one's carry scan)."""
     _ensure_init()
     rc = lib.bgpu_mul_u64_device(C.c_void_p(a_ptr), na, C.c_void_p(b_ptr), nb,
                                  C.c_void_p(out_ptr), method, C.c_void_p(stream or None))

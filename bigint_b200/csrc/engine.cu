@@ -48,6 +48,14 @@ struct Engine {
     // digit buffers of the device-resident reciprocal (one per live value)
     uint32_t* rs[11] = {};
     size_t rs_bytes[11] = {};
+    // stream and scratch layout of the last NTT product launched
+    cudaStream_t ntt_stream = nullptr;
+    int ntt_log_n = -1;
+    bool ntt_square = false;
+    // output of the previous bgpu_mul_u64_device call and its stream
+    cudaStream_t prev_stream = nullptr;
+    const void* prev_out = nullptr;
+    size_t prev_out_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint32_t last_launches = 0;
     // optional per-kernel timing of NTT products: a ring of event sets, one
@@ -200,7 +208,7 @@ int prepare_scratch(int log_n, bool square, ProductScratch* s) {
 // nd32 values are operand lengths in 32-bit digits.
 int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, void* out,
                     int out_fmt, size_t out_cap, uint32_t flags, cudaStream_t st,
-                    bgpu_stats* stats) {
+                    bgpu_stats* stats, bool overlap_prev = false) {
     const uint32_t method = flags & BGPU_METHOD_MASK;
     const uint64_t total32 = (uint64_t)a.nd32 + b.nd32;
     const int log_n = ceil_log2(total32 - 1);
@@ -213,6 +221,14 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
     CarryLaunch cl;
     cl.ticket_base = g.ticket_base;
     cl.epoch = ++g.epoch;
+    // The scratch layout (residue planes first, then the chunk sums, spills
+    // and flags the carry scan reads) depends on the length and on squaring:
+    // only an identical layout keeps this forward pass's planes clear of the
+    // previous product's carry data while that scan still runs.
+    cl.overlap_prev = overlap_prev && st == g.ntt_stream && ln == g.ntt_log_n && square == g.ntt_square;
+    g.ntt_stream = st;
+    g.ntt_log_n = ln;
+    g.ntt_square = square;
     g.ticket_base += carry_blocks((uint32_t)(((size_t)1 << ln) / 8));
     cudaEvent_t* ev = nullptr;
     if (g.kernel_timing) {
@@ -1296,6 +1312,18 @@ int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, siz
     cudaSetDevice(g.device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);  // 0 = the legacy default stream
     const bool square = (d_a == d_b && na == nb);
+    // A promised-independent product overlaps the previous one's tail unless
+    // its operands overlap the previous call's output on this stream.
+    auto hits_prev = [&](const uint64_t* p, size_t n) {
+        const char* lo = reinterpret_cast<const char*>(p);
+        const char* plo = static_cast<const char*>(g.prev_out);
+        return lo < plo + g.prev_out_bytes && plo < lo + n * 8;
+    };
+    const bool overlap = (flags & BGPU_INDEPENDENT) &&
+                         !(st == g.prev_stream && (hits_prev(d_a, na) || hits_prev(d_b, nb)));
+    g.prev_stream = st;
+    g.prev_out = d_out;
+    g.prev_out_bytes = (na + nb) * 8;
     if (const uint32_t sm = small_method(flags, na, nb)) {
         g.last_launches = 1;
         return launch_small(sm, d_a, na, d_b, nb, d_out, st);
@@ -1303,7 +1331,7 @@ int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, siz
     if (na + nb > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
     OperandDesc oa{d_a, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
     OperandDesc ob{d_b, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
-    return multiply_device(oa, ob, square, d_out, kFmtLimb64, na + nb, flags, st, nullptr);
+    return multiply_device(oa, ob, square, d_out, kFmtLimb64, na + nb, flags, st, nullptr, overlap);
 }
 
 int bgpu_device_status(void* stream) {

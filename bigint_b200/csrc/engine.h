@@ -92,6 +92,10 @@ struct CarryLaunch {
     uint64_t epoch;
     unsigned long long* ticket = nullptr;  // batch launches: ticket counter
     uint32_t* err = nullptr;               // batch launches: sticky error word
+    // The forward pass may run under the tail of whatever kernel precedes it
+    // on the stream (the previous product's carry scan), waiting for it only
+    // before it exits; only for operands that nothing in flight writes.
+    bool overlap_prev = false;
 };
 
 // Launch the full NTT product pipeline (4 kernels) on `stream`.

@@ -191,6 +191,12 @@ struct FwdColsArgs {
     const ProductDesc* descs;
     ProductDesc one;
     int nops, log_n, log_n1, slot;
+    // 1: the operands and this pass's residue planes are free of the
+    // preceding kernel (its trigger came after the previous product's
+    // inverse pass finished), so the pass starts under that kernel's tail and
+    // waits for it only at the end -- which keeps every later kernel ordered
+    // after it, since each of them waits for this pass to complete
+    int overlap;
 };
 
 // Returned by value: binding a reference to the kernel parameter would force
@@ -233,7 +239,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
         sS[col * SROW + m] = make_uint2(w, w * pinv);
     }
     if constexpr (NR == 1) __syncthreads();
-    pdl_wait();
+    if (!a.overlap) pdl_wait();
 
     // Round 0: rows n2 = base + (j << LO) read from the caller's digits.
     {
@@ -302,6 +308,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     // Let the row pass launch only once this CTA's work is done: an early
     // trigger parks row-pass CTAs on SMs the column pass still fills.
     pdl_trigger();
+    if (a.overlap) pdl_wait();
 }
 
 // ---- kernel 2: middle row pass ----------------------------------------------
@@ -1029,6 +1036,7 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
     f.log_n = log_n;
     f.log_n1 = sh.log_n1;
     f.slot = slot;
+    f.overlap = cl.overlap_prev && count == 1 ? 1 : 0;
     cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, &f, nullptr, tiles, count, st)
                             : dispatch_outer<1>(sh.log_n2, &f, nullptr, tiles, count, st);
     if (e != cudaSuccess) return e;

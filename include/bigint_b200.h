@@ -51,6 +51,12 @@ extern "C" {
 #define BGPU_FFT_AVERAGE_BOUND 0x10u
 /* FFT form: force b bits per point (8..20) in flags bits 8..12. */
 #define BGPU_FFT_BITS(b) ((uint32_t)(b) << 8)
+/* bgpu_mul_u64_device only: the caller promises that nothing still running
+ * or queued on the stream writes this product's operands (a stream of
+ * independent products).  The transform of this product may then start while
+ * the previous product's carry scan finishes; every later kernel still runs
+ * after both.  Ignored when the operands overlap the previous call's output. */
+#define BGPU_INDEPENDENT 0x20u
 
 #define BGPU_SCHOOLBOOK_MAX_LIMBS 256u
 #define BGPU_KARATSUBA_MAX_LIMBS 256u

@@ -142,6 +142,46 @@ def test_digits_transform_sized_by_bit_length(bb, port):
         assert np.array_equal(got, port.mul_digits(a, b)), k
 
 
+def test_independent_products_back_to_back(bb, port):
+    """BGPU_INDEPENDENT: each transform starts under the previous product's
+    carry scan.  Mixed sizes, squares, a product whose operand is the previous
+    output (the overlap must then be refused) and one reusing the previous
+    output buffer as its own output: every product exact."""
+    import torch
+
+    rng = np.random.default_rng(SEED + 17)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    sizes = [(1 << 14, 1 << 14), (1 << 12, 1 << 15), (3000, 3000), (1 << 14, 1 << 14), (5000, 77),
+             (1 << 16, 1 << 16)] * 3
+    ops = [(rand_limbs(rng, na), rand_limbs(rng, nb)) for na, nb in sizes]
+    dops = [(torch.from_numpy(a.view(np.int64)).to(dev), torch.from_numpy(b.view(np.int64)).to(dev))
+            for a, b in ops]
+    # every fourth product squares its first operand; outputs hold exactly
+    # na + nb limbs, all of which the product writes
+    outs = [torch.empty(2 * a.size if k % 4 == 3 else a.size + b.size, dtype=torch.int64, device=dev)
+            for k, (a, b) in enumerate(ops)]
+    torch.cuda.synchronize()
+    flags = bb.BGPU_METHOD_AUTO | bb.BGPU_INDEPENDENT
+    with torch.cuda.stream(stream):
+        for k, ((a, b), (da, db)) in enumerate(zip(ops, dops)):
+            sq = k % 4 == 3
+            bb.mul_device(da.data_ptr(), a.size, (da if sq else db).data_ptr(), a.size if sq else b.size,
+                          outs[k].data_ptr(), stream=stream.cuda_stream, method=flags)
+        # chained: the operand is the previous product's output
+        prev = outs[-1]
+        chained = torch.empty(2 * prev.numel(), dtype=torch.int64, device=dev)
+        bb.mul_device(prev.data_ptr(), prev.numel(), prev.data_ptr(), prev.numel(), chained.data_ptr(),
+                      stream=stream.cuda_stream, method=flags)
+    bb.device_status(stream.cuda_stream)
+    for k, (a, b) in enumerate(ops):
+        want = port.mul(a) if k % 4 == 3 else port.mul(a, b)
+        got = outs[k].cpu().numpy().view(np.uint64)
+        assert np.array_equal(got[: want.size], want) and not got[want.size:].any(), k
+    p = outs[-1].cpu().numpy().view(np.uint64)
+    assert port.mod_m61(p) ** 2 % M61 == port.mod_m61(chained.cpu().numpy().view(np.uint64))
+
+
 def test_headline_size_vs_port(bb, port):
     """2^24 x 2^24-bit product (the bench workload) limb-exact."""
     rng = np.random.default_rng(SEED + 15)
