@@ -29,7 +29,7 @@ struct Engine {
     cudaStream_t h2d = nullptr, d2h = nullptr;
     void* d_many = nullptr;
     size_t many_bytes = 0;
-    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
+    cudaEvent_t ev_in[4] = {}, ev_comp[4] = {}, ev_out[4] = {};
     NttConsts consts[kNumSets]{};
     void* d_tables[kNumSets] = {};
     void* d_fft_tables = nullptr;
@@ -95,7 +95,7 @@ void release_locked() {
     if (g.ev1) cudaEventDestroy(g.ev1);
     for (auto e : g.kev) cudaEventDestroy(e);
     cudaFree(g.d_many);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 4; ++i) {
         if (g.ev_in[i]) cudaEventDestroy(g.ev_in[i]);
         if (g.ev_comp[i]) cudaEventDestroy(g.ev_comp[i]);
         if (g.ev_out[i]) cudaEventDestroy(g.ev_out[i]);
@@ -140,7 +140,7 @@ int init_locked(int device) {
     if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.h2d, cudaStreamNonBlocking));
     if (rc == BGPU_OK) rc = cuda_status(cudaStreamCreateWithFlags(&g.d2h, cudaStreamNonBlocking));
-    for (int i = 0; i < 2 && rc == BGPU_OK; ++i) {
+    for (int i = 0; i < 4 && rc == BGPU_OK; ++i) {
         rc = cuda_status(cudaEventCreateWithFlags(&g.ev_in[i], cudaEventDisableTiming));
         if (rc == BGPU_OK) rc = cuda_status(cudaEventCreateWithFlags(&g.ev_comp[i], cudaEventDisableTiming));
         if (rc == BGPU_OK) rc = cuda_status(cudaEventCreateWithFlags(&g.ev_out[i], cudaEventDisableTiming));
@@ -588,10 +588,10 @@ int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64
     return BGPU_OK;
 }
 
-// Many host-resident products, pipelined: two device slots; product i's
-// operands go up on the H2D stream while product i-1 computes and product
-// i-2's result comes back on the D2H stream.  Every product still makes its
-// own host->device and device->host copies.
+// Many host-resident products, pipelined over four device slots (two for
+// products above 256 MB): product i's operands go up on the H2D stream while
+// earlier products compute and their results come back on the D2H stream.
+// Every product still makes its own host->device and device->host copies.
 int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags) {
     struct Item { size_t na, nb; bool square; };
     std::vector<Item> it(count);
@@ -614,7 +614,11 @@ int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags
         }
     }
     const size_t slot = slot_in + slot_out;
-    int rc = ensure(&g.d_many, &g.many_bytes, 2 * slot);
+    // Four device slots keep both copy directions busy (the upload of
+    // product i waits only for the download of product i - 4); products
+    // above 256 MB of operands and result use two.
+    const size_t nslots = slot <= ((size_t)256 << 20) ? 4 : 2;
+    int rc = ensure(&g.d_many, &g.many_bytes, nslots * slot);
     if (rc != BGPU_OK) return rc;
     if (max_ln) {  // size the transform scratch once, before anything is in flight
         ProductScratch s{};
@@ -626,14 +630,14 @@ int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags
     for (size_t i = 0; i < count; ++i) {
         const bgpu_host_product& q = p[i];
         const Item& m = it[i];
-        const int k = (int)(i & 1);
+        const int k = (int)(i % nslots);
         char* base = static_cast<char*>(g.d_many) + k * slot;
         uint64_t* da = reinterpret_cast<uint64_t*>(base);
         uint64_t* db = m.square ? da : reinterpret_cast<uint64_t*>(base + align256(m.na * 8));
         uint64_t* dout = reinterpret_cast<uint64_t*>(base + slot_in);
         const size_t nout = q.na + q.nb;
         cudaError_t e = cudaSuccess;
-        if (i >= 2) e = cudaStreamWaitEvent(g.h2d, g.ev_out[k], 0);  // slot k's last result is out
+        if (i >= nslots) e = cudaStreamWaitEvent(g.h2d, g.ev_out[k], 0);  // slot k's last result is out
         if (m.na == 0 || m.nb == 0) {  // a zero operand: the product is zero
             if (e == cudaSuccess) e = cudaMemsetAsync(dout, 0, nout * 8, g.h2d);
             if (e == cudaSuccess) e = cudaEventRecord(g.ev_comp[k], g.h2d);

@@ -105,7 +105,7 @@ int bgpu_mul_digits(const uint32_t* a, size_t na, const uint32_t* b, size_t nb,
 /* Many independent products of host-resident operands, pipelined: each
  * product's operands are copied to the GPU, multiplied and the product copied
  * back, with the copies of neighbouring products overlapping the multiply
- * (two device slots, separate copy streams).  The reference multiplies one
+ * (four device slots, separate copy streams).  The reference multiplies one
  * pair per call (_mul, include/bigint/mul.h:208-220); this is that call over a
  * list, for callers with many products at hand (binary splitting,
  * examples/pi.cpp:41-80).  out receives na + nb limbs (out_cap >= na + nb;
