@@ -262,6 +262,7 @@ def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int):
         impl, kind, cores = Port(), "port", 1
         fn = impl.ntt_mul
     fn(a[:1024], b[:1024])  # warm the pool
+    fn(a, b)  # and the full-size path: the reference's first large products run slower
     reps, t0 = 0, time.perf_counter()
     while True:
         fn(a, b)
@@ -287,6 +288,63 @@ def _event_ms(torch, stream, fn, reps):
         e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def plain_2p20_form(bb, torch, device, port, cpu: bool = True):
+    """Config "plain NTT, 2^20 x 2^20": one product of two seeded uniform
+    2^20-bit operands (16384 limbs each, top bit set), device resident (CUDA
+    events, one product at a time) and through the host API
+    (bgpu_mul_u64, pageable buffers, wall clock), compared limb-exact with the
+    reference's ntt::mul (src/mul/ntt_multithread.cpp:444), which is timed on
+    the host cores beside it."""
+    rng = np.random.default_rng(SEED + 1)
+    n = (1 << 20) // 64
+    a = rng.integers(0, 2**64, n, dtype=np.uint64)
+    b = rng.integers(0, 2**64, n, dtype=np.uint64)
+    a[-1] |= np.uint64(1 << 63)
+    b[-1] |= np.uint64(1 << 63)
+    stream = torch.cuda.Stream(device)
+    sp = stream.cuda_stream
+    da, db = _dev_limbs(torch, device, a), _dev_limbs(torch, device, b)
+    out = torch.empty(2 * n, dtype=torch.int64, device=device)
+
+    def run(i):
+        bb.mul_device(da.data_ptr(), n, db.data_ptr(), n, out.data_ptr(), stream=sp,
+                      method=bb.BGPU_METHOD_NTT)
+    run(0)
+    bb.device_status(sp)
+    dev_ms = _event_ms(torch, stream, run, 50)
+    bb.device_status(sp)
+    got_dev = out.cpu().numpy().view(np.uint64)
+    bb.mul(a, b)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        got = bb.mul(a, b)
+    host_ms = (time.perf_counter() - t0) / 20 * 1e3
+    res = {"a_bits": 1 << 20, "b_bits": 1 << 20, "device_ms": dev_ms, "host_api_ms": host_ms,
+           "products_per_s": 1e3 / dev_ms}
+    from oracle.pyoracle import Reference, have_reference
+
+    if have_reference():
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        for _ in range(3):  # the pool's threads and first-touch pages warm up over the first calls
+            want = ref.ntt_mul(a, b)
+        if cpu:
+            ts = []
+            for _ in range(7):
+                t0 = time.perf_counter()
+                ref.ntt_mul(a, b)
+                ts.append(time.perf_counter() - t0)
+            res["cpu_reference"] = {"ms": statistics.median(ts) * 1e3, "threads": host_cores(),
+                                    "call": "bigint::mul::ntt::mul (median of 7 after 3 warm-up calls)"}
+        res["verified"] = "limb-exact vs the reference's ntt::mul"
+    else:
+        want = port.ntt_mul(a, b)
+        res["verified"] = "limb-exact vs the C restatement"
+    if not (np.array_equal(got, want) and np.array_equal(got_dev[: want.size], want)):
+        raise SystemExit("bench plain 2^20: product differs from the reference")
+    return res
 
 
 def sweep_form(bb, torch, device, port):
@@ -853,7 +911,8 @@ def run_gpu_arm(args) -> None:
     forms = None
     if not args.no_forms:
         torch.cuda.synchronize(device)
-        forms = {"batched_2p24": batched_same_size_form(bb, torch, device, port, A, B),
+        forms = {"plain_2p20": plain_2p20_form(bb, torch, device, port, cpu=not args.no_cpu_baseline),
+                 "batched_2p24": batched_same_size_form(bb, torch, device, port, A, B),
                  "ntt_size_sweep": sweep_form(bb, torch, device, port),
                  "fp64_fft": fft_form(bb, torch, device),
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
@@ -907,7 +966,7 @@ def run_gpu_arm(args) -> None:
     print(json.dumps(line))
 
 
-FORMS = ("batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
+FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
          "batched_4096",
          "product_tree_2p20")
 
@@ -925,7 +984,9 @@ def run_single_form(args) -> None:
     bb.init(0)
     port = Port()
     name = args.form
-    if name == "batched_2p24":
+    if name == "plain_2p20":
+        res = plain_2p20_form(bb, torch, device, port, cpu=not args.no_cpu_baseline)
+    elif name == "batched_2p24":
         A, B = make_operands(args.bits, pairs=32)
         res = batched_same_size_form(bb, torch, device, port, A, B)
     elif name == "ntt_size_sweep":
