@@ -349,8 +349,10 @@ def plain_2p20_form(bb, torch, device, port, cpu: bool = True):
 
 def sweep_form(bb, torch, device, port):
     """Config "NTT size sweep": squares at 2^16..2^30 bits, uniform and all-ones
-    limbs, plus the 1:8 and 1:64 unbalanced pairs; device-resident products
-    back to back on one stream (operands smaller than L2 stay cached there)."""
+    limbs, plus the 1:8 and 1:64 unbalanced pairs, and two sizes beyond the
+    largest transform (2^31 x 2^31 bits, a 2^32-bit square: block products);
+    device-resident products back to back on one stream (operands smaller
+    than L2 stay cached there)."""
     stream = torch.cuda.Stream(device)
     sp = stream.cuda_stream
     M = (1 << 61) - 1
@@ -358,6 +360,8 @@ def sweep_form(bb, torch, device, port):
     rows = []
     cases = [(1 << b, 1 << b, "square") for b in range(16, 31, 2)]
     cases += [(1 << 24, 1 << 21, "1:8"), (1 << 20, 1 << 14, "1:64")]
+    # beyond the largest transform (2^31 product bits): blocks of 2^30-bit NTT products
+    cases += [(1 << 31, 1 << 31, "1:1"), (1 << 32, 1 << 32, "square")]
     for abits, bbits, kind in cases:
         na, nb = abits // 64, bbits // 64
         for fill in ("uniform", "all-ones"):
@@ -378,6 +382,8 @@ def sweep_form(bb, torch, device, port):
                 bb.mul_device(da.data_ptr(), na, db.data_ptr(), nb, out.data_ptr(), stream=sp,
                               method=bb.BGPU_METHOD_NTT)
             reps = 3 if abits >= 1 << 28 else 20
+            if abits >= 1 << 31:
+                reps = 2
             run(0)
             bb.device_status(sp)
             ms = _event_ms(torch, stream, run, reps)

@@ -48,6 +48,9 @@ struct Engine {
     // digit buffers of the device-resident reciprocal (one per live value)
     uint32_t* rs[11] = {};
     size_t rs_bytes[11] = {};
+    // block products of the decomposition beyond the largest transform
+    void* d_huge = nullptr;
+    size_t huge_bytes = 0;
     // stream and scratch layout of the last NTT product launched
     cudaStream_t ntt_stream = nullptr;
     int ntt_log_n = -1;
@@ -86,6 +89,7 @@ void release_locked() {
     cudaFree(g.d_fft_tables);
     cudaFree(g.d_fft_err);
     cudaFree(g.d_scratch);
+    cudaFree(g.d_huge);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
@@ -245,6 +249,45 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
     }
     (void)method;
     return cuda_status(e);
+}
+
+// True when a product of na x nb limbs needs more points than the largest
+// transform.
+bool beyond_transform(size_t na, size_t nb) {
+    return ceil_log2(2 * (uint64_t)(na + nb) - 1) > kMaxLogN;
+}
+
+// Product beyond the largest transform (huge.cu): both operands in blocks of
+// kHugeBlockLimbs limbs, every block pair one NTT product, each added into
+// dout (na + nb limbs) at its offset with a carry scan over the rest.  A
+// square computes each off-diagonal block pair once and adds it twice.
+int huge_product(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, uint64_t* dout, bool square,
+                 cudaStream_t st) {
+    const uint64_t S = kHugeBlockLimbs, L = na + nb;
+    const size_t acc = align256((size_t)accumulate_blocks(L) * 4);
+    int rc = ensure(&g.d_huge, &g.huge_bytes, 2 * S * 8 + 2 * acc);
+    if (rc != BGPU_OK) return rc;
+    uint64_t* tmp = static_cast<uint64_t*>(g.d_huge);
+    uint32_t* agg = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(g.d_huge) + 2 * S * 8);
+    uint32_t* cin = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(agg) + acc);
+    cudaError_t e = cudaMemsetAsync(dout, 0, L * 8, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    for (uint64_t ia = 0; ia < na; ia += S) {
+        for (uint64_t ib = square ? ia : 0; ib < nb; ib += S) {
+            const uint64_t la = std::min<uint64_t>(S, na - ia), lb = std::min<uint64_t>(S, nb - ib);
+            const bool diag = square && ia == ib;
+            OperandDesc oa{da + ia, (uint32_t)la, (uint32_t)(2 * la), kFmtLimb64};
+            OperandDesc ob{db + ib, (uint32_t)lb, (uint32_t)(2 * lb), kFmtLimb64};
+            rc = multiply_device(oa, diag ? oa : ob, diag, tmp, kFmtLimb64, la + lb, BGPU_METHOD_AUTO, st,
+                                 nullptr);
+            if (rc != BGPU_OK) return rc;
+            for (int twice = 0; twice < (square && !diag ? 2 : 1); ++twice) {
+                e = launch_accumulate(dout + ia + ib, L - (ia + ib), tmp, la + lb, agg, cin, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+        }
+    }
+    return BGPU_OK;
 }
 
 // The small-product kernel a call uses (BGPU_METHOD_AUTO: by the tuned
@@ -438,6 +481,9 @@ int mul_u64_locked(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, u
         rc = launch_small(sm, da, na, db, nb, dout, st);
         g.last_launches = 1;
         if (stats) stats->method = (int32_t)sm;
+    } else if (beyond_transform(na, nb)) {
+        rc = huge_product(da, na, db, nb, dout, square, st);
+        if (stats) stats->method = BGPU_METHOD_NTT;
     } else {
         OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
         OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
@@ -474,6 +520,7 @@ int device_product(const uint64_t* da, size_t na, const uint64_t* db, size_t nb,
         *launches += 1;
         return launch_small(sm, da, na, db, nb, dout, st);
     }
+    if (beyond_transform(na, nb)) return huge_product(da, na, db, nb, dout, square, st);
     OperandDesc oa{da, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
     OperandDesc ob{db, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
     *launches += kNttLaunches;
@@ -515,17 +562,15 @@ int pow_u64_locked(const uint64_t* base, size_t nbase, uint32_t exponent, uint64
         uint64_t bb = bbits, rb = 0;
         for (uint32_t e = exponent; e; e >>= 1) {
             if (e & 1) {
-                if (rb) {
+                if (rb) {  // products beyond the largest transform run as its blocks
                     const uint64_t t32 = 2 * (uint64_t)(limbs(rb) + limbs(bb));
-                    if (t32 > ((uint64_t)1 << kMaxLogN)) return BGPU_ERR_CAPACITY;
-                    max_ln = std::max(max_ln, ceil_log2(t32 - 1));
+                    max_ln = std::max(max_ln, std::min(kMaxLogN, ceil_log2(t32 - 1)));
                 }
                 rb += bb;
             }
             if (e > 1) {
                 const uint64_t t32 = 4 * (uint64_t)limbs(bb);
-                if (t32 > ((uint64_t)1 << kMaxLogN)) return BGPU_ERR_CAPACITY;
-                max_ln = std::max(max_ln, ceil_log2(t32 - 1));
+                max_ln = std::max(max_ln, std::min(kMaxLogN, ceil_log2(t32 - 1)));
                 bb *= 2;
                 max_base = std::max(max_base, limbs(bb));
             }
@@ -722,7 +767,12 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     }
     cudaError_t e = cudaSuccess;
     if (stats) cudaEventRecord(g.ev0, st);
-    if (const uint32_t sm = small_method(flags, la64, lb64)) {
+    // Small products run on u64 limbs; so do products beyond the largest
+    // transform (blocks of NTT products, huge.cu).
+    const uint32_t sm = small_method(flags, la64, lb64);
+    const uint64_t n32 = (bits28(pa, la) + 31) / 32 + (bits28(pb, lb) + 31) / 32;
+    const bool huge = !sm && ceil_log2(n32 - 1) > kMaxLogN;
+    if (sm || huge) {
         uint64_t* la_d = reinterpret_cast<uint64_t*>(io + l_off);
         uint64_t* lb_d = square ? la_d : la_d + align256((la64 + 1) * 8) / 8;
         uint64_t* lo_d = reinterpret_cast<uint64_t*>(io + l_off + align256((la64 + 1) * 8) +
@@ -731,11 +781,13 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
         if (e == cudaSuccess && !square)
             e = launch_digits28_to_limbs(db, (uint32_t)lb, lb_d, (uint32_t)lb64, st);
         rc = cuda_status(e);
-        if (rc == BGPU_OK) rc = launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st);
+        if (rc == BGPU_OK)
+            rc = sm ? launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st)
+                    : huge_product(la_d, la64, lb_d, lb64, lo_d, square, st);
         if (rc == BGPU_OK)
             rc = cuda_status(launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st));
         g.last_launches = square ? 3 : 4;
-        if (stats) stats->method = (int32_t)sm;
+        if (stats) stats->method = sm ? (int32_t)sm : BGPU_METHOD_NTT;
     } else {
         // 32-bit digit counts from the true bit lengths: a number of exactly
         // 2^k bits has ceil(2^k / 28) digits, whose 28 * digits overshoots 2^k
@@ -996,7 +1048,11 @@ int digits_product(const DVal& a, size_t off_a, const DVal& b, size_t off_b, uin
     const size_t la = a.n - off_a, lb = b.n - off_b;
     const size_t la64 = (la * 28 + 63) / 64, lb64 = (lb * 28 + 63) / 64;
     cudaStream_t st = g.stream;
-    if (const uint32_t sm = small_method(BGPU_METHOD_AUTO, la64, lb64)) {
+    const uint64_t bits_a = 28 * (uint64_t)(la - 1) + (32 - __builtin_clz(a.top));
+    const uint64_t bits_b = 28 * (uint64_t)(lb - 1) + (32 - __builtin_clz(b.top));
+    const uint32_t sm = small_method(BGPU_METHOD_AUTO, la64, lb64);
+    const bool huge = !sm && ceil_log2((bits_a + 31) / 32 + (bits_b + 31) / 32 - 1) > kMaxLogN;
+    if (sm || huge) {  // on u64 limbs: the small kernels, or NTT blocks beyond the largest transform
         int rc;
         uint32_t* scr = rslot(kRsScratch, 2 * ((la64 + 1) + (lb64 + 1) + (la64 + lb64)), &rc);
         if (rc != BGPU_OK) return rc;
@@ -1006,13 +1062,13 @@ int digits_product(const DVal& a, size_t off_a, const DVal& b, size_t off_b, uin
         cudaError_t e = launch_digits28_to_limbs(pa, (uint32_t)la, la_d, (uint32_t)la64, st);
         if (e == cudaSuccess) e = launch_digits28_to_limbs(pb, (uint32_t)lb, lb_d, (uint32_t)lb64, st);
         rc = cuda_status(e);
-        if (rc == BGPU_OK) rc = launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st);
+        if (rc == BGPU_OK)
+            rc = sm ? launch_small(sm, la_d, la64, lb_d, lb64, lo_d, st)
+                    : huge_product(la_d, la64, lb_d, lb64, lo_d, false, st);
         if (rc == BGPU_OK)
             rc = cuda_status(launch_limbs_to_digits28(lo_d, (uint32_t)(la64 + lb64), dres, (uint32_t)nres, st));
         return rc;
     }
-    const uint64_t bits_a = 28 * (uint64_t)(la - 1) + (32 - __builtin_clz(a.top));
-    const uint64_t bits_b = 28 * (uint64_t)(lb - 1) + (32 - __builtin_clz(b.top));
     OperandDesc oa{pa, (uint32_t)la, (uint32_t)((bits_a + 31) / 32), kFmtDigit28};
     OperandDesc ob{pb, (uint32_t)lb, (uint32_t)((bits_b + 31) / 32), kFmtDigit28};
     return multiply_device(oa, ob, false, dres, kFmtDigit28, nres, BGPU_METHOD_AUTO, st, nullptr);
@@ -1333,6 +1389,7 @@ int bgpu_mul_u64_device(const uint64_t* d_a, size_t na, const uint64_t* d_b, siz
         return launch_small(sm, d_a, na, d_b, nb, d_out, st);
     }
     if (na + nb > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    if (beyond_transform(na, nb)) return huge_product(d_a, na, d_b, nb, d_out, square, st);
     OperandDesc oa{d_a, (uint32_t)na, (uint32_t)(2 * na), kFmtLimb64};
     OperandDesc ob{d_b, (uint32_t)nb, (uint32_t)(2 * nb), kFmtLimb64};
     return multiply_device(oa, ob, square, d_out, kFmtLimb64, na + nb, flags, st, nullptr, overlap);

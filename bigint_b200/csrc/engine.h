@@ -251,6 +251,15 @@ cudaError_t launch_extent(const uint32_t* d, uint32_t n, uint32_t from0, uint32_
 cudaError_t launch_shift_digits(const uint32_t* v, uint32_t n, uint32_t s, bool left, uint32_t* out,
                                 cudaStream_t st);
 
+// Products beyond the largest transform (huge.cu): out[0..L) += add[0..nadd)
+// (nadd <= L) with the carry carried through all of out; agg and cin hold
+// accumulate_blocks(L) words each.  kHugeBlockLimbs is the operand block of
+// the block decomposition: two blocks make the largest general NTT product.
+constexpr uint64_t kHugeBlockLimbs = (uint64_t)1 << 24;
+uint32_t accumulate_blocks(uint64_t L);
+cudaError_t launch_accumulate(uint64_t* out, uint64_t L, const uint64_t* add, uint64_t nadd, uint32_t* agg,
+                              uint32_t* cin, cudaStream_t st);
+
 // Host <-> device copies of the host API: page-locked caller memory goes
 // straight to the copy engines, pageable memory through a ring of
 // page-locked slots filled by a pool of host threads.  host_to_device may

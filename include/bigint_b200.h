@@ -29,7 +29,7 @@ extern "C" {
 #define BGPU_ERR_INVALID_ARG -1   /* null pointer, zero length, digit >= 2^28 ... */
 #define BGPU_ERR_NO_DEVICE -2     /* no CUDA device / CUDA runtime error at init */
 #define BGPU_ERR_OOM -3           /* device or pinned-host allocation failed */
-#define BGPU_ERR_CAPACITY -4      /* product beyond the largest supported transform */
+#define BGPU_ERR_CAPACITY -4      /* size beyond what the entry point supports */
 #define BGPU_ERR_OUT_CAPACITY -5  /* caller's output buffer too small; *out_len = needed */
 #define BGPU_ERR_CUDA -6          /* CUDA error during the multiply */
 #define BGPU_ERR_DEVICE_TIMEOUT -7/* a bounded device-side wait gave up (carry look-back), or the
@@ -85,7 +85,10 @@ const char* bgpu_strerror(int code);
 /* Product of u64-limb integers: the `_mul` seam (include/bigint/mul.h:208-220)
  * and ntt::mul (src/mul/ntt_multithread.cpp:444-530).  Writes the product
  * without leading zeros into out[0..*out_len).  A zero operand gives
- * *out_len == 0 (brute::mul's result, include/bigint/mul.h:82-102). */
+ * *out_len == 0 (brute::mul's result, include/bigint/mul.h:82-102).  Products
+ * above 2^31 bits, beyond the largest transform (where the reference uses
+ * ssa::mul, src/mul/ssa.cpp:383), run as blocks of 2^30-bit NTT products
+ * added on the device; na + nb is limited to 2^31 limbs. */
 int bgpu_mul_u64(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
                  size_t out_cap, size_t* out_len, uint32_t flags, bgpu_stats* stats);
 
@@ -127,8 +130,9 @@ int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t 
  * (include/bigint/bigint_base.h:60-69, the squaring chain its benchmark
  * example times, examples/benchmark.cpp:22), every product on the GPU with no
  * host round trip between them.  Writes the power without leading zeros;
- * 0^0 = 1 like the reference's res = 1.  BGPU_ERR_CAPACITY when a product of
- * the chain exceeds the largest transform. */
+ * 0^0 = 1 like the reference's res = 1.  Products beyond the largest
+ * transform run as its blocks, as in bgpu_mul_u64; BGPU_ERR_CAPACITY when
+ * the power exceeds 2^30 limbs. */
 int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
                  size_t out_cap, size_t* out_len);
 

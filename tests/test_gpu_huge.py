@@ -1,0 +1,116 @@
+"""Products beyond the largest transform (2^26 points, 2^31 product bits).
+
+The reference switches to Schoenhage-Strassen there (src/mul/ssa.cpp:383);
+the engine cuts both operands into 2^30-bit blocks, multiplies every block
+pair on the NTT and adds the block products into the result with a device
+carry scan.  At these sizes the CPU oracle takes minutes, so the checks are
+size-independent: the residue identity mod 2^61-1, the low limb, operand
+order, and the all-ones closed form, whose carries cross every block
+boundary."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import SEED, rand_digits, rand_limbs
+
+pytestmark = pytest.mark.gpu
+M61 = (1 << 61) - 1
+ONES = np.uint64(0xFFFFFFFFFFFFFFFF)
+BLOCK = 1 << 24  # limbs per operand block
+
+
+def check_product(port, a, b, c):
+    assert c.size == a.size + b.size
+    assert port.mod_m61(a) * port.mod_m61(b) % M61 == port.mod_m61(c)
+    assert (int(a[0]) * int(b[0])) & ((1 << 64) - 1) == int(c[0])
+
+
+def test_general_2p31_product(bb, port):
+    """2^31 x 2^31 bits: four block products."""
+    rng = np.random.default_rng(SEED + 500)
+    n = 2 * BLOCK
+    a, b = rand_limbs(rng, n), rand_limbs(rng, n)
+    c, st = bb.mul(a, b, stats=True)
+    check_product(port, a, b, c)
+    assert np.array_equal(bb.mul(b, a), c)
+
+
+def test_uneven_blocks_and_ragged_tails(bb, port):
+    rng = np.random.default_rng(SEED + 501)
+    a, b = rand_limbs(rng, 3 * BLOCK + 5), rand_limbs(rng, BLOCK + 77)
+    c = bb.mul(a, b)
+    check_product(port, a, b, c)
+    assert np.array_equal(bb.mul(b, a), c)
+
+
+def test_all_ones_square_crosses_blocks(bb):
+    """(2^k - 1)^2 = 2^2k - 2^(k+1) + 1: every block product's carry runs
+    through the all-ones limbs of the result."""
+    n = 2 * BLOCK + 3
+    ones = np.full(n, ONES)
+    c = bb.mul(ones)
+    assert c.size == 2 * n
+    assert c[0] == 1 and not c[1:n].any() and c[n] == np.uint64(0xFFFFFFFFFFFFFFFE)
+    assert np.all(c[n + 1:] == ONES)
+    c2 = bb.mul(ones, ones.copy())  # distinct buffers: the general path
+    assert np.array_equal(c2, c)
+
+
+def test_square_matches_general(bb, port):
+    rng = np.random.default_rng(SEED + 502)
+    a = rand_limbs(rng, 2 * BLOCK + 1000)
+    sq = bb.mul(a)
+    assert np.array_equal(sq, bb.mul(a, a.copy()))
+    ra = port.mod_m61(a)
+    assert ra * ra % M61 == port.mod_m61(sq)
+
+
+def test_device_entry(bb, port):
+    import torch
+
+    rng = np.random.default_rng(SEED + 503)
+    a, b = rand_limbs(rng, BLOCK + 12345), rand_limbs(rng, BLOCK + 999)
+    dev = torch.device("cuda", 0)
+    da = torch.from_numpy(a.view(np.int64)).to(dev)
+    db = torch.from_numpy(b.view(np.int64)).to(dev)
+    out = torch.empty(a.size + b.size, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    bb.mul_device(da.data_ptr(), a.size, db.data_ptr(), b.size, out.data_ptr())
+    bb.device_status()
+    check_product(port, a, b, out.cpu().numpy().view(np.uint64))
+
+
+def mod_m61_digits(d: np.ndarray) -> int:
+    """(sum d_i 2^(28 i)) mod 2^61-1 for 28-bit digits, vectorised: 2^(28 i)
+    is a rotation by 28 i mod 61 bits."""
+    d = d.astype(np.uint64)
+    e = (np.arange(d.size, dtype=np.uint64) * np.uint64(28)) % np.uint64(61)
+    low = (d & ((np.uint64(1) << (np.uint64(61) - e)) - np.uint64(1))) << e
+    high = d >> (np.uint64(61) - e)
+    v = (low + high) % np.uint64(M61)  # each term reduced
+    while v.size > 1:  # pairwise sums, folded back below 2^61 at every level
+        if v.size & 1:
+            v = np.append(v, np.uint64(0))
+        v = v[0::2] + v[1::2]
+        v = (v & np.uint64(M61)) + (v >> np.uint64(61))
+    return int(v[0]) % M61
+
+
+def test_digits_beyond_the_transform(bb):
+    """mul_digits above 2^31 product bits goes through u64 limbs and the block
+    products."""
+    rng = np.random.default_rng(SEED + 504)
+    n = (1 << 30) // 28 + 1000  # two operands just over 2^30 bits each
+    a, b = rand_digits(rng, n), rand_digits(rng, n)
+    c = bb.mul_digits(a, b)
+    assert mod_m61_digits(a) * mod_m61_digits(b) % M61 == mod_m61_digits(c)
+    assert (int(a[0]) * int(b[0])) & ((1 << 28) - 1) == int(c[0])
+
+
+def test_fast_pow_crosses_the_transform(bb, port):
+    """A squaring chain whose last products are beyond the largest transform."""
+    base, e = 3, 3 * (1 << 30) // 2  # 3^e: about 2^31.2 bits
+    got = bb.fast_pow(base, e)
+    assert port.mod_m61(got) == pow(base, e, M61)
+    assert int(got[0]) == pow(base, e, 1 << 64)
