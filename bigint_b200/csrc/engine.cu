@@ -652,9 +652,8 @@ int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags
         it[i] = {na, nb, square};
         slot_in = std::max(slot_in, align256(na * 8) + align256(nb * 8));
         slot_out = std::max(slot_out, align256((na + nb) * 8));
-        if (na && nb && !small_method(flags, na, nb)) {
-            const int ln = ceil_log2(2 * (uint64_t)(na + nb) - 1);
-            if (ln > kMaxLogN) return BGPU_ERR_CAPACITY;
+        if (na && nb && !small_method(flags, na, nb)) {  // beyond the largest transform: its blocks
+            const int ln = std::min(kMaxLogN, ceil_log2(2 * (uint64_t)(na + nb) - 1));
             max_ln = std::max(max_ln, ln < 5 ? 5 : ln);
         }
     }
@@ -696,6 +695,8 @@ int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags
             if (const uint32_t sm = small_method(flags, m.na, m.nb)) {
                 rc = launch_small(sm, da, m.na, db, m.nb, dout, st);
                 nl += 1;
+            } else if (beyond_transform(m.na, m.nb)) {
+                rc = huge_product(da, m.na, db, m.nb, dout, m.square, st);
             } else {
                 OperandDesc oa{da, (uint32_t)m.na, (uint32_t)(2 * m.na), kFmtLimb64};
                 OperandDesc ob{db, (uint32_t)m.nb, (uint32_t)(2 * m.nb), kFmtLimb64};

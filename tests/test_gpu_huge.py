@@ -114,3 +114,14 @@ def test_fast_pow_crosses_the_transform(bb, port):
     got = bb.fast_pow(base, e)
     assert port.mod_m61(got) == pow(base, e, M61)
     assert int(got[0]) == pow(base, e, 1 << 64)
+
+
+def test_pipelined_host_api_with_a_huge_product(bb, port):
+    """bgpu_mul_u64_many: a product beyond the transform between ordinary ones."""
+    rng = np.random.default_rng(SEED + 505)
+    pairs = [(rand_limbs(rng, 5000), rand_limbs(rng, 7000)),
+             (rand_limbs(rng, BLOCK + 3), rand_limbs(rng, BLOCK + 5)),
+             (rand_limbs(rng, 100), rand_limbs(rng, 60))]
+    outs = bb.mul_many(pairs)
+    for (a, b), c in zip(pairs, outs):
+        check_product(port, a, b, c)
