@@ -582,6 +582,44 @@ def reciprocal_form(bb, cpu: bool = True, reps: int = 5):
     return res
 
 
+def decimal_print_form(cpu: bool = True):
+    """Decimal conversion of a 2^22-bit integer (1.26 M digits) by the
+    reference's own BigInt::print (src/bigint.cpp:175-247: print_dec's
+    divide and conquer over get_pow_of_ten and divmod), unmodified C++ with
+    its products hooked to this engine (bigint_b200/hooks/reference_hook.cpp),
+    beside the same code on the host cores alone; the two strings compared.
+    The conversion itself has no GPU kernels of its own: this measures what the
+    drop-in hook gives the reference's decimal output."""
+    from oracle.pyoracle import REF_GPU_SO, Reference, have_reference, have_reference_gpu
+
+    if not have_reference_gpu():
+        return {"unavailable": "oracle/_ref/libbigint_ref_gpu.so not built"}
+    rng = np.random.default_rng(SEED + 8)
+    limbs = rng.integers(0, 2**64, (1 << 22) // 64, dtype=np.uint64)
+    limbs[-1] |= np.uint64(1 << 63)
+    hooked = Reference(REF_GPU_SO)
+    hooked.init_thread_pool(1)
+    if not hooked.has_to_dec:
+        return {"unavailable": "reference shim without ref_to_dec_string"}
+    hooked.to_dec_string(limbs[:4096])
+    t0 = time.perf_counter()
+    s_gpu = hooked.to_dec_string(limbs)
+    res = {"input_bits": 1 << 22, "decimal_digits": len(s_gpu),
+           "reference_code_on_gpu": {"s": time.perf_counter() - t0,
+                                     "call": "BigInt::print with ntt::mul / fft::mul hooked to bgpu_mul_u64"}}
+    if cpu and have_reference():
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        ref.to_dec_string(limbs[:4096])
+        t0 = time.perf_counter()
+        s_cpu = ref.to_dec_string(limbs)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(), "call": "BigInt::print"}
+        if s_cpu != s_gpu:
+            raise SystemExit("bench decimal: hooked reference prints a different number")
+        res["verified"] = "identical decimal text"
+    return res
+
+
 def limbs_to_digits28_np(limbs) -> np.ndarray:
     """u64 limbs -> little-endian 28-bit digits without leading zeros."""
     bits = np.unpackbits(np.ascontiguousarray(limbs, dtype=np.uint64).view(np.uint8), bitorder="little")
@@ -924,6 +962,7 @@ def run_gpu_arm(args) -> None:
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
+                 "decimal_print_2p22": decimal_print_form(cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
                                                 cpu=(rank == 0 and not args.no_cpu_baseline))}
@@ -973,7 +1012,7 @@ def run_gpu_arm(args) -> None:
 
 
 FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
-         "batched_4096",
+         "decimal_print_2p22", "batched_4096",
          "product_tree_2p20")
 
 
@@ -1005,6 +1044,8 @@ def run_single_form(args) -> None:
         res = mul_digits_form(bb, port, cpu=not args.no_cpu_baseline)
     elif name == "reciprocal_2p24":
         res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
+    elif name == "decimal_print_2p22":
+        res = decimal_print_form(cpu=not args.no_cpu_baseline)
     elif name == "batched_4096":
         res = batched_form(bb, torch, device, port)
     else:

@@ -157,6 +157,10 @@ class Reference(_Lib):
                                                   _u32p, C.c_size_t, _szp, C.POINTER(C.c_int64),
                                                   C.POINTER(C.c_int)]
             L.ref_bigfloat_reciprocal.restype = C.c_int
+        self.has_to_dec = hasattr(L, "ref_to_dec_string")
+        if self.has_to_dec:
+            L.ref_to_dec_string.argtypes = [_u64p, C.c_size_t, C.c_char_p, C.c_size_t, _szp]
+            L.ref_to_dec_string.restype = C.c_int
         self.has_reciprocal = hasattr(L, "ref_reciprocal")
         if self.has_reciprocal:
             L.ref_reciprocal.argtypes = [_u64p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t, _szp,
@@ -223,6 +227,18 @@ class Reference(_Lib):
             raise OracleError(f"ref_bigfloat_reciprocal returned {rc}")
         return ((din[: nin.value].copy(), int(ppin.value), bool(neg)),
                 (out[: nout.value].copy(), int(pp.value), bool(oneg.value)))
+
+    def to_dec_string(self, limbs) -> str:
+        """Decimal text of the integer with little-endian u64 ``limbs``
+        (BigInt::print)."""
+        leaves = _limbs(limbs)
+        cap = int(leaves.size * 64 * 0.30103) + 32
+        out = C.create_string_buffer(cap)
+        n = C.c_size_t(0)
+        rc = self.lib.ref_to_dec_string(_p64(leaves), leaves.size, out, cap, C.byref(n))
+        if rc != 0:
+            raise OracleError(f"ref_to_dec_string returned {rc}")
+        return out.raw[: n.value].decode()
 
     def fast_pow_digits(self, base: int, exponent: int) -> np.ndarray:
         """fast_pow(BigInt(base), exponent) as reference 28-bit Digits."""

@@ -15,6 +15,7 @@
 //   ref_fast_pow    -> bigint::fast_pow<BigInt>   include/bigint/bigint_base.h:60
 //   ref_reciprocal  -> BigFloat::reciprocal       src/bigint.cpp:1044 (Newton, BigFloat::mul)
 //   ref_bigfloat_reciprocal -> the same on BigFloat(x, offset), negated on request
+//   ref_to_dec_string -> BigInt::print (decimal)  src/bigint.cpp:175-247
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -22,6 +23,7 @@
 #include <cstdint>
 #include <cstring>
 #include <span>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -161,6 +163,26 @@ int ref_bigfloat_reciprocal(const uint64_t* limbs, size_t n, int64_t offset, int
     *point_pos = r.get_point_pos();
     *out_neg = r.sign() < 0 ? 1 : 0;
     return copy_out32(r.get_data(), out, cap, out_len);
+}
+
+// Decimal text of X (little-endian u64 limbs, built through the hex-string
+// constructor, src/bigint.cpp:25) by BigInt::print (src/bigint.cpp:175-247,
+// print_dec's divide-and-conquer over get_pow_of_ten and divmod).  Returns -1
+// when cap is too small (out_len holds the size needed).
+int ref_to_dec_string(const uint64_t* limbs, size_t n, char* out, size_t cap, size_t* out_len) {
+    static const char hexd[] = "0123456789abcdef";
+    std::string hex;
+    hex.reserve(16 * n);
+    for (size_t i = n; i-- > 0;)
+        for (int k = 15; k >= 0; --k) hex.push_back(hexd[(limbs[i] >> (4 * k)) & 15]);
+    bigint::BigInt x(hex, true);
+    std::ostringstream os;
+    x.print(os);
+    const std::string s = os.str();
+    *out_len = s.size();
+    if (s.size() > cap) return -1;
+    std::memcpy(out, s.data(), s.size());
+    return 0;
 }
 
 // fast_pow over BigInt, as the reference's benchmark example calls it
