@@ -59,3 +59,26 @@ def test_bigfloat_reciprocal(bb, reference, reference_gpu, nleaves, prec):
     dg, pg = reference_gpu.reciprocal_digits(leaves, prec)
     dr, pr = reference.reciprocal_digits(leaves, prec)
     assert pg == pr and np.array_equal(dg, dr)
+
+
+@pytest.mark.parametrize("nlimbs", [1000, 16384])
+def test_decimal_print(bb, reference, reference_gpu, nlimbs):
+    """BigInt::print (src/bigint.cpp:175-247): print_dec's divmod and
+    get_pow_of_ten products go through the hook; the decimal text must not
+    change."""
+    if not reference.has_to_dec:
+        pytest.skip("reference shim without ref_to_dec_string")
+    rng = np.random.default_rng(SEED + 94 + nlimbs)
+    limbs = rng.integers(0, 2**64, nlimbs, dtype=np.uint64)
+    limbs[-1] |= np.uint64(1 << 63)
+    text = reference_gpu.to_dec_string(limbs)
+    assert text == reference.to_dec_string(limbs)
+    if nlimbs == 1000:  # small enough for Python's own conversion
+        import sys
+
+        old = sys.get_int_max_str_digits()
+        sys.set_int_max_str_digits(0)
+        try:
+            assert text == str(int.from_bytes(limbs.tobytes(), "little"))
+        finally:
+            sys.set_int_max_str_digits(old)
