@@ -15,6 +15,7 @@ this package           reference                                       C-ABI
 ``  precision, pos)``
 ``fast_pow(base, e)``  ``fast_pow<BigInt>`` (bigint_base.h:60-69)      ``bgpu_pow_u64``
 ``reciprocal_digits``  ``BigFloat::reciprocal`` (bigint.cpp:1044-1071) ``bgpu_reciprocal_digits``
+``from_decimal(text)`` ``BigInt(const std::string&)`` (bigint.cpp:25-124) ``bgpu_from_decimal``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
 =====================  ==============================================  =========================
 
@@ -46,6 +47,7 @@ from ._lib import (  # noqa: F401
     brute_mul,
     device_status,
     fft_mul,
+    from_decimal,
     get_batch_split,
     get_split,
     get_tuning,

@@ -103,6 +103,8 @@ def _load() -> C.CDLL:
     L.bgpu_mul_u64_many.restype = C.c_int
     L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]
     L.bgpu_pow_u64.restype = C.c_int
+    L.bgpu_from_decimal.argtypes = [C.c_char_p, C.c_size_t, u32p, C.c_size_t, szp, C.POINTER(C.c_int)]
+    L.bgpu_from_decimal.restype = C.c_int
     L.bgpu_reciprocal_digits.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, u32p,
                                          C.c_size_t, szp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.bgpu_reciprocal_digits.restype = C.c_int
@@ -379,6 +381,21 @@ def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = Non
     if stats:
         return ret, _stats(st)
     return ret
+
+
+def from_decimal(text):
+    """Decimal text to ``(Digits, negative)``, as the reference's
+    ``BigInt(const std::string&)`` reads it (src/bigint.cpp:25-124): a '-'
+    before the first digit makes it negative, other non-digits are skipped.
+    The value is built on the GPU (``bgpu_from_decimal``)."""
+    _ensure_init()
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    cap = len(b) // 8 + 8
+    out = np.empty(cap, dtype=np.uint32)
+    n, neg = C.c_size_t(0), C.c_int(0)
+    _check(lib.bgpu_from_decimal(b, len(b), out.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(n),
+                                 C.byref(neg)), "bgpu_from_decimal")
+    return out[: n.value], bool(neg.value)
 
 
 def reciprocal_digits(digits, point_pos: int = 0, neg: bool = False, precision: int = 0):

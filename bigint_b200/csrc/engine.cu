@@ -51,6 +51,9 @@ struct Engine {
     // block products of the decomposition beyond the largest transform
     void* d_huge = nullptr;
     size_t huge_bytes = 0;
+    // decimal conversion: digits, two level arrays, powers of ten, output
+    void* d_dec = nullptr;
+    size_t dec_bytes = 0;
     // stream and scratch layout of the last NTT product launched
     cudaStream_t ntt_stream = nullptr;
     int ntt_log_n = -1;
@@ -90,6 +93,7 @@ void release_locked() {
     cudaFree(g.d_fft_err);
     cudaFree(g.d_scratch);
     cudaFree(g.d_huge);
+    cudaFree(g.d_dec);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
@@ -1412,6 +1416,109 @@ static EngineHooks hooks_locked() {
     for (int ps = 0; ps < kNumSets; ++ps) h.consts[ps] = g.consts[ps];
     h.err = g.d_err;
     return h;
+}
+
+// Decimal text to Digits: BigInt(const std::string&) with hex = false
+// (src/bigint.cpp:25-90) and convert_from_dec_string (:92-124).  The sign and
+// the digit characters are picked out on the host exactly as the reference
+// reads them; the value is built on the device (decimal.cu): leaves of 19
+// digits, then levels of hi * 10^(19 * 2^j) + lo, each level one batch plan
+// of equal products and one segmented carry add.
+static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t out_cap, size_t* out_len,
+                               int* out_neg) {
+    size_t i = 0;
+    bool neg = false;
+    for (; i < len; ++i) {  // before the first digit, any '-' makes the number negative
+        const unsigned char c = (unsigned char)s[i];
+        if (c >= '0' && c <= '9') break;
+        if (c == '-') neg = true;
+    }
+    std::vector<uint8_t> dig;
+    dig.reserve(len - i);
+    for (; i < len; ++i) {  // other characters are skipped; leading zeros dropped
+        const unsigned char c = (unsigned char)s[i];
+        if (c < '0' || c > '9' || (dig.empty() && c == '0')) continue;
+        dig.push_back((uint8_t)(c - '0'));
+    }
+    const uint64_t D = dig.size();
+    if (D == 0) {  // the reference's zero: one digit 0, not negative
+        *out_len = 1;
+        *out_neg = 0;
+        if (out_cap < 1) return BGPU_ERR_OUT_CAPACITY;
+        out[0] = 0;
+        return BGPU_OK;
+    }
+    const uint64_t leaves = (D + 18) / 19;
+    const int J = ceil_log2(leaves);
+    if (J > 25) return BGPU_ERR_CAPACITY;  // the top level's product is the largest general transform
+    const uint64_t NL = (uint64_t)1 << J;  // limbs of every level
+    const uint32_t w0 = (uint32_t)std::min<uint64_t>(32, NL);
+    int j0 = 0;
+    while ((1u << j0) < w0) ++j0;
+    const uint64_t nd = (64 * NL + 27) / 28;  // Digits of the result, before stripping
+    const size_t dig_off = 0, lvl_off = align256(D), q_off = lvl_off + 2 * align256(NL * 8);
+    const size_t o_off = q_off + align256(NL * 8);
+    int rc = ensure(&g.d_dec, &g.dec_bytes, o_off + align256(nd * 4));
+    if (rc != BGPU_OK) return rc;
+    char* base = static_cast<char*>(g.d_dec);
+    uint8_t* ddig = reinterpret_cast<uint8_t*>(base + dig_off);
+    uint64_t* lvl[2] = {reinterpret_cast<uint64_t*>(base + lvl_off),
+                        reinterpret_cast<uint64_t*>(base + lvl_off + align256(NL * 8))};
+    uint64_t* q = reinterpret_cast<uint64_t*>(base + q_off);  // 10^(19 * 2^j) at limb 2^j - 1, 2^j limbs
+    uint32_t* dout = reinterpret_cast<uint32_t*>(base + o_off);
+    cudaStream_t st = g.stream;
+    rc = host_to_device(ddig, dig.data(), D, st, nullptr);
+    if (rc != BGPU_OK) return rc;
+    const uint64_t ten19 = 10000000000000000000ull;
+    cudaError_t e = cudaMemcpyAsync(q, &ten19, 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    uint32_t nl = 0;
+    for (int j = 0; j + 1 < J; ++j) {  // 10^(19 * 2^(j+1)) = (10^(19 * 2^j))^2, on the device
+        const uint64_t w = (uint64_t)1 << j;
+        rc = device_product(q + (w - 1), w, q + (w - 1), w, q + (2 * w - 1), st, &nl);
+        if (rc != BGPU_OK) return rc;
+    }
+    e = launch_dec_leaves(ddig, D, w0, NL / w0, lvl[0], st);
+    if (e != cudaSuccess) return cuda_status(e);
+    int cur = 0;
+    std::vector<bgpu_product> prods;
+    for (int j = j0; j < J; ++j) {
+        const uint64_t w1 = (uint64_t)1 << j, pairs = NL / (2 * w1);
+        prods.resize(pairs);
+        for (uint64_t p = 0; p < pairs; ++p)
+            prods[p] = bgpu_product{lvl[cur] + (2 * p + 1) * w1, w1, q + (w1 - 1), w1, lvl[cur ^ 1] + p * 2 * w1};
+        bgpu_batch_plan_s* plan = nullptr;
+        rc = batch_plan_create(prods.data(), pairs, BGPU_METHOD_AUTO, g.device, hooks_locked(), &plan);
+        if (rc != BGPU_OK) return rc;
+        rc = batch_plan_run(plan, st);
+        if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
+        batch_plan_destroy(plan);
+        if (rc != BGPU_OK) return rc;
+        e = launch_seg_add_low(lvl[cur ^ 1], lvl[cur], (uint32_t)w1, pairs, st);
+        if (e != cudaSuccess) return cuda_status(e);
+        cur ^= 1;
+    }
+    e = launch_limbs_to_digits28(lvl[cur], (uint32_t)NL, dout, (uint32_t)nd, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    std::vector<uint32_t> h(nd);
+    rc = device_to_host(h.data(), dout, nd * 4, st);
+    rc = check_device_error(rc);
+    if (rc != BGPU_OK) return rc;
+    const size_t n = strip32(h.data(), nd);
+    *out_len = n;
+    *out_neg = neg ? 1 : 0;
+    if (n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+    memcpy(out, h.data(), n * 4);
+    g.last_launches = nl;
+    return BGPU_OK;
+}
+
+int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, size_t* out_len, int* is_neg) {
+    if ((!s && len) || !out_len || !is_neg || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return from_decimal_locked(s, len, out, out_cap, out_len, is_neg);
 }
 
 int bgpu_batch_plan_create(const bgpu_product* products, size_t count, uint32_t flags,

@@ -260,6 +260,14 @@ uint32_t accumulate_blocks(uint64_t L);
 cudaError_t launch_accumulate(uint64_t* out, uint64_t L, const uint64_t* add, uint64_t nadd, uint32_t* agg,
                               uint32_t* cin, cudaStream_t st);
 
+// Decimal text to binary (decimal.cu): leaves of 19 digits built w limbs per
+// segment (w <= 32) from dig[0..D) (values 0..9, most significant first), and
+// out[p*2w1 ..] += prev[2p*w1 .. 2p*w1 + w1) over nseg segments of 2*w1 limbs.
+cudaError_t launch_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64_t nseg, uint64_t* out,
+                              cudaStream_t st);
+cudaError_t launch_seg_add_low(uint64_t* out, const uint64_t* prev, uint32_t w1, uint64_t nseg,
+                               cudaStream_t st);
+
 // Host <-> device copies of the host API: page-locked caller memory goes
 // straight to the copy engines, pageable memory through a ring of
 // page-locked slots filled by a pool of host threads.  host_to_device may

@@ -136,6 +136,17 @@ int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t 
 int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
                  size_t out_cap, size_t* out_len);
 
+/* Decimal text to a BigInt: the reference's BigInt(const std::string&) with
+ * hex = false (src/bigint.cpp:25-90) and its convert_from_dec_string
+ * (:92-124).  Characters before the first digit may hold '-' (the number is
+ * then negative); characters that are not digits are skipped.  Writes the
+ * BigInt's Digits (28-bit, no leading zeros; zero is the single digit 0, not
+ * negative) and its sign.  The value is built on the GPU: 19-digit leaves
+ * paired level by level through hi * 10^(19 * 2^j) + lo, every level one batch
+ * of equal-size products.  Up to 19 * 2^25 digits (BGPU_ERR_CAPACITY above). */
+int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, size_t* out_len,
+                      int* is_neg);
+
 /* Reciprocal of a BigFloat: BigFloat::reciprocal(precision)
  * (src/bigint.cpp:1044-1071), its Newton iteration
  * x += mul(x, 1 - mul(b, x, p + 1), p + 1) run with every value on the GPU

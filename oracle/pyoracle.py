@@ -161,6 +161,11 @@ class Reference(_Lib):
         if self.has_to_dec:
             L.ref_to_dec_string.argtypes = [_u64p, C.c_size_t, C.c_char_p, C.c_size_t, _szp]
             L.ref_to_dec_string.restype = C.c_int
+        self.has_from_dec = hasattr(L, "ref_from_dec_string")
+        if self.has_from_dec:
+            L.ref_from_dec_string.argtypes = [C.c_char_p, C.c_size_t, _u32p, C.c_size_t, _szp,
+                                              C.POINTER(C.c_int)]
+            L.ref_from_dec_string.restype = C.c_int
         self.has_reciprocal = hasattr(L, "ref_reciprocal")
         if self.has_reciprocal:
             L.ref_reciprocal.argtypes = [_u64p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t, _szp,
@@ -239,6 +244,16 @@ class Reference(_Lib):
         if rc != 0:
             raise OracleError(f"ref_to_dec_string returned {rc}")
         return out.raw[: n.value].decode()
+
+    def from_dec_string(self, text: bytes):
+        """BigInt(text) (decimal): (Digits, negative)."""
+        cap = len(text) // 8 + 8
+        out = np.zeros(cap, dtype=np.uint32)
+        n, neg = C.c_size_t(0), C.c_int(0)
+        rc = self.lib.ref_from_dec_string(text, len(text), _p32(out), cap, C.byref(n), C.byref(neg))
+        if rc != 0:
+            raise OracleError(f"ref_from_dec_string returned {rc}")
+        return out[: n.value].copy(), bool(neg.value)
 
     def fast_pow_digits(self, base: int, exponent: int) -> np.ndarray:
         """fast_pow(BigInt(base), exponent) as reference 28-bit Digits."""

@@ -16,6 +16,7 @@
 //   ref_reciprocal  -> BigFloat::reciprocal       src/bigint.cpp:1044 (Newton, BigFloat::mul)
 //   ref_bigfloat_reciprocal -> the same on BigFloat(x, offset), negated on request
 //   ref_to_dec_string -> BigInt::print (decimal)  src/bigint.cpp:175-247
+//   ref_from_dec_string -> BigInt(std::string)     src/bigint.cpp:25-124
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -183,6 +184,14 @@ int ref_to_dec_string(const uint64_t* limbs, size_t n, char* out, size_t cap, si
     if (s.size() > cap) return -1;
     std::memcpy(out, s.data(), s.size());
     return 0;
+}
+
+// BigInt(const std::string&) (decimal; src/bigint.cpp:25-124): the Digits
+// and the sign of the parsed number.
+int ref_from_dec_string(const char* s, size_t len, uint32_t* out, size_t cap, size_t* out_len, int* neg) {
+    const bigint::BigInt x(std::string(s, len), false);
+    *neg = x.sign() < 0 ? 1 : 0;
+    return copy_out32(x.get_data(), out, cap, out_len);
 }
 
 // fast_pow over BigInt, as the reference's benchmark example calls it
