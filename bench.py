@@ -620,6 +620,40 @@ def decimal_print_form(cpu: bool = True):
     return res
 
 
+def decimal_parse_form(bb, cpu: bool = True):
+    """Decimal text of 5 M digits (about 2^24 bits) to a BigInt: the
+    reference's BigInt(const std::string&) (src/bigint.cpp:25-124) on the
+    host cores beside bgpu_from_decimal (leaves and level products on the
+    GPU), host text in and host Digits out, results compared."""
+    rng = np.random.default_rng(SEED + 9)
+    d = rng.integers(0, 10, 5_000_000, dtype=np.uint8)
+    d[0] = 4
+    text = (d + ord("0")).tobytes()
+    bb.from_decimal(text[:100000])
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        got, neg = bb.from_decimal(text)
+        times.append(time.perf_counter() - t0)
+    res = {"decimal_digits": len(text), "s": statistics.median(times), "api": "bgpu_from_decimal"}
+    from oracle.pyoracle import Reference, have_reference
+
+    if have_reference() and Reference().has_from_dec:
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        ref.from_dec_string(text[:100000])
+        if cpu:
+            t0 = time.perf_counter()
+        want, wneg = ref.from_dec_string(text)
+        if cpu:
+            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                    "call": "BigInt(const std::string&)"}
+        if not (np.array_equal(got, want) and neg == wneg):
+            raise SystemExit("bench decimal parse: result differs from the reference's")
+        res["verified"] = "identical Digits"
+    return res
+
+
 def limbs_to_digits28_np(limbs) -> np.ndarray:
     """u64 limbs -> little-endian 28-bit digits without leading zeros."""
     bits = np.unpackbits(np.ascontiguousarray(limbs, dtype=np.uint64).view(np.uint8), bitorder="little")
@@ -963,6 +997,7 @@ def run_gpu_arm(args) -> None:
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
                  "decimal_print_2p22": decimal_print_form(cpu=not args.no_cpu_baseline),
+                 "decimal_parse_5m": decimal_parse_form(bb, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
                                                 cpu=(rank == 0 and not args.no_cpu_baseline))}
@@ -1012,7 +1047,7 @@ def run_gpu_arm(args) -> None:
 
 
 FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
-         "decimal_print_2p22", "batched_4096",
+         "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
          "product_tree_2p20")
 
 
@@ -1046,6 +1081,8 @@ def run_single_form(args) -> None:
         res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_print_2p22":
         res = decimal_print_form(cpu=not args.no_cpu_baseline)
+    elif name == "decimal_parse_5m":
+        res = decimal_parse_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "batched_4096":
         res = batched_form(bb, torch, device, port)
     else:

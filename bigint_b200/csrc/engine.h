@@ -261,7 +261,7 @@ cudaError_t launch_accumulate(uint64_t* out, uint64_t L, const uint64_t* add, ui
                               uint32_t* cin, cudaStream_t st);
 
 // Decimal text to binary (decimal.cu): leaves of 19 digits built w limbs per
-// segment (w <= 32) from dig[0..D) (values 0..9, most significant first), and
+// segment (w <= 128) from dig[0..D) (values 0..9, most significant first), and
 // out[p*2w1 ..] += prev[2p*w1 .. 2p*w1 + w1) over nseg segments of 2*w1 limbs.
 cudaError_t launch_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64_t nseg, uint64_t* out,
                               cudaStream_t st);
