@@ -582,21 +582,29 @@ def reciprocal_form(bb, cpu: bool = True, reps: int = 5):
     return res
 
 
-def decimal_print_form(cpu: bool = True):
-    """Decimal conversion of a 2^22-bit integer (1.26 M digits) by the
-    reference's own BigInt::print (src/bigint.cpp:175-247: print_dec's
-    divide and conquer over get_pow_of_ten and divmod), unmodified C++ with
-    its products hooked to this engine (bigint_b200/hooks/reference_hook.cpp),
-    beside the same code on the host cores alone; the two strings compared.
-    The conversion itself has no GPU kernels of its own: this measures what the
-    drop-in hook gives the reference's decimal output."""
+def decimal_print_form(bb, cpu: bool = True):
+    """Decimal text of a 2^22-bit integer (1.26 M digits): bgpu_to_decimal
+    (the whole conversion on the GPU, host Digits in, host text out); the
+    reference's own BigInt::print (src/bigint.cpp:175-247: print_dec's divide
+    and conquer over get_pow_of_ten and divmod), unmodified C++, with its
+    products hooked to this engine (bigint_b200/hooks/reference_hook.cpp); and
+    the same code on the host cores alone.  All three strings compared."""
     from oracle.pyoracle import REF_GPU_SO, Reference, have_reference, have_reference_gpu
 
-    if not have_reference_gpu():
-        return {"unavailable": "oracle/_ref/libbigint_ref_gpu.so not built"}
     rng = np.random.default_rng(SEED + 8)
     limbs = rng.integers(0, 2**64, (1 << 22) // 64, dtype=np.uint64)
     limbs[-1] |= np.uint64(1 << 63)
+    digits = limbs_to_digits28_np(limbs)
+    bb.to_decimal(digits[:1000])
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        s_native = bb.to_decimal(digits)
+        times.append(time.perf_counter() - t0)
+    res = {"input_bits": 1 << 22, "decimal_digits": len(s_native), "s": statistics.median(times),
+           "api": "bgpu_to_decimal"}
+    if not have_reference_gpu():
+        return res
     hooked = Reference(REF_GPU_SO)
     hooked.init_thread_pool(1)
     if not hooked.has_to_dec:
@@ -604,9 +612,10 @@ def decimal_print_form(cpu: bool = True):
     hooked.to_dec_string(limbs[:4096])
     t0 = time.perf_counter()
     s_gpu = hooked.to_dec_string(limbs)
-    res = {"input_bits": 1 << 22, "decimal_digits": len(s_gpu),
-           "reference_code_on_gpu": {"s": time.perf_counter() - t0,
-                                     "call": "BigInt::print with ntt::mul / fft::mul hooked to bgpu_mul_u64"}}
+    res["reference_code_on_gpu"] = {"s": time.perf_counter() - t0,
+                                    "call": "BigInt::print with ntt::mul / fft::mul hooked to bgpu_mul_u64"}
+    if s_gpu != s_native:
+        raise SystemExit("bench decimal: bgpu_to_decimal and the hooked reference print different text")
     if cpu and have_reference():
         ref = Reference()
         ref.init_thread_pool(host_cores())
@@ -616,7 +625,7 @@ def decimal_print_form(cpu: bool = True):
         res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(), "call": "BigInt::print"}
         if s_cpu != s_gpu:
             raise SystemExit("bench decimal: hooked reference prints a different number")
-        res["verified"] = "identical decimal text"
+        res["verified"] = "identical decimal text (native, hooked reference, pure reference)"
     return res
 
 
@@ -996,7 +1005,7 @@ def run_gpu_arm(args) -> None:
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
-                 "decimal_print_2p22": decimal_print_form(cpu=not args.no_cpu_baseline),
+                 "decimal_print_2p22": decimal_print_form(bb, cpu=not args.no_cpu_baseline),
                  "decimal_parse_5m": decimal_parse_form(bb, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
                  "product_tree_2p20": tree_form(bb, torch, device, port,
@@ -1080,7 +1089,7 @@ def run_single_form(args) -> None:
     elif name == "reciprocal_2p24":
         res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_print_2p22":
-        res = decimal_print_form(cpu=not args.no_cpu_baseline)
+        res = decimal_print_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_parse_5m":
         res = decimal_parse_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "batched_4096":

@@ -16,6 +16,7 @@ this package           reference                                       C-ABI
 ``fast_pow(base, e)``  ``fast_pow<BigInt>`` (bigint_base.h:60-69)      ``bgpu_pow_u64``
 ``reciprocal_digits``  ``BigFloat::reciprocal`` (bigint.cpp:1044-1071) ``bgpu_reciprocal_digits``
 ``from_decimal(text)`` ``BigInt(const std::string&)`` (bigint.cpp:25-124) ``bgpu_from_decimal``
+``to_decimal(d, neg)`` ``BigInt::print`` (bigint.cpp:175-247)          ``bgpu_to_decimal``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
 =====================  ==============================================  =========================
 
@@ -73,4 +74,5 @@ from ._lib import (  # noqa: F401
     set_kernel_timing,
     set_tuning,
     shutdown,
+    to_decimal,
 )

@@ -103,6 +103,8 @@ def _load() -> C.CDLL:
     L.bgpu_mul_u64_many.restype = C.c_int
     L.bgpu_pow_u64.argtypes = [u64p, C.c_size_t, C.c_uint32, u64p, C.c_size_t, szp]
     L.bgpu_pow_u64.restype = C.c_int
+    L.bgpu_to_decimal.argtypes = [u32p, C.c_size_t, C.c_int, C.c_char_p, C.c_size_t, szp]
+    L.bgpu_to_decimal.restype = C.c_int
     L.bgpu_from_decimal.argtypes = [C.c_char_p, C.c_size_t, u32p, C.c_size_t, szp, C.POINTER(C.c_int)]
     L.bgpu_from_decimal.restype = C.c_int
     L.bgpu_reciprocal_digits.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, u32p,
@@ -381,6 +383,22 @@ def mul_digits(a, b=None, output_precision: int = 0, point_pos: int | None = Non
     if stats:
         return ret, _stats(st)
     return ret
+
+
+def to_decimal(digits, neg: bool = False) -> str:
+    """Decimal text of a BigInt given by its 28-bit Digits and sign, as the
+    reference's ``BigInt::print`` writes it (src/bigint.cpp:175-247); the
+    conversion runs on the GPU (``bgpu_to_decimal``)."""
+    _ensure_init()
+    d = _as_digits(digits)
+    if d.size == 0:
+        raise BigIntGPUError(-1, "bgpu_to_decimal (empty input)")
+    cap = int(d.size * 28 * 0.30103) + 64
+    out = C.create_string_buffer(cap)
+    n = C.c_size_t(0)
+    _check(lib.bgpu_to_decimal(d.ctypes.data_as(C.POINTER(C.c_uint32)), d.size, int(bool(neg)), out, cap,
+                               C.byref(n)), "bgpu_to_decimal")
+    return out.raw[: n.value].decode()
 
 
 def from_decimal(text):

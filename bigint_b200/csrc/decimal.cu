@@ -125,7 +125,178 @@ __global__ void __launch_bounds__(kAddThreads) k_seg_add_low(uint64_t* out, cons
     }
 }
 
+// ---- binary to decimal -------------------------------------------------------
+//
+// The reverse walk: a level-j segment s < Q^2 (Q = 10^(19 w), w = 2^(j-1)
+// limbs) splits into s div Q and s mod Q.  The host has the exact reciprocal
+// V = floor(2^(128 w) / Q) and T = s * V and U = (T >> 128 w) * Q as batched
+// products; q = T >> 128 w is q_true or q_true - 1 (V exact, s < 2^(128 w)).
+// One block per segment then forms r = s - U and, when r >= Q, subtracts Q
+// once more and adds 1 to q.
+
+// Block-wide sum or difference of two limb runs with the carry (or borrow)
+// carried across tiles; out may alias x.  Returns the carry out.
+__device__ uint32_t block_addsub(uint64_t* out, const uint64_t* x, uint32_t nx, const uint64_t* y, uint32_t ny,
+                                 uint32_t n, bool sub, uint32_t cin) {
+    for (uint32_t t0 = 0; t0 < n; t0 += kAddTile) {
+        const uint32_t j0 = t0 + threadIdx.x * kAddPer;
+        uint64_t a[kAddPer], b[kAddPer];
+        uint32_t st = 2u;
+#pragma unroll
+        for (int k = 0; k < kAddPer; ++k) {
+            const uint32_t j = j0 + (uint32_t)k;
+            a[k] = j < nx ? x[j] : 0ull;
+            b[k] = j < ny ? y[j] : 0ull;
+            uint32_t g, pr;
+            if (sub) {
+                g = a[k] < b[k];
+                pr = a[k] == b[k];
+            } else {
+                const uint64_t t = a[k] + b[k];
+                g = t < a[k];
+                pr = t == ~0ull;
+            }
+            if (j < n) st = compose(st, g | (pr << 1));
+        }
+        uint32_t total;
+        const uint32_t before = block_exclusive(st, &total);
+        uint64_t c = (before & 1u) | ((before >> 1) & cin);
+#pragma unroll
+        for (int k = 0; k < kAddPer; ++k) {
+            const uint32_t j = j0 + (uint32_t)k;
+            if (j >= n) break;
+            if (sub) {
+                const uint64_t t = a[k] - b[k], r = t - c;
+                c = (uint64_t)(a[k] < b[k]) | (uint64_t)(t < c);
+                out[j] = r;
+            } else {
+                const uint64_t t = a[k] + b[k], r = t + c;
+                c = (uint64_t)(t < a[k]) | (uint64_t)(r < t);
+                out[j] = r;
+            }
+        }
+        cin = (total & 1u) | ((total >> 1) & cin);
+        __syncthreads();  // the next tile reads what this one wrote only through its own indices
+    }
+    return cin;
+}
+
+// 1 when x (nx limbs) >= y (ny limbs), block-wide.
+__device__ bool block_geq(const uint64_t* x, uint32_t nx, const uint64_t* y, uint32_t ny) {
+    __shared__ unsigned long long s_key;
+    if (threadIdx.x == 0) s_key = 0;
+    __syncthreads();
+    const uint32_t n = nx > ny ? nx : ny;
+    unsigned long long best = 0;
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const uint64_t a = j < nx ? x[j] : 0ull, b = j < ny ? y[j] : 0ull;
+        if (a != b) best = ((unsigned long long)(j + 1) << 1) | (a > b ? 1u : 0u);
+    }
+    if (best) atomicMax(&s_key, best);
+    __syncthreads();
+    const unsigned long long key = s_key;
+    __syncthreads();
+    return key == 0 || (key & 1u);
+}
+
+// Segment p of the level above (2w limbs at cur + 2 w p) with U_p = q * Q
+// (2w limbs at u + 2 w p) and q (w limbs at t + (2w + m) p + 2w) written as
+// the two halves of the level below: next[2 w p ..] = r, next[2 w p + w ..] = q.
+__global__ void __launch_bounds__(kAddThreads) k_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t,
+                                                             uint32_t tstride, const uint64_t* q_pow, uint32_t w,
+                                                             uint64_t* next) {
+    const uint64_t p = blockIdx.x;
+    const uint64_t* s = cur + 2 * (uint64_t)w * p;
+    uint64_t* r = u + 2 * (uint64_t)w * p;
+    uint64_t* q = t + (uint64_t)tstride * p + 2 * w;
+    block_addsub(r, s, 2 * w, r, 2 * w, 2 * w, true, 0);  // r = s - q Q, in place of U
+    __syncthreads();
+    if (block_geq(r, 2 * w, q_pow, w)) {  // q was one short
+        block_addsub(r, r, 2 * w, q_pow, w, 2 * w, true, 0);
+        __syncthreads();
+        block_addsub(q, q, w, nullptr, 0, w, false, 1);
+        __syncthreads();
+    }
+    uint64_t* lo = next + 2 * (uint64_t)w * p;
+    for (uint32_t j = threadIdx.x; j < w; j += blockDim.x) {
+        lo[j] = r[j];
+        lo[w + j] = q[j];
+    }
+}
+
+// Decimal text of segment p (w limbs, value < 10^(19 w)): 19 w characters,
+// most significant first, at out + 19 w (nseg - 1 - p); by repeated division
+// of its 32-bit halves by 10^9.
+__global__ void k_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nseg, char* out) {
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nseg) return;
+    uint32_t x[2 * kLeafLimbs];
+    const uint32_t nw = 2 * w;
+    for (uint32_t i = 0; i < w; ++i) {
+        const uint64_t v = in[p * w + i];
+        x[2 * i] = (uint32_t)v;
+        x[2 * i + 1] = (uint32_t)(v >> 32);
+    }
+    const uint32_t nchar = 19 * w;
+    char* o = out + (uint64_t)nchar * (nseg - 1 - p);
+    uint32_t top = nw;  // words above top are zero
+    for (uint32_t done = 0; done < nchar; done += 9) {
+        while (top > 0 && x[top - 1] == 0) --top;
+        uint64_t rem = 0;
+        for (uint32_t i = top; i-- > 0;) {
+            const uint64_t cur = (rem << 32) | x[i];
+            x[i] = (uint32_t)(cur / 1000000000u);
+            rem = cur % 1000000000u;
+        }
+        for (uint32_t k = 0; k < 9 && done + k < nchar; ++k) {
+            o[nchar - 1 - (done + k)] = (char)('0' + rem % 10);
+            rem /= 10;
+        }
+    }
+}
+
+// r[i] = ~x[i] for i < el, r[el] = 0 (then r + 1 = 2^(64 el) - x for 0 < x < 2^(64 el)).
+__global__ void k_not_limbs(const uint64_t* x, uint32_t el, uint64_t* r) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= el; i += gridDim.x * blockDim.x)
+        r[i] = i < el ? ~x[i] : 0ull;
+}
+
+// One block: when r (nr limbs) >= q (nq limbs), r -= q and v += 1 (nv limbs);
+// *flag = 1 if it did.
+__global__ void __launch_bounds__(kAddThreads) k_fix_step(uint64_t* r, uint32_t nr, const uint64_t* q, uint32_t nq,
+                                                          uint64_t* v, uint32_t nv, uint32_t* flag) {
+    const bool ge = block_geq(r, nr, q, nq);
+    if (ge) {
+        block_addsub(r, r, nr, q, nq, nr, true, 0);
+        __syncthreads();
+        block_addsub(v, v, nv, nullptr, 0, nv, false, 1);
+    }
+    if (threadIdx.x == 0) *flag = ge ? 1u : 0u;
+}
+
 }  // namespace
+
+cudaError_t launch_not_limbs(const uint64_t* x, uint32_t el, uint64_t* r, cudaStream_t st) {
+    k_not_limbs<<<(el + 256) / 256 < 1184 ? (el + 256) / 256 : 1184, 256, 0, st>>>(x, el, r);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fix_step(uint64_t* r, uint32_t nr, const uint64_t* q, uint32_t nq, uint64_t* v, uint32_t nv,
+                            uint32_t* flag, cudaStream_t st) {
+    k_fix_step<<<1, kAddThreads, 0, st>>>(r, nr, q, nq, v, nv, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t, uint32_t tstride, const uint64_t* q_pow,
+                               uint32_t w, uint64_t nseg, uint64_t* next, cudaStream_t st) {
+    k_seg_divstep<<<(uint32_t)nseg, kAddThreads, 0, st>>>(cur, u, t, tstride, q_pow, w, next);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nseg, char* out, cudaStream_t st) {
+    k_dec_print_leaves<<<(uint32_t)((nseg + 63) / 64), 64, 0, st>>>(in, w, nseg, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64_t nseg, uint64_t* out,
                               cudaStream_t st) {

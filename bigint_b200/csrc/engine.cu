@@ -1513,6 +1513,176 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
     return BGPU_OK;
 }
 
+// BigInt to decimal text: BigInt::print (src/bigint.cpp:175-247), the
+// reference's print_dec divide and conquer, on the device (decimal.cu).  The
+// value is split top-down into halves by Q_k = 10^(19 * 2^k): a level-j
+// segment s < Q_(j-1)^2 becomes s mod Q_(j-1) and s div Q_(j-1), the quotient
+// estimated with the exact reciprocal V_(j-1) = floor(2^(128 * 2^(j-1)) / Q_(j-1))
+// (two batched products per level) and corrected once per segment on the
+// device.  The reciprocals are a chain: V_k^2 is at most V_(k+1) (both are
+// floors of the same real, squared), one Newton step from below brings it
+// within a few units, and single correction steps make it exact.  Leaves of
+// 128 limbs print 2432 characters per thread.
+static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* out, size_t out_cap,
+                             size_t* out_len) {
+    for (size_t i = 0; i < n; ++i)
+        if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    n = strip32(digits, n);
+    if (n == 0) {  // the reference prints zero as "0", without a sign
+        *out_len = 1;
+        if (out_cap < 1) return BGPU_ERR_OUT_CAPACITY;
+        out[0] = '0';
+        return BGPU_OK;
+    }
+    const uint64_t bits = 28 * (uint64_t)(n - 1) + (32 - __builtin_clz(digits[n - 1]));
+    const uint64_t dmax = (uint64_t)std::ceil((double)bits * 0.30102999566398120) + 1;  // >= decimal digits
+    const int J = ceil_log2((dmax + 18) / 19);
+    if (J > 25) return BGPU_ERR_CAPACITY;
+    const uint64_t NL = (uint64_t)1 << J;
+    const uint32_t w0 = (uint32_t)std::min<uint64_t>(128, NL);
+    int jleaf = 0;
+    while ((1u << jleaf) < w0) ++jleaf;
+    auto mk = [](int k) { return ((uint64_t)1 << k) + (((uint64_t)1 << k) >> 6) + 2; };  // limbs of V_k
+    // arena (limbs)
+    uint64_t off = 0;
+    auto take = [&](uint64_t limbs) {
+        const uint64_t o = off;
+        off += (limbs + 31) & ~(uint64_t)31;
+        return o;
+    };
+    const uint64_t o_lvl0 = take(NL), o_lvl1 = take(NL), o_q = take(NL), o_v = take(NL + NL / 32 + 4 * J + 8);
+    const uint64_t o_t = take(2 * NL + 4 * J + 64), o_u = take(NL), o_x = take(7 * NL + 64), o_one = take(4);
+    const uint64_t o_dig = take((n + 1) / 2 + 1), o_chr = take((19 * NL + 7) / 8 + 1);
+    int rc = ensure(&g.d_dec, &g.dec_bytes, off * 8);
+    if (rc != BGPU_OK) return rc;
+    uint64_t* A = static_cast<uint64_t*>(g.d_dec);
+    uint64_t* lvl[2] = {A + o_lvl0, A + o_lvl1};
+    uint64_t* qp = A + o_q;
+    uint64_t* vp = A + o_v;
+    uint64_t* tb = A + o_t;
+    uint64_t* ub = A + o_u;
+    uint64_t* xs = A + o_x;
+    uint64_t* one = A + o_one;
+    uint32_t* flag = reinterpret_cast<uint32_t*>(A + o_one + 1);
+    uint32_t* ddig = reinterpret_cast<uint32_t*>(A + o_dig);
+    char* chars = reinterpret_cast<char*>(A + o_chr);
+    // carry-scan scratch of the chain's additions, in the (not yet used) U buffer
+    uint32_t* agg = reinterpret_cast<uint32_t*>(A + o_u);
+    uint32_t* cin = agg + ((accumulate_blocks(NL + 2) + 63) & ~63u);
+    std::vector<uint64_t> voff(J + 1, 0);
+    for (int k = 1; k <= J; ++k) voff[k] = voff[k - 1] + mk(k - 1);
+    cudaStream_t st = g.stream;
+
+    // the value, as NL limbs
+    rc = host_to_device(ddig, digits, n * 4, st, nullptr);
+    if (rc != BGPU_OK) return rc;
+    cudaError_t e = launch_digits28_to_limbs(ddig, (uint32_t)n, lvl[0], (uint32_t)NL, st);
+    const uint64_t consts[2] = {10000000000000000000ull, 1};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(qp, &consts[0], 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(one, &consts[1], 8, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    uint32_t nl = 0;
+    for (int k = 0; k + 1 < J; ++k) {  // Q_(k+1) = Q_k^2
+        const uint64_t w = (uint64_t)1 << k;
+        rc = device_product(qp + (w - 1), w, qp + (w - 1), w, qp + (2 * w - 1), st, &nl);
+        if (rc != BGPU_OK) return rc;
+    }
+    if (J > jleaf) {
+        // V_0 = floor(2^128 / 10^19), then the chain up to V_(J-1)
+        const unsigned __int128 v0 = ~(unsigned __int128)0 / 10000000000000000000ull;
+        std::vector<uint64_t> hv(mk(0), 0);
+        hv[0] = (uint64_t)v0;
+        hv[1] = (uint64_t)(v0 >> 64);
+        e = cudaMemcpyAsync(vp, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e);
+        for (int k = 0; k + 1 < J; ++k) {
+            const uint64_t K = (uint64_t)1 << (k + 1), el = 2 * K, m = mk(k), m1 = mk(k + 1);
+            const uint64_t* q = qp + (K - 1);
+            uint64_t* v = vp + voff[k];
+            uint64_t* v1 = vp + voff[k + 1];
+            uint64_t* X = xs;                    // 2m
+            uint64_t* P = X + 2 * m + 8;         // K + 2m
+            uint64_t* R = P + K + 2 * m + 8;     // el + 1
+            uint64_t* Dd = R + el + 8;           // 2m + el + 1
+            rc = device_product(v, m, v, m, X, st, &nl);  // X = V_k^2 <= V_(k+1)
+            if (rc == BGPU_OK) rc = device_product(q, K, X, 2 * m, P, st, &nl);  // P = Q X < 2^(64 el)
+            if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
+            if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
+            if (rc == BGPU_OK) rc = device_product(X, 2 * m, R, el + 1, Dd, st, &nl);  // X (2^E - Q X)
+            // V' = X + floor(X R / 2^E): Newton from below, within a few units of V_(k+1)
+            if (rc == BGPU_OK) rc = cuda_status(cudaMemsetAsync(v1, 0, m1 * 8, st));
+            if (rc == BGPU_OK)
+                rc = cuda_status(cudaMemcpyAsync(v1, X, std::min(2 * m, m1) * 8, cudaMemcpyDeviceToDevice, st));
+            if (rc == BGPU_OK)
+                rc = cuda_status(launch_accumulate(v1, m1, Dd + el, std::min<uint64_t>(2 * m + 1, m1),
+                                                   agg, cin, st));
+            // exact: R = 2^E - Q V' (>= 0); while R >= Q: R -= Q, V' += 1
+            if (rc == BGPU_OK) rc = device_product(q, K, v1, m1, P, st, &nl);
+            if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
+            if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
+            for (int it = 0; rc == BGPU_OK; ++it) {
+                if (it == 64) return BGPU_ERR_CUDA;  // the Newton step is within a few units
+                uint32_t f = 0;
+                rc = cuda_status(launch_fix_step(R, (uint32_t)(el + 1), q, (uint32_t)K, v1, (uint32_t)m1, flag, st));
+                if (rc == BGPU_OK) rc = cuda_status(cudaMemcpyAsync(&f, flag, 4, cudaMemcpyDeviceToHost, st));
+                if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
+                if (!f) break;
+            }
+            if (rc != BGPU_OK) return rc;
+        }
+    }
+    // top-down division levels
+    int cur = 0;
+    std::vector<bgpu_product> prods;
+    for (int j = J; j > jleaf; --j) {
+        const uint64_t w = (uint64_t)1 << (j - 1), count = NL >> j, m = mk(j - 1), ts = 2 * w + m;
+        const uint64_t* q = qp + (w - 1);
+        const uint64_t* v = vp + voff[j - 1];
+        for (int pass = 0; pass < 2; ++pass) {
+            prods.resize(count);
+            for (uint64_t p = 0; p < count; ++p)
+                prods[p] = pass == 0
+                               ? bgpu_product{lvl[cur] + 2 * w * p, 2 * w, v, m, tb + ts * p}
+                               : bgpu_product{tb + ts * p + 2 * w, w, q, w, ub + 2 * w * p};
+            bgpu_batch_plan_s* plan = nullptr;
+            rc = batch_plan_create(prods.data(), count, BGPU_METHOD_AUTO, g.device, hooks_locked(), &plan);
+            if (rc != BGPU_OK) return rc;
+            rc = batch_plan_run(plan, st);
+            if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
+            batch_plan_destroy(plan);
+            if (rc != BGPU_OK) return rc;
+        }
+        e = launch_seg_divstep(lvl[cur], ub, tb, (uint32_t)ts, q, (uint32_t)w, count, lvl[cur ^ 1], st);
+        if (e != cudaSuccess) return cuda_status(e);
+        cur ^= 1;
+    }
+    e = launch_dec_print_leaves(lvl[cur], w0, NL / w0, chars, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    std::vector<char> h(19 * NL);
+    rc = device_to_host(h.data(), chars, h.size(), st);
+    rc = check_device_error(rc);
+    if (rc != BGPU_OK) return rc;
+    size_t first = 0;
+    while (first + 1 < h.size() && h[first] == '0') ++first;
+    const size_t len = (h.size() - first) + (neg ? 1 : 0);
+    *out_len = len;
+    g.last_launches = nl;
+    if (len > out_cap) return BGPU_ERR_OUT_CAPACITY;
+    size_t o = 0;
+    if (neg) out[o++] = '-';
+    memcpy(out + o, h.data() + first, h.size() - first);
+    return BGPU_OK;
+}
+
+int bgpu_to_decimal(const uint32_t* digits, size_t n, int is_neg, char* out, size_t out_cap, size_t* out_len) {
+    if (!digits || n == 0 || !out_len || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return to_decimal_locked(digits, n, is_neg != 0, out, out_cap, out_len);
+}
+
 int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, size_t* out_len, int* is_neg) {
     if ((!s && len) || !out_len || !is_neg || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(g_mu);

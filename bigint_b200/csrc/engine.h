@@ -268,6 +268,18 @@ cudaError_t launch_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64
 cudaError_t launch_seg_add_low(uint64_t* out, const uint64_t* prev, uint32_t w1, uint64_t nseg,
                                cudaStream_t st);
 
+// Binary to decimal (decimal.cu): one block per level-above segment of 2w
+// limbs, r = s - U and the one-step quotient correction, written as the two
+// w-limb halves of the level below; the decimal text of w-limb leaves; the
+// complement r = ~x over el limbs (r[el] = 0); and one exact correction step
+// of a reciprocal (r >= q: r -= q, v += 1, *flag = 1).
+cudaError_t launch_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t, uint32_t tstride, const uint64_t* q_pow,
+                               uint32_t w, uint64_t nseg, uint64_t* next, cudaStream_t st);
+cudaError_t launch_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nseg, char* out, cudaStream_t st);
+cudaError_t launch_not_limbs(const uint64_t* x, uint32_t el, uint64_t* r, cudaStream_t st);
+cudaError_t launch_fix_step(uint64_t* r, uint32_t nr, const uint64_t* q, uint32_t nq, uint64_t* v, uint32_t nv,
+                            uint32_t* flag, cudaStream_t st);
+
 // Host <-> device copies of the host API: page-locked caller memory goes
 // straight to the copy engines, pageable memory through a ring of
 // page-locked slots filled by a pool of host threads.  host_to_device may

@@ -136,6 +136,15 @@ int bgpu_mul_u64_many(const bgpu_host_product* products, size_t count, uint32_t 
 int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t* out,
                  size_t out_cap, size_t* out_len);
 
+/* BigInt to decimal text: the reference's BigInt::print (src/bigint.cpp:175-247,
+ * print_dec).  The input is the BigInt's Digits (28-bit) and sign; writes the
+ * text ('-' for a negative nonzero value, no leading zeros, "0" for zero),
+ * identical to the reference's, not NUL-terminated.  The conversion runs on
+ * the GPU: halves by 10^(19 * 2^k) top down, with exact reciprocals and
+ * batched products, and leaves of 2432 digits.  BGPU_ERR_OUT_CAPACITY when
+ * out_cap is too small (*out_len = needed). */
+int bgpu_to_decimal(const uint32_t* digits, size_t n, int is_neg, char* out, size_t out_cap, size_t* out_len);
+
 /* Decimal text to a BigInt: the reference's BigInt(const std::string&) with
  * hex = false (src/bigint.cpp:25-90) and its convert_from_dec_string
  * (:92-124).  Characters before the first digit may hold '-' (the number is

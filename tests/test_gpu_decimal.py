@@ -80,3 +80,56 @@ def test_large(bb, ref):
     d = rng.integers(0, 10, 1262612, dtype=np.uint8)
     d[0] = 3
     check(bb, ref, (d + ord("0")).tobytes())
+
+
+# ---- BigInt to decimal text (bgpu_to_decimal) against BigInt::print ----------
+
+def print_check(bb, ref, d, neg=False):
+    from oracle.pyoracle import digits28_to_limbs
+
+    got = bb.to_decimal(d, neg)
+    limbs = digits28_to_limbs(d)
+    want = ref.to_dec_string(limbs) if limbs.size else "0"
+    if neg and want != "0":
+        want = "-" + want
+    assert got == want, (d.size, got[:30], want[:30], len(got), len(want))
+
+
+def test_print_small_and_edges(bb, ref):
+    for v in [0, 1, 9, 10, 10**19 - 1, 10**19, 10**19 + 1, 2**64 - 1, 2**64, 10**38, 10**57 - 1, 2**200]:
+        d = np.array([(v >> (28 * i)) & ((1 << 28) - 1) for i in range(max(1, (v.bit_length() + 27) // 28))],
+                     dtype=np.uint32)
+        print_check(bb, ref, d)
+        print_check(bb, ref, d, neg=True)
+
+
+def test_print_sizes_across_levels(bb, ref):
+    """Values whose decimal length crosses the 2432-digit leaves and each
+    division level."""
+    rng = np.random.default_rng(SEED + 610)
+    for decimal_len in [100, 2431, 2432, 2433, 4865, 9729, 20000, 77824, 77825, 155649, 400000]:
+        nd = int(decimal_len / 0.30103 / 28) + 1
+        d = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
+        d[-1] = 1 + d[-1] % ((1 << 27) - 1)
+        print_check(bb, ref, d)
+
+
+def test_print_powers_of_ten_and_ones(bb, ref):
+    """10^k - 1, 10^k and all-ones Digits: quotient corrections at every level."""
+    for k in (2432, 4864, 9728, 19456, 38912):
+        text = "9" * k
+        d, _ = bb.from_decimal(text)
+        assert bb.to_decimal(d) == text
+        d, _ = bb.from_decimal("1" + "0" * k)
+        assert bb.to_decimal(d) == "1" + "0" * k
+    print_check(bb, ref, np.full(30000, (1 << 28) - 1, dtype=np.uint32))
+
+
+def test_print_round_trip_large(bb, ref):
+    rng = np.random.default_rng(SEED + 611)
+    dd = rng.integers(0, 10, 1262612, dtype=np.uint8)
+    dd[0] = 5
+    text = (dd + ord("0")).tobytes().decode()
+    d, neg = bb.from_decimal(text)
+    assert bb.to_decimal(d, neg) == text
+    print_check(bb, ref, d)
