@@ -54,6 +54,8 @@ struct Engine {
     // decimal conversion: digits, two level arrays, powers of ten, output
     void* d_dec = nullptr;
     size_t dec_bytes = 0;
+    void* d_desc = nullptr;  // small-product descriptors of the decimal levels
+    size_t desc_bytes = 0;
     // stream and scratch layout of the last NTT product launched
     cudaStream_t ntt_stream = nullptr;
     int ntt_log_n = -1;
@@ -94,6 +96,7 @@ void release_locked() {
     cudaFree(g.d_scratch);
     cudaFree(g.d_huge);
     cudaFree(g.d_dec);
+    cudaFree(g.d_desc);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
@@ -1418,6 +1421,46 @@ static EngineHooks hooks_locked() {
     return h;
 }
 
+// A batch of equal-size device products on `st` (the levels of the decimal
+// conversions): schoolbook or Karatsuba classes as one launch over a
+// descriptor array, up to 128 transform-size products as direct launches,
+// more through a batch plan.
+static int run_products(const bgpu_product* pr, size_t count, cudaStream_t st, uint32_t* launches) {
+    if (count == 0) return BGPU_OK;
+    const size_t na = pr[0].na, nb = pr[0].nb;
+    const Tuning& tu = tuning();
+    const bool school = na + nb <= tu.batch_schoolbook_max_limbs;
+    if (school || (na + nb <= tu.batch_karatsuba_max_limbs && karatsuba_fits(na, nb))) {
+        std::vector<SchoolDesc> d(count);
+        for (size_t i = 0; i < count; ++i)
+            d[i] = SchoolDesc{pr[i].a, pr[i].b, pr[i].out, (uint32_t)pr[i].na, (uint32_t)pr[i].nb};
+        int rc = ensure(&g.d_desc, &g.desc_bytes, count * sizeof(SchoolDesc));
+        if (rc != BGPU_OK) return rc;
+        cudaError_t e = cudaMemcpyAsync(g.d_desc, d.data(), count * sizeof(SchoolDesc), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // d goes out of scope
+        const SchoolDesc* dd = static_cast<const SchoolDesc*>(g.d_desc);
+        if (e == cudaSuccess)
+            e = school ? launch_schoolbook_batch(dd, (uint32_t)count, st) : launch_karatsuba_batch(dd, (uint32_t)count, st);
+        *launches += 1;
+        return cuda_status(e);
+    }
+    if (count <= 128) {
+        for (size_t i = 0; i < count; ++i) {
+            const int rc = device_product(pr[i].a, pr[i].na, pr[i].b, pr[i].nb, pr[i].out, st, launches);
+            if (rc != BGPU_OK) return rc;
+        }
+        return BGPU_OK;
+    }
+    bgpu_batch_plan_s* plan = nullptr;
+    int rc = batch_plan_create(pr, count, BGPU_METHOD_AUTO, g.device, hooks_locked(), &plan);
+    if (rc != BGPU_OK) return rc;
+    rc = batch_plan_run(plan, st);
+    if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
+    *launches += batch_plan_launches(plan);
+    batch_plan_destroy(plan);
+    return rc;
+}
+
 // Decimal text to Digits: BigInt(const std::string&) with hex = false
 // (src/bigint.cpp:25-90) and convert_from_dec_string (:92-124).  The sign and
 // the digit characters are picked out on the host exactly as the reference
@@ -1487,12 +1530,7 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
         prods.resize(pairs);
         for (uint64_t p = 0; p < pairs; ++p)
             prods[p] = bgpu_product{lvl[cur] + (2 * p + 1) * w1, w1, q + (w1 - 1), w1, lvl[cur ^ 1] + p * 2 * w1};
-        bgpu_batch_plan_s* plan = nullptr;
-        rc = batch_plan_create(prods.data(), pairs, BGPU_METHOD_AUTO, g.device, hooks_locked(), &plan);
-        if (rc != BGPU_OK) return rc;
-        rc = batch_plan_run(plan, st);
-        if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
-        batch_plan_destroy(plan);
+        rc = run_products(prods.data(), pairs, st, &nl);
         if (rc != BGPU_OK) return rc;
         e = launch_seg_add_low(lvl[cur ^ 1], lvl[cur], (uint32_t)w1, pairs, st);
         if (e != cudaSuccess) return cuda_status(e);
@@ -1645,12 +1683,7 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
                 prods[p] = pass == 0
                                ? bgpu_product{lvl[cur] + 2 * w * p, 2 * w, v, m, tb + ts * p}
                                : bgpu_product{tb + ts * p + 2 * w, w, q, w, ub + 2 * w * p};
-            bgpu_batch_plan_s* plan = nullptr;
-            rc = batch_plan_create(prods.data(), count, BGPU_METHOD_AUTO, g.device, hooks_locked(), &plan);
-            if (rc != BGPU_OK) return rc;
-            rc = batch_plan_run(plan, st);
-            if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
-            batch_plan_destroy(plan);
+            rc = run_products(prods.data(), count, st, &nl);
             if (rc != BGPU_OK) return rc;
         }
         e = launch_seg_divstep(lvl[cur], ub, tb, (uint32_t)ts, q, (uint32_t)w, count, lvl[cur ^ 1], st);
