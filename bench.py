@@ -603,6 +603,23 @@ def decimal_print_form(bb, cpu: bool = True):
         times.append(time.perf_counter() - t0)
     res = {"input_bits": 1 << 22, "decimal_digits": len(s_native), "s": statistics.median(times),
            "api": "bgpu_to_decimal"}
+    # a 46.6 M-digit number (2,418,800 limbs), printed and parsed back on the
+    # GPU; the reference's decimal conversion takes minutes at this size, so
+    # each direction is checked against it at the size above and in the tests
+    big = rng.integers(0, 2**64, 2_418_800, dtype=np.uint64)
+    big[-1] |= np.uint64(1 << 63)
+    big_digits = limbs_to_digits28_np(big)
+    bb.to_decimal(big_digits)
+    t0 = time.perf_counter()
+    text = bb.to_decimal(big_digits)
+    t_print = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    back, _ = bb.from_decimal(text)
+    t_parse = time.perf_counter() - t0
+    if not np.array_equal(back, big_digits):
+        raise SystemExit("bench decimal: 46.6 M-digit round trip differs")
+    res["large"] = {"input_bits": int(big.size * 64), "decimal_digits": len(text), "to_decimal_s": t_print,
+                    "from_decimal_s": t_parse, "verified": "round trip identical"}
     if not have_reference_gpu():
         return res
     hooked = Reference(REF_GPU_SO)
