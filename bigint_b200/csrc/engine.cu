@@ -56,6 +56,7 @@ struct Engine {
     size_t dec_bytes = 0;
     void* d_desc = nullptr;  // small-product descriptors of the decimal levels
     size_t desc_bytes = 0;
+    unsigned long long* h_small = nullptr;  // page-locked readback words of the step-by-step paths
     // stream and scratch layout of the last NTT product launched
     cudaStream_t ntt_stream = nullptr;
     int ntt_log_n = -1;
@@ -97,6 +98,7 @@ void release_locked() {
     cudaFree(g.d_huge);
     cudaFree(g.d_dec);
     cudaFree(g.d_desc);
+    if (g.h_small) cudaFreeHost(g.h_small);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
@@ -876,10 +878,24 @@ uint32_t* rslot(int k, size_t words, int* rc) {
 }
 
 // Runs what is queued and reads `count` words back.
+// Small readbacks go through one page-locked block (a pageable copy costs a
+// driver staging pass per call).  Device errors are not read here: the
+// callers check the sticky error word once, at the end or on failure.
+unsigned long long* small_host() {
+    if (!g.h_small && cudaHostAlloc(reinterpret_cast<void**>(&g.h_small), 64, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        g.h_small = nullptr;
+    }
+    return g.h_small;
+}
+
 int read_back(const uint32_t* d, uint32_t* h, size_t count) {
-    cudaError_t e = cudaMemcpyAsync(h, d, count * 4, cudaMemcpyDeviceToHost, g.stream);
+    unsigned long long* hp = count <= 16 ? small_host() : nullptr;
+    void* dst = hp ? static_cast<void*>(hp) : static_cast<void*>(h);
+    cudaError_t e = cudaMemcpyAsync(dst, d, count * 4, cudaMemcpyDeviceToHost, g.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
-    return check_device_error(cuda_status(e));
+    if (e == cudaSuccess && hp) memcpy(h, hp, count * 4);
+    return cuda_status(e);
 }
 
 // The four-word result block of the compare and extent kernels, zeroed.
@@ -901,9 +917,7 @@ int extent(unsigned long long* dr, const uint32_t* d, size_t n, size_t from0, si
                                   (uint32_t)std::min<size_t>(from1, UINT32_MAX), dr, g.stream);
     if (e != cudaSuccess) return cuda_status(e);
     unsigned long long h[4];
-    e = cudaMemcpyAsync(h, dr, sizeof(h), cudaMemcpyDeviceToHost, g.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
-    const int rc = check_device_error(cuda_status(e));
+    const int rc = read_back(reinterpret_cast<const uint32_t*>(dr), reinterpret_cast<uint32_t*>(h), 8);
     if (rc != BGPU_OK) return rc;
     r[0] = (uint32_t)(h[0] >> 32);
     r[3] = (uint32_t)h[0];
@@ -1187,8 +1201,27 @@ int upload_digits(int slot, const std::vector<uint32_t>& v, int64_t pp, bool neg
     return BGPU_OK;
 }
 
+int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool neg, size_t precision,
+                     uint32_t* out, size_t out_cap, size_t* out_len, int64_t* out_pp, int* out_neg);
+
+// A failed step-by-step call reports a device-side error (sticky, e.g. a
+// carry-scan timeout in one of its products) in preference to what the
+// failure looked like on the host, and leaves the error word clear.
+int with_device_status(int rc) {
+    if (rc == BGPU_OK || rc == BGPU_ERR_OUT_CAPACITY) return rc;
+    cudaStreamSynchronize(g.stream);
+    const int dev = check_device_error(BGPU_OK);
+    return dev != BGPU_OK ? dev : rc;
+}
+
 int reciprocal_locked(const uint32_t* digits, size_t n, int64_t point_pos, bool neg, size_t precision,
                       uint32_t* out, size_t out_cap, size_t* out_len, int64_t* out_pp, int* out_neg) {
+    return with_device_status(reciprocal_steps(digits, n, point_pos, neg, precision, out, out_cap, out_len,
+                                               out_pp, out_neg));
+}
+
+int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool neg, size_t precision,
+                     uint32_t* out, size_t out_cap, size_t* out_len, int64_t* out_pp, int* out_neg) {
     if (n >= ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
     for (size_t i = 0; i < n; ++i)
         if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
@@ -1663,8 +1696,7 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
                 if (it == 64) return BGPU_ERR_CUDA;  // the Newton step is within a few units
                 uint32_t f = 0;
                 rc = cuda_status(launch_fix_step(R, (uint32_t)(el + 1), q, (uint32_t)K, v1, (uint32_t)m1, flag, st));
-                if (rc == BGPU_OK) rc = cuda_status(cudaMemcpyAsync(&f, flag, 4, cudaMemcpyDeviceToHost, st));
-                if (rc == BGPU_OK) rc = cuda_status(cudaStreamSynchronize(st));
+                if (rc == BGPU_OK) rc = read_back(flag, &f, 1);
                 if (!f) break;
             }
             if (rc != BGPU_OK) return rc;
@@ -1713,7 +1745,7 @@ int bgpu_to_decimal(const uint32_t* digits, size_t n, int is_neg, char* out, siz
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
-    return to_decimal_locked(digits, n, is_neg != 0, out, out_cap, out_len);
+    return with_device_status(to_decimal_locked(digits, n, is_neg != 0, out, out_cap, out_len));
 }
 
 int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, size_t* out_len, int* is_neg) {
@@ -1721,7 +1753,7 @@ int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, 
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
-    return from_decimal_locked(s, len, out, out_cap, out_len, is_neg);
+    return with_device_status(from_decimal_locked(s, len, out, out_cap, out_len, is_neg));
 }
 
 int bgpu_batch_plan_create(const bgpu_product* products, size_t count, uint32_t flags,
