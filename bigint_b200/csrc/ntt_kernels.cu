@@ -820,12 +820,17 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     }
     if (a.out_fmt == kFmtLimb64) {
         uint64_t* o = static_cast<uint64_t*>(pd.out);
+        const bool vec = (reinterpret_cast<uintptr_t>(o) & 15u) == 0;  // 16-byte stores when aligned
 #pragma unroll
         for (int i = 0; i < kCarryPer; ++i) {
             const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
             if (cc >= ntot) continue;
             const size_t base = (size_t)cc * 4;
-            if (base + 4 <= out_cap) {
+            if (base + 4 <= out_cap && vec) {
+                ulonglong2* d = reinterpret_cast<ulonglong2*>(o + base);
+                d[0] = make_ulonglong2(S[i][0], S[i][1]);
+                d[1] = make_ulonglong2(S[i][2], S[i][3]);
+            } else if (base + 4 <= out_cap) {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) o[base + k] = S[i][k];
             } else {
