@@ -338,12 +338,17 @@ bool auto_fft(uint32_t flags, size_t na, size_t nb) {
 
 constexpr double kFftMaxErr = 0.25;  // larger rounding distances are recomputed on the NTT
 
+unsigned long long* small_host();
+
 int check_device_error(int rc) {
     if (rc != BGPU_OK) return rc;
     uint32_t err = 0;
-    cudaError_t e = cudaMemcpyAsync(&err, g.d_err, sizeof(err), cudaMemcpyDeviceToHost, g.stream);
+    unsigned long long* hp = small_host();  // page-locked: no driver staging pass
+    uint32_t* dst = hp ? reinterpret_cast<uint32_t*>(hp + 7) : &err;
+    cudaError_t e = cudaMemcpyAsync(dst, g.d_err, sizeof(err), cudaMemcpyDeviceToHost, g.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g.stream);
     if (e != cudaSuccess) return cuda_status(e);
+    err = *dst;
     if (err) {
         // Clear the error and restart the carry-scan tickets from zero, so a
         // launch that failed part-way cannot leave the counter and the host's
