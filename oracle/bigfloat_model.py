@@ -1,0 +1,175 @@
+"""Step model of the device-resident reciprocal (test infrastructure only).
+
+A pure-Python restatement, on Python integers, of the steps the engine runs
+on the GPU for ``bgpu_reciprocal_digits`` (bigint_b200/csrc/engine.cu), which
+replay the reference's BigFloat::reciprocal (src/bigint.cpp:1044-1071):
+
+* ``mul_trunc`` -- BigFloat::mul with the truncation of mul_digits
+  (include/bigint/mul.h:227-243, 301-312), computed the device's way: the
+  truncated operands keep any zero digits at their bottom, and the first
+  nonzero digit at or above the cut (``hi - prec`` for the two possible
+  product lengths) is the result's bottom;
+* ``add_or_sub`` -- BigFloat::add_or_sub (src/bigint.cpp:849-936) as the exact
+  sum or difference in the reference's frame, leading and bottom zeros
+  removed;
+* ``shift``, ``to_double``, ``from_double`` -- src/bigint.cpp:681-812.
+
+tests/test_oracle_bigfloat.py pins this model against the reference's own
+reciprocal; the GPU tests pin the device against the reference.  Only the
+tests import this module.
+"""
+from __future__ import annotations
+
+import struct
+
+MASK = (1 << 28) - 1
+
+
+def _int(d):
+    return sum(int(x) << (28 * i) for i, x in enumerate(d))
+
+
+def _digits(v: int, n: int):
+    return [(v >> (28 * i)) & MASK for i in range(n)]
+
+
+def _ctrunc_div(a: int, b: int) -> int:  # C++ integer division (toward zero)
+    q = abs(a) // b
+    return q if a >= 0 else -q
+
+
+class Val:
+    """A BigFloat: digits (28-bit, little endian), point position, sign."""
+
+    def __init__(self, d, pp: int, neg: bool):
+        self.d, self.pp, self.neg = [int(x) for x in d], int(pp), bool(neg)
+
+    def zero(self) -> bool:
+        return len(self.d) == 1 and self.d[0] == 0
+
+    def tz(self) -> int:
+        t = 0
+        while t < len(self.d) and self.d[t] == 0:
+            t += 1
+        return t
+
+
+def plan_shift(pp: int, offset: int, low: int):
+    """BigFloat::shift's choice (src/bigint.cpp:769-789): (pp, mode, s)."""
+    pp -= _ctrunc_div(offset, 28)
+    o = offset - _ctrunc_div(offset, 28) * 28
+    if o == 0:
+        return pp, 0, 0
+    if o > 0:
+        o = 28 - o
+        pp -= 1
+    else:
+        o = -o
+    ctz = (low & -low).bit_length() - 1 if low else 32
+    if ctz >= o:
+        return pp, 1, o
+    return pp + 1, 2, 28 - o
+
+
+def shift(v: Val, offset: int) -> Val:
+    pp, mode, s = plan_shift(v.pp, offset, v.d[0])
+    d, n = list(v.d), len(v.d)
+    if mode == 1:
+        d = [((d[i] >> s) | ((d[i + 1] << (28 - s)) if i + 1 < n else 0)) & MASK for i in range(n)]
+    elif mode == 2:
+        d = [(((d[i] << s) if i < n else 0) | ((d[i - 1] >> (28 - s)) if i > 0 else 0)) & MASK
+             for i in range(n + 1)]
+    while len(d) > 1 and d[-1] == 0:
+        d.pop()
+    neg = v.neg
+    if len(d) == 1 and d[0] == 0:
+        pp, neg = 0, False
+    return Val(d, pp, neg)
+
+
+def mul_trunc(a: Val, b: Val, prec: int) -> Val:
+    if a.zero() or b.zero():
+        return Val([0], 0, False)
+    oa = len(a.d) - prec if len(a.d) > prec else 0
+    ob = len(b.d) - prec if len(b.d) > prec else 0
+    la, lb = len(a.d) - oa, len(b.d) - ob
+    res = _digits(_int(a.d[oa:]) * _int(b.d[ob:]), la + lb + 1)
+    hi = max(i for i, x in enumerate(res) if x) + 1
+    assert hi in (la + lb - 1, la + lb)
+    cut = hi - prec if hi > prec else 0
+    first = min(i for i in range(cut, hi) if res[i])
+    return Val(res[first:hi], a.pp + b.pp - (oa + ob + first), a.neg != b.neg)
+
+
+def add_or_sub(a: Val, b: Val, is_sub: bool) -> Val:
+    if a.zero():
+        return Val(b.d, b.pp, (not b.neg) if (is_sub and not b.zero()) else b.neg)
+    if b.zero():
+        return a
+    ppr = max(a.pp - a.tz(), b.pp - b.tz())
+    length = max(len(a.d) - a.pp, len(b.d) - b.pp) + ppr
+    A = _int(a.d) << (28 * (ppr - a.pp)) if ppr >= a.pp else _int(a.d) >> (28 * (a.pp - ppr))
+    B = _int(b.d) << (28 * (ppr - b.pp)) if ppr >= b.pp else _int(b.d) >> (28 * (b.pp - ppr))
+    neg = a.neg
+    if a.neg != (b.neg != is_sub):
+        if A == B:
+            return Val([0], 0, False)
+        if B > A:
+            A, B, neg = B, A, not neg
+        r = A - B
+    else:
+        r = A + B
+    res = _digits(r, length + 1)
+    hi = max(i for i, x in enumerate(res) if x) + 1
+    lo = min(i for i, x in enumerate(res) if x)
+    return Val(res[lo:hi], ppr - lo, neg)
+
+
+def to_double(b: Val) -> float:
+    n, top = len(b.d), b.d[-1]
+    hbw = top.bit_length()
+    e = 28 * (n - 1 - b.pp) + hbw - 1
+    off = 52 - (hbw - 1)
+    mant = (top & ((1 << (hbw - 1)) - 1)) << off
+    i = n - 1
+    while off > 0 and i > 0:
+        off -= 28
+        i -= 1
+        mant |= b.d[i] >> -off if off < 0 else b.d[i] << off
+    return struct.unpack("<d", struct.pack("<Q", (int(b.neg) << 63) | ((e + 1023) << 52) | mant))[0]
+
+
+def from_double(v: float) -> Val:
+    raw = struct.unpack("<Q", struct.pack("<d", v))[0]
+    neg, eb, base = bool(raw >> 63), (raw >> 52) & 2047, raw & ((1 << 52) - 1)
+    off = -52 - 1023
+    if eb == 0:
+        off += 1
+    else:
+        base |= 1 << 52
+        off += eb
+    d = []
+    while base:
+        d.append(base & MASK)
+        base >>= 28
+    return shift(Val(d, 0, neg), off)
+
+
+def reciprocal(digits, pp: int, neg: bool, precision: int) -> Val:
+    d = [int(x) for x in digits]
+    if precision == 0:
+        precision = len(d)
+    expo = 28 * (len(d) - 1 - pp) + d[-1].bit_length()
+    b = shift(Val(d, pp, neg), -expo)
+    t = b.tz()
+    b = Val(b.d[t:], b.pp - t, b.neg)
+    x = from_double(1 / to_double(b))
+    one = Val([1], 0, False)
+    cur = 52 // 28
+    while cur < precision:
+        cur *= 2
+        t1 = mul_trunc(b, x, cur + 1)
+        t2 = add_or_sub(one, t1, True)
+        t3 = mul_trunc(x, t2, cur + 1)
+        x = add_or_sub(x, t3, False)
+    return shift(x, -expo)
