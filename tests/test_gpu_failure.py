@@ -58,3 +58,47 @@ def test_concurrent_host_threads(bb, port):
     assert not errors
     for i, (g, w) in enumerate(zip(got, want)):
         assert np.array_equal(g, w), i
+
+
+def test_concurrent_mixed_entry_points(bb, port):
+    """Threads calling different entry points at once (u64 and Digits
+    products through the staged host copies, the reciprocal, decimal parse and
+    print, fast_pow) share the engine's buffers; each result must equal the
+    same call made alone."""
+    import threading
+
+    rng = np.random.default_rng(SEED + 82)
+    a, b = rand_limbs(rng, 90000), rand_limbs(rng, 70000)
+    d = rng.integers(0, 1 << 28, 150000, dtype=np.uint32)
+    d[-1] |= 1
+    text = "".join(map(str, rng.integers(0, 10, 60000)))
+    calls = [
+        lambda: bb.mul(a, b),
+        lambda: bb.mul_digits(d, d[:70000].copy()),
+        lambda: bb.reciprocal_digits(d[:30000])[0],
+        lambda: bb.from_decimal(text)[0],
+        lambda: bb.to_decimal(d[:40000]),
+        lambda: bb.fast_pow(7, 1000003),
+    ]
+    alone = [c() for c in calls]
+    got = [[None] * len(calls) for _ in range(3)]
+    errors = []
+
+    def worker(r):
+        try:
+            for i in range(len(calls)):
+                k = (i + r) % len(calls)
+                got[r][k] = calls[k]()
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(r,)) for r in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors
+    for r in range(3):
+        for k, want in enumerate(alone):
+            g = got[r][k]
+            assert (g == want) if isinstance(want, str) else np.array_equal(g, want), (r, k)
