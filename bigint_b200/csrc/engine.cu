@@ -57,6 +57,14 @@ struct Engine {
     void* d_desc = nullptr;  // small-product descriptors of the decimal levels
     size_t desc_bytes = 0;
     unsigned long long* h_small = nullptr;  // page-locked readback words of the step-by-step paths
+    // powers of ten Q_k = 10^(19 * 2^k) (limb 2^k - 1, 2^k limbs) and their
+    // reciprocals V_k = floor(2^(128 * 2^k) / Q_k), cached across decimal calls
+    uint64_t* d_pq = nullptr;
+    size_t pq_bytes = 0;
+    int pq_levels = 0;
+    uint64_t* d_pv = nullptr;
+    size_t pv_bytes = 0;
+    int pv_levels = 0;
     // stream and scratch layout of the last NTT product launched
     cudaStream_t ntt_stream = nullptr;
     int ntt_log_n = -1;
@@ -99,6 +107,8 @@ void release_locked() {
     cudaFree(g.d_dec);
     cudaFree(g.d_desc);
     if (g.h_small) cudaFreeHost(g.h_small);
+    cudaFree(g.d_pq);
+    cudaFree(g.d_pv);
     cudaFree(g.d_err);
     cudaFree(g.d_ticket);
     cudaFree(g.d_io);
@@ -1459,6 +1469,137 @@ static EngineHooks hooks_locked() {
     return h;
 }
 
+// Limbs of V_k and its offset in the reciprocal cache.
+static uint64_t pow_mk(int k) { return ((uint64_t)1 << k) + (((uint64_t)1 << k) >> 6) + 2; }
+static uint64_t pow_voff(int k) {
+    uint64_t o = 0;
+    for (int i = 0; i < k; ++i) o += pow_mk(i);
+    return o;
+}
+
+// Grows a device buffer to `need` bytes keeping its first `keep` bytes.
+static int grow_keep(uint64_t** p, size_t* bytes, size_t need, size_t keep, cudaStream_t st) {
+    if (*bytes >= need) return BGPU_OK;
+    void* np = nullptr;
+    if (cudaMalloc(&np, need) != cudaSuccess) {
+        cudaGetLastError();
+        return BGPU_ERR_OOM;
+    }
+    cudaError_t e = cudaSuccess;
+    if (*p && keep) e = cudaMemcpyAsync(np, *p, keep, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaFree(np);
+        return cuda_status(e);
+    }
+    cudaFree(*p);
+    *p = static_cast<uint64_t*>(np);
+    *bytes = need;
+    return BGPU_OK;
+}
+
+// Q_0 .. Q_(J-1) (and with_v: V_0 .. V_(J-1)) in the engine's cache, computed
+// on the device the first time a size needs them; later calls of the same or
+// smaller size reuse them, as the reference keeps its powers of ten
+// (get_pow_of_ten, src/bigint.cpp:154-173).  The reciprocals are a chain:
+// V_k^2 <= V_(k+1) (both floors of the same real, squared), one Newton step
+// from below brings it within a few units, and single correction steps
+// (r >= Q: r -= Q, V += 1) make it exact.
+static int ensure_powers(int J, bool with_v, cudaStream_t st, uint32_t* nl) {
+    if (J <= 0) return BGPU_OK;
+    if (g.pq_levels < J) {
+        const int have = g.pq_levels;
+        int rc = grow_keep(&g.d_pq, &g.pq_bytes, ((size_t)1 << J) * 8,
+                           have ? (((size_t)1 << have) - 1) * 8 : 0, st);
+        if (rc != BGPU_OK) return rc;
+        if (have == 0) {
+            const uint64_t ten19 = 10000000000000000000ull;
+            cudaError_t e = cudaMemcpyAsync(g.d_pq, &ten19, 8, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        for (int k = std::max(have, 1) - 1; k + 1 < J; ++k) {  // Q_(k+1) = Q_k^2
+            const uint64_t w = (uint64_t)1 << k;
+            rc = device_product(g.d_pq + (w - 1), w, g.d_pq + (w - 1), w, g.d_pq + (2 * w - 1), st, nl);
+            if (rc != BGPU_OK) return rc;
+        }
+        g.pq_levels = J;
+    }
+    if (!with_v || g.pv_levels >= J) return BGPU_OK;
+    const int have = g.pv_levels;
+    int rc = grow_keep(&g.d_pv, &g.pv_bytes, pow_voff(J) * 8 + 64, pow_voff(have) * 8, st);
+    if (rc != BGPU_OK) return rc;
+    if (have == 0) {  // V_0 = floor(2^128 / 10^19)
+        const unsigned __int128 v0 = ~(unsigned __int128)0 / 10000000000000000000ull;
+        std::vector<uint64_t> hv(pow_mk(0), 0);
+        hv[0] = (uint64_t)v0;
+        hv[1] = (uint64_t)(v0 >> 64);
+        cudaError_t e = cudaMemcpyAsync(g.d_pv, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_status(e);
+        g.pv_levels = 1;
+        if (J == 1) return BGPU_OK;
+    }
+    // scratch of the largest step (K = 2^(J-1)): X, P, R, D, the constant 1, a
+    // flag and the carry-scan words
+    const uint64_t Kmax = (uint64_t)1 << (J - 1);
+    const uint64_t mmax = pow_mk(J - 2 < 0 ? 0 : J - 2);
+    const uint64_t nacc = accumulate_blocks(2 * Kmax + 2);
+    const uint64_t scratch = 6 * mmax + Kmax + 4 * Kmax + 64 + 8 + nacc + 64;
+    uint64_t* xs = nullptr;
+    if (cudaMalloc(reinterpret_cast<void**>(&xs), scratch * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return BGPU_ERR_OOM;
+    }
+    uint64_t* one = xs + scratch - nacc - 16;
+    uint32_t* flag = reinterpret_cast<uint32_t*>(one + 1);
+    uint32_t* agg = reinterpret_cast<uint32_t*>(one + 8);
+    uint32_t* cin = agg + nacc;
+    const uint64_t c1 = 1;
+    cudaError_t e = cudaMemcpyAsync(one, &c1, 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    rc = cuda_status(e);
+    for (int k = g.pv_levels - 1; rc == BGPU_OK && k + 1 < J; ++k) {
+        const uint64_t K = (uint64_t)1 << (k + 1), el = 2 * K, m = pow_mk(k), m1 = pow_mk(k + 1);
+        const uint64_t* q = g.d_pq + (K - 1);
+        const uint64_t* v = g.d_pv + pow_voff(k);
+        uint64_t* v1 = g.d_pv + pow_voff(k + 1);
+        uint64_t* X = xs;                 // 2m
+        uint64_t* P = X + 2 * m + 8;      // K + 2m
+        uint64_t* R = P + K + 2 * m + 8;  // el + 1
+        uint64_t* Dd = R + el + 8;        // 2m + el + 1
+        rc = device_product(v, m, v, m, X, st, nl);  // X = V_k^2 <= V_(k+1)
+        if (rc == BGPU_OK) rc = device_product(q, K, X, 2 * m, P, st, nl);  // P = Q X < 2^(64 el)
+        if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
+        if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
+        if (rc == BGPU_OK) rc = device_product(X, 2 * m, R, el + 1, Dd, st, nl);  // X (2^E - Q X)
+        // V' = X + floor(X R / 2^E): Newton from below, within a few units of V_(k+1)
+        if (rc == BGPU_OK) rc = cuda_status(cudaMemsetAsync(v1, 0, m1 * 8, st));
+        if (rc == BGPU_OK)
+            rc = cuda_status(cudaMemcpyAsync(v1, X, std::min(2 * m, m1) * 8, cudaMemcpyDeviceToDevice, st));
+        if (rc == BGPU_OK)
+            rc = cuda_status(launch_accumulate(v1, m1, Dd + el, std::min<uint64_t>(2 * m + 1, m1), agg, cin, st));
+        // exact: R = 2^E - Q V' (>= 0); while R >= Q: R -= Q, V' += 1
+        if (rc == BGPU_OK) rc = device_product(q, K, v1, m1, P, st, nl);
+        if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
+        if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
+        for (int it = 0; rc == BGPU_OK; ++it) {
+            if (it == 64) {  // the Newton step is within a few units
+                rc = BGPU_ERR_CUDA;
+                break;
+            }
+            uint32_t f = 0;
+            rc = cuda_status(launch_fix_step(R, (uint32_t)(el + 1), q, (uint32_t)K, v1, (uint32_t)m1, flag, st));
+            if (rc == BGPU_OK) rc = read_back(flag, &f, 1);
+            if (!f) break;
+        }
+        if (rc == BGPU_OK) g.pv_levels = k + 2;
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(xs);
+    return rc;
+}
+
 // A batch of equal-size device products on `st` (the levels of the decimal
 // conversions): schoolbook or Karatsuba classes as one launch over a
 // descriptor array, up to 128 transform-size products as direct launches,
@@ -1537,29 +1678,22 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
     int j0 = 0;
     while ((1u << j0) < w0) ++j0;
     const uint64_t nd = (64 * NL + 27) / 28;  // Digits of the result, before stripping
-    const size_t dig_off = 0, lvl_off = align256(D), q_off = lvl_off + 2 * align256(NL * 8);
-    const size_t o_off = q_off + align256(NL * 8);
+    const size_t dig_off = 0, lvl_off = align256(D), o_off = lvl_off + 2 * align256(NL * 8);
     int rc = ensure(&g.d_dec, &g.dec_bytes, o_off + align256(nd * 4));
     if (rc != BGPU_OK) return rc;
     char* base = static_cast<char*>(g.d_dec);
     uint8_t* ddig = reinterpret_cast<uint8_t*>(base + dig_off);
     uint64_t* lvl[2] = {reinterpret_cast<uint64_t*>(base + lvl_off),
                         reinterpret_cast<uint64_t*>(base + lvl_off + align256(NL * 8))};
-    uint64_t* q = reinterpret_cast<uint64_t*>(base + q_off);  // 10^(19 * 2^j) at limb 2^j - 1, 2^j limbs
     uint32_t* dout = reinterpret_cast<uint32_t*>(base + o_off);
     cudaStream_t st = g.stream;
     rc = host_to_device(ddig, dig.data(), D, st, nullptr);
     if (rc != BGPU_OK) return rc;
-    const uint64_t ten19 = 10000000000000000000ull;
-    cudaError_t e = cudaMemcpyAsync(q, &ten19, 8, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_status(e);
     uint32_t nl = 0;
-    for (int j = 0; j + 1 < J; ++j) {  // 10^(19 * 2^(j+1)) = (10^(19 * 2^j))^2, on the device
-        const uint64_t w = (uint64_t)1 << j;
-        rc = device_product(q + (w - 1), w, q + (w - 1), w, q + (2 * w - 1), st, &nl);
-        if (rc != BGPU_OK) return rc;
-    }
-    e = launch_dec_leaves(ddig, D, w0, NL / w0, lvl[0], st);
+    rc = ensure_powers(J, false, st, &nl);  // 10^(19 * 2^j) at limb 2^j - 1, 2^j limbs
+    if (rc != BGPU_OK) return rc;
+    const uint64_t* q = g.d_pq;
+    cudaError_t e = launch_dec_leaves(ddig, D, w0, NL / w0, lvl[0], st);
     if (e != cudaSuccess) return cuda_status(e);
     int cur = 0;
     std::vector<bgpu_product> prods;
@@ -1618,7 +1752,7 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
     const uint32_t w0 = (uint32_t)std::min<uint64_t>(128, NL);
     int jleaf = 0;
     while ((1u << jleaf) < w0) ++jleaf;
-    auto mk = [](int k) { return ((uint64_t)1 << k) + (((uint64_t)1 << k) >> 6) + 2; };  // limbs of V_k
+    auto mk = pow_mk;
     // arena (limbs)
     uint64_t off = 0;
     auto take = [&](uint64_t limbs) {
@@ -1626,94 +1760,35 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
         off += (limbs + 31) & ~(uint64_t)31;
         return o;
     };
-    const uint64_t o_lvl0 = take(NL), o_lvl1 = take(NL), o_q = take(NL), o_v = take(NL + NL / 32 + 4 * J + 8);
-    const uint64_t o_t = take(2 * NL + 4 * J + 64), o_u = take(NL), o_x = take(7 * NL + 64), o_one = take(4);
+    const uint64_t o_lvl0 = take(NL), o_lvl1 = take(NL), o_t = take(2 * NL + 4 * J + 64), o_u = take(NL);
     const uint64_t o_dig = take((n + 1) / 2 + 1), o_chr = take((19 * NL + 7) / 8 + 1);
     int rc = ensure(&g.d_dec, &g.dec_bytes, off * 8);
     if (rc != BGPU_OK) return rc;
     uint64_t* A = static_cast<uint64_t*>(g.d_dec);
     uint64_t* lvl[2] = {A + o_lvl0, A + o_lvl1};
-    uint64_t* qp = A + o_q;
-    uint64_t* vp = A + o_v;
     uint64_t* tb = A + o_t;
     uint64_t* ub = A + o_u;
-    uint64_t* xs = A + o_x;
-    uint64_t* one = A + o_one;
-    uint32_t* flag = reinterpret_cast<uint32_t*>(A + o_one + 1);
     uint32_t* ddig = reinterpret_cast<uint32_t*>(A + o_dig);
     char* chars = reinterpret_cast<char*>(A + o_chr);
-    // carry-scan scratch of the chain's additions, in the (not yet used) U buffer
-    uint32_t* agg = reinterpret_cast<uint32_t*>(A + o_u);
-    uint32_t* cin = agg + ((accumulate_blocks(NL + 2) + 63) & ~63u);
-    std::vector<uint64_t> voff(J + 1, 0);
-    for (int k = 1; k <= J; ++k) voff[k] = voff[k - 1] + mk(k - 1);
     cudaStream_t st = g.stream;
 
-    // the value, as NL limbs
+    // the value, as NL limbs; the powers of ten and their reciprocals
     rc = host_to_device(ddig, digits, n * 4, st, nullptr);
     if (rc != BGPU_OK) return rc;
     cudaError_t e = launch_digits28_to_limbs(ddig, (uint32_t)n, lvl[0], (uint32_t)NL, st);
-    const uint64_t consts[2] = {10000000000000000000ull, 1};
-    if (e == cudaSuccess) e = cudaMemcpyAsync(qp, &consts[0], 8, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(one, &consts[1], 8, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_status(e);
     uint32_t nl = 0;
-    for (int k = 0; k + 1 < J; ++k) {  // Q_(k+1) = Q_k^2
-        const uint64_t w = (uint64_t)1 << k;
-        rc = device_product(qp + (w - 1), w, qp + (w - 1), w, qp + (2 * w - 1), st, &nl);
-        if (rc != BGPU_OK) return rc;
-    }
-    if (J > jleaf) {
-        // V_0 = floor(2^128 / 10^19), then the chain up to V_(J-1)
-        const unsigned __int128 v0 = ~(unsigned __int128)0 / 10000000000000000000ull;
-        std::vector<uint64_t> hv(mk(0), 0);
-        hv[0] = (uint64_t)v0;
-        hv[1] = (uint64_t)(v0 >> 64);
-        e = cudaMemcpyAsync(vp, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_status(e);
-        for (int k = 0; k + 1 < J; ++k) {
-            const uint64_t K = (uint64_t)1 << (k + 1), el = 2 * K, m = mk(k), m1 = mk(k + 1);
-            const uint64_t* q = qp + (K - 1);
-            uint64_t* v = vp + voff[k];
-            uint64_t* v1 = vp + voff[k + 1];
-            uint64_t* X = xs;                    // 2m
-            uint64_t* P = X + 2 * m + 8;         // K + 2m
-            uint64_t* R = P + K + 2 * m + 8;     // el + 1
-            uint64_t* Dd = R + el + 8;           // 2m + el + 1
-            rc = device_product(v, m, v, m, X, st, &nl);  // X = V_k^2 <= V_(k+1)
-            if (rc == BGPU_OK) rc = device_product(q, K, X, 2 * m, P, st, &nl);  // P = Q X < 2^(64 el)
-            if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
-            if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
-            if (rc == BGPU_OK) rc = device_product(X, 2 * m, R, el + 1, Dd, st, &nl);  // X (2^E - Q X)
-            // V' = X + floor(X R / 2^E): Newton from below, within a few units of V_(k+1)
-            if (rc == BGPU_OK) rc = cuda_status(cudaMemsetAsync(v1, 0, m1 * 8, st));
-            if (rc == BGPU_OK)
-                rc = cuda_status(cudaMemcpyAsync(v1, X, std::min(2 * m, m1) * 8, cudaMemcpyDeviceToDevice, st));
-            if (rc == BGPU_OK)
-                rc = cuda_status(launch_accumulate(v1, m1, Dd + el, std::min<uint64_t>(2 * m + 1, m1),
-                                                   agg, cin, st));
-            // exact: R = 2^E - Q V' (>= 0); while R >= Q: R -= Q, V' += 1
-            if (rc == BGPU_OK) rc = device_product(q, K, v1, m1, P, st, &nl);
-            if (rc == BGPU_OK) rc = cuda_status(launch_not_limbs(P, (uint32_t)el, R, st));
-            if (rc == BGPU_OK) rc = cuda_status(launch_accumulate(R, el + 1, one, 1, agg, cin, st));
-            for (int it = 0; rc == BGPU_OK; ++it) {
-                if (it == 64) return BGPU_ERR_CUDA;  // the Newton step is within a few units
-                uint32_t f = 0;
-                rc = cuda_status(launch_fix_step(R, (uint32_t)(el + 1), q, (uint32_t)K, v1, (uint32_t)m1, flag, st));
-                if (rc == BGPU_OK) rc = read_back(flag, &f, 1);
-                if (!f) break;
-            }
-            if (rc != BGPU_OK) return rc;
-        }
-    }
+    rc = ensure_powers(J, J > jleaf, st, &nl);
+    if (rc != BGPU_OK) return rc;
+    const uint64_t* qp = g.d_pq;
+    const uint64_t* vp = g.d_pv;
     // top-down division levels
     int cur = 0;
     std::vector<bgpu_product> prods;
     for (int j = J; j > jleaf; --j) {
         const uint64_t w = (uint64_t)1 << (j - 1), count = NL >> j, m = mk(j - 1), ts = 2 * w + m;
         const uint64_t* q = qp + (w - 1);
-        const uint64_t* v = vp + voff[j - 1];
+        const uint64_t* v = vp + pow_voff(j - 1);
         for (int pass = 0; pass < 2; ++pass) {
             prods.resize(count);
             for (uint64_t p = 0; p < count; ++p)
