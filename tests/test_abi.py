@@ -37,7 +37,8 @@ def lib():
 def test_header_declares_entry_points():
     names = declared_functions()
     for must in ("bgpu_init", "bgpu_shutdown", "bgpu_strerror", "bgpu_mul_u64", "bgpu_mul_digits",
-                 "bgpu_mul_u64_device", "bgpu_device_status"):
+                 "bgpu_mul_u64_device", "bgpu_device_status", "bgpu_mul_u64_many", "bgpu_pow_u64",
+                 "bgpu_reciprocal_digits", "bgpu_from_decimal", "bgpu_to_decimal"):
         assert must in names
 
 
@@ -82,3 +83,26 @@ def test_calls_before_init_report_not_initialized(lib):
     pa = a.ctypes.data_as(u64p)
     assert lib.bgpu_mul_u64(pa, 4, pa, 4, out.ctypes.data_as(u64p), 8, C.byref(n), 0, None) == -8
     assert lib.bgpu_device_status(None) == -8
+    u32p = C.POINTER(C.c_uint32)
+    d = np.ones(4, dtype=np.uint32)
+    pd = d.ctypes.data_as(u32p)
+    pp, neg = C.c_int64(0), C.c_int(0)
+    assert lib.bgpu_reciprocal_digits(pd, 4, 0, 0, 0, pd, 4, C.byref(n), C.byref(pp), C.byref(neg)) == -8
+    assert lib.bgpu_from_decimal(b"12", 2, pd, 4, C.byref(n), C.byref(neg)) == -8
+    buf = C.create_string_buffer(16)
+    assert lib.bgpu_to_decimal(pd, 4, 0, buf, 16, C.byref(n)) == -8
+
+
+def test_new_entry_points_reject_bad_arguments_on_host(lib):
+    u32p = C.POINTER(C.c_uint32)
+    d = np.ones(4, dtype=np.uint32)
+    pd = d.ctypes.data_as(u32p)
+    n, pp, neg = C.c_size_t(0), C.c_int64(0), C.c_int(0)
+    buf = C.create_string_buffer(16)
+    assert lib.bgpu_reciprocal_digits(None, 4, 0, 0, 0, pd, 4, C.byref(n), C.byref(pp), C.byref(neg)) == -1
+    assert lib.bgpu_reciprocal_digits(pd, 0, 0, 0, 0, pd, 4, C.byref(n), C.byref(pp), C.byref(neg)) == -1
+    assert lib.bgpu_reciprocal_digits(pd, 4, 0, 0, 0, pd, 4, None, C.byref(pp), C.byref(neg)) == -1
+    assert lib.bgpu_from_decimal(b"12", 2, pd, 4, None, C.byref(neg)) == -1
+    assert lib.bgpu_to_decimal(None, 4, 0, buf, 16, C.byref(n)) == -1
+    assert lib.bgpu_to_decimal(pd, 0, 0, buf, 16, C.byref(n)) == -1
+    assert lib.bgpu_to_decimal(pd, 4, 0, buf, 16, None) == -1
