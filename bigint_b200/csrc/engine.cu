@@ -1679,7 +1679,9 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
     while ((1u << j0) < w0) ++j0;
     const uint64_t nd = (64 * NL + 27) / 28;  // Digits of the result, before stripping
     const size_t dig_off = 0, lvl_off = align256(D), o_off = lvl_off + 2 * align256(NL * 8);
-    int rc = ensure(&g.d_dec, &g.dec_bytes, o_off + align256(nd * 4));
+    const size_t acc_off = o_off + align256(nd * 4);
+    const size_t acc_words = accumulate_blocks(NL) + 64;
+    int rc = ensure(&g.d_dec, &g.dec_bytes, acc_off + 2 * acc_words * 4);
     if (rc != BGPU_OK) return rc;
     char* base = static_cast<char*>(g.d_dec);
     uint8_t* ddig = reinterpret_cast<uint8_t*>(base + dig_off);
@@ -1693,18 +1695,31 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
     rc = ensure_powers(J, false, st, &nl);  // 10^(19 * 2^j) at limb 2^j - 1, 2^j limbs
     if (rc != BGPU_OK) return rc;
     const uint64_t* q = g.d_pq;
-    cudaError_t e = launch_dec_leaves(ddig, D, w0, NL / w0, lvl[0], st);
+    uint32_t* agg = reinterpret_cast<uint32_t*>(base + acc_off);
+    uint32_t* cin = agg + acc_words;
+    // Only segments holding digits are built: the levels are 2^J limbs wide but
+    // the number may fill little more than half of them.  Everything above is
+    // zero from the start, and what a level leaves of the level two below
+    // lies inside the region it overwrites (its segments are coarser).
+    cudaError_t e = cudaMemsetAsync(lvl[0], 0, NL * 8, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(lvl[1], 0, NL * 8, st);
+    if (e == cudaSuccess) e = launch_dec_leaves(ddig, D, w0, (leaves + w0 - 1) / w0, lvl[0], st);
     if (e != cudaSuccess) return cuda_status(e);
     int cur = 0;
     std::vector<bgpu_product> prods;
     for (int j = j0; j < J; ++j) {
-        const uint64_t w1 = (uint64_t)1 << j, pairs = NL / (2 * w1);
+        const uint64_t w1 = (uint64_t)1 << j, pairs = (leaves + 2 * w1 - 1) / (2 * w1);
         prods.resize(pairs);
         for (uint64_t p = 0; p < pairs; ++p)
             prods[p] = bgpu_product{lvl[cur] + (2 * p + 1) * w1, w1, q + (w1 - 1), w1, lvl[cur ^ 1] + p * 2 * w1};
         rc = run_products(prods.data(), pairs, st, &nl);
         if (rc != BGPU_OK) return rc;
-        e = launch_seg_add_low(lvl[cur ^ 1], lvl[cur], (uint32_t)w1, pairs, st);
+        if (pairs <= 8 && w1 >= 4096) {  // few long segments: one multi-block carry scan each
+            for (uint64_t p = 0; p < pairs && e == cudaSuccess; ++p)
+                e = launch_accumulate(lvl[cur ^ 1] + p * 2 * w1, 2 * w1, lvl[cur] + 2 * p * w1, w1, agg, cin, st);
+        } else {
+            e = launch_seg_add_low(lvl[cur ^ 1], lvl[cur], (uint32_t)w1, pairs, st);
+        }
         if (e != cudaSuccess) return cuda_status(e);
         cur ^= 1;
     }
@@ -1786,7 +1801,10 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
     int cur = 0;
     std::vector<bgpu_product> prods;
     for (int j = J; j > jleaf; --j) {
-        const uint64_t w = (uint64_t)1 << (j - 1), count = NL >> j, m = mk(j - 1), ts = 2 * w + m;
+        // segments above the value's last decimal digit are zero: their halves
+        // are never read (the level below reads only its own, finer, active part)
+        const uint64_t w = (uint64_t)1 << (j - 1), m = mk(j - 1), ts = 2 * w + m;
+        const uint64_t count = std::min<uint64_t>(NL >> j, (dmax + 19 * 2 * w - 1) / (19 * 2 * w));
         const uint64_t* q = qp + (w - 1);
         const uint64_t* v = vp + pow_voff(j - 1);
         for (int pass = 0; pass < 2; ++pass) {
@@ -1802,9 +1820,10 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
         if (e != cudaSuccess) return cuda_status(e);
         cur ^= 1;
     }
-    e = launch_dec_print_leaves(lvl[cur], w0, NL / w0, chars, st);
+    const uint64_t nleaf = std::min<uint64_t>(NL / w0, (dmax + 19 * w0 - 1) / (19 * w0));
+    e = launch_dec_print_leaves(lvl[cur], w0, nleaf, chars, st);
     if (e != cudaSuccess) return cuda_status(e);
-    std::vector<char> h(19 * NL);
+    std::vector<char> h(19 * w0 * nleaf);
     rc = device_to_host(h.data(), chars, h.size(), st);
     rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
