@@ -79,3 +79,36 @@ def test_fft_square_and_unbalanced(bb, port):
     assert np.array_equal(bb.fft_mul(a), port.ntt_mul(a))
     b = rand_limbs(rng, 300)
     assert np.array_equal(bb.fft_mul(a, b), port.mul(a, b))
+
+
+def test_reference_regression_sizes(bb, port):
+    """The reference's own FFT regression (tests/measure_digit_bits.cpp:135-168):
+    uniform 28-bit digits at {200, 500, 1000, 3000, 8000, 20000, 25000}
+    digits, four repetitions each, automatic bits per point, against the
+    integer product."""
+    from oracle.pyoracle import digits28_to_limbs
+
+    rng = np.random.default_rng(SEED)
+    for nd in (200, 500, 1000, 3000, 8000, 20000, 25000):
+        for _ in range(4):
+            a = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
+            b = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
+            a[-1] |= 1
+            b[-1] |= 1
+            la, lb = digits28_to_limbs(a), digits28_to_limbs(b)
+            got, st = bb.fft_mul(la, lb, stats=True)
+            assert np.array_equal(got, port.mul(la, lb)), nd
+            assert st.method == bb.BGPU_METHOD_FFT and st.max_round_err < 0.25, (nd, st)
+
+
+def test_smallest_transforms(bb):
+    """Products of one to a few limbs through the FFT form: the shortest
+    transforms (the reference's radix-4 FFT mishandles length 4,
+    src/mul/fft.cpp:135; nothing here may)."""
+    rng = np.random.default_rng(SEED + 23)
+    for na, nb in [(1, 1), (1, 2), (2, 2), (3, 1), (4, 4), (5, 3)]:
+        for fill in ("rand", "ones"):
+            a = np.full(na, ONES) if fill == "ones" else rand_limbs(rng, na)
+            b = np.full(nb, ONES) if fill == "ones" else rand_limbs(rng, nb)
+            got = bb.fft_mul(a, b)
+            assert limbs_to_int(got) == limbs_to_int(a) * limbs_to_int(b), (na, nb, fill)
