@@ -182,6 +182,17 @@ def test_independent_products_back_to_back(bb, port):
     assert port.mod_m61(p) ** 2 % M61 == port.mod_m61(chained.cpu().numpy().view(np.uint64))
 
 
+def test_reference_mul_digits_regression(bb, port):
+    """The reference's mul_digits regression (tests/measure_digit_bits.cpp:170-184):
+    the full dispatch chain at {100, 1000, 10000, 40000} uniform 28-bit
+    digits, three repetitions each, seeded like the reference."""
+    rng = np.random.default_rng(SEED)
+    for nd in (100, 1000, 10000, 40000):
+        for _ in range(3):
+            a, b = rand_digits(rng, nd), rand_digits(rng, nd)
+            assert np.array_equal(bb.mul_digits(a, b), port.mul_digits(a, b)), nd
+
+
 def test_headline_size_vs_port(bb, port):
     """2^24 x 2^24-bit product (the bench workload) limb-exact."""
     rng = np.random.default_rng(SEED + 15)
