@@ -584,6 +584,49 @@ def reciprocal_form(bb, cpu: bool = True, reps: int = 5):
     return res
 
 
+def divmod_form(bb, port, cpu: bool = True, reps: int = 5):
+    """BigInt::divmod (src/bigint.cpp:625-673) of a 2^24-bit integer by a
+    2^23-bit one, truncating, through bgpu_divmod_digits: the reciprocal at
+    n_a + 16 digits, the estimate, Q * b and the check all on the device, wall
+    clock from host Digits to host Digits; the reference's own divmod on the
+    host cores beside it (one run), quotient and remainder compared."""
+    rng = np.random.default_rng(SEED + 10)
+    la = rng.integers(0, 2**64, (1 << 24) // 64, dtype=np.uint64)
+    lb = rng.integers(0, 2**64, (1 << 23) // 64, dtype=np.uint64)
+    la[-1] |= np.uint64(1 << 63)
+    lb[-1] |= np.uint64(1 << 63)
+    a, b = limbs_to_digits28_np(la), limbs_to_digits28_np(lb)
+    bb.divmod_digits(a, b)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        (q, qn), (r, rn) = bb.divmod_digits(a, b)
+        times.append(time.perf_counter() - t0)
+    res = {"a_bits": 1 << 24, "b_bits": 1 << 23, "mode": "Truncate", "quotient_digits": int(q.size),
+           "s": statistics.median(times), "api": "bgpu_divmod_digits (host Digits in and out)"}
+    from oracle.pyoracle import Reference, have_reference
+
+    if cpu and have_reference() and Reference().has_divmod:
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        t0 = time.perf_counter()
+        (wq, wqn), (wr, wrn) = ref.divmod(la, False, lb, False, 0, True)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                "call": "BigInt::divmod"}
+        if not (np.array_equal(q, wq) and qn == wqn and np.array_equal(r, wr) and rn == wrn):
+            raise SystemExit("bench divmod: result differs from the reference's")
+        res["verified"] = "identical to the reference's quotient and remainder"
+    else:
+        m61 = (1 << 61) - 1
+        lq, lr = digits28_to_limbs_np(q), digits28_to_limbs_np(r)
+        if (port.mod_m61(lq) * port.mod_m61(lb) + port.mod_m61(lr)) % m61 != port.mod_m61(la) or qn or rn:
+            raise SystemExit("bench divmod: A != Q * B + R")
+        if r.size > b.size or (r.size == b.size and r[::-1].tolist() >= b[::-1].tolist()):
+            raise SystemExit("bench divmod: remainder not below the divisor")
+        res["verified"] = "A = Q * B + R mod 2^61 - 1 and 0 <= R < B"
+    return res
+
+
 def decimal_print_form(bb, cpu: bool = True):
     """Decimal text of a 2^22-bit integer (1.26 M digits): bgpu_to_decimal
     (the whole conversion on the GPU, host Digits in, host text out); the
@@ -1033,6 +1076,7 @@ def run_gpu_arm(args) -> None:
                  "fast_pow": fast_pow_form(bb, port, cpu=not args.no_cpu_baseline),
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
+                 "divmod_2p24": divmod_form(bb, port, cpu=not args.no_cpu_baseline),
                  "decimal_print_2p22": decimal_print_form(bb, cpu=not args.no_cpu_baseline),
                  "decimal_parse_5m": decimal_parse_form(bb, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
@@ -1084,7 +1128,7 @@ def run_gpu_arm(args) -> None:
 
 
 FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
-         "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
+         "divmod_2p24", "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
          "product_tree_2p20")
 
 
@@ -1116,6 +1160,8 @@ def run_single_form(args) -> None:
         res = mul_digits_form(bb, port, cpu=not args.no_cpu_baseline)
     elif name == "reciprocal_2p24":
         res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
+    elif name == "divmod_2p24":
+        res = divmod_form(bb, port, cpu=not args.no_cpu_baseline)
     elif name == "decimal_print_2p22":
         res = decimal_print_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_parse_5m":

@@ -15,6 +15,7 @@ this package           reference                                       C-ABI
 ``  precision, pos)``
 ``fast_pow(base, e)``  ``fast_pow<BigInt>`` (bigint_base.h:60-69)      ``bgpu_pow_u64``
 ``reciprocal_digits``  ``BigFloat::reciprocal`` (bigint.cpp:1044-1071) ``bgpu_reciprocal_digits``
+``divmod_digits``      ``BigInt::divmod`` (bigint.cpp:625-673)          ``bgpu_divmod_digits``
 ``from_decimal(text)`` ``BigInt(const std::string&)`` (bigint.cpp:25-124) ``bgpu_from_decimal``
 ``to_decimal(d, neg)`` ``BigInt::print`` (bigint.cpp:175-247)          ``bgpu_to_decimal``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
@@ -42,11 +43,16 @@ from ._lib import (  # noqa: F401
     BGPU_TUNE_FFT_MIN_LIMBS,
     BGPU_TUNE_KARATSUBA_MAX_LIMBS,
     BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS,
+    ROUND_CEIL,
+    ROUND_FLOOR,
+    ROUND_HALF_UP,
+    ROUND_TRUNCATE,
     BatchPlan,
     BigIntGPUError,
     Stats,
     brute_mul,
     device_status,
+    divmod_digits,
     fft_mul,
     from_decimal,
     get_batch_split,

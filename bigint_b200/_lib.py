@@ -110,6 +110,10 @@ def _load() -> C.CDLL:
     L.bgpu_reciprocal_digits.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, u32p,
                                          C.c_size_t, szp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.bgpu_reciprocal_digits.restype = C.c_int
+    L.bgpu_divmod_digits.argtypes = [u32p, C.c_size_t, C.c_int, u32p, C.c_size_t, C.c_int, C.c_uint32, C.c_int,
+                                     u32p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int), u32p,
+                                     C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+    L.bgpu_divmod_digits.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_uint32, C.c_void_p]
     L.bgpu_mul_u64_device.restype = C.c_int
@@ -441,6 +445,38 @@ def reciprocal_digits(digits, point_pos: int = 0, neg: bool = False, precision: 
         cap = n.value
     _check(rc, "bgpu_reciprocal_digits")
     return out[: n.value], int(pp.value), bool(ng.value)
+
+
+ROUND_TRUNCATE, ROUND_FLOOR, ROUND_CEIL, ROUND_HALF_UP = 0, 1, 2, 3  # the reference's RoundMode
+
+
+def divmod_digits(a, b, a_neg: bool = False, b_neg: bool = False, mode: int = ROUND_TRUNCATE,
+                  check: bool = True):
+    """``BigInt::divmod(b, mode, check)`` (src/bigint.cpp:625-673) on the GPU.
+
+    ``a`` and ``b`` are 28-bit Digits without leading zeros (zero is ``[0]``)
+    with separate signs.  Returns ``((q_digits, q_neg), (r_digits, r_neg))``,
+    identical to the reference's quotient and remainder; the reciprocal, the
+    estimate, Q * b and the adjustment all run on the device
+    (``bgpu_divmod_digits``)."""
+    _ensure_init()
+    da, db = _as_digits(a), _as_digits(b)
+    if da.size == 0 or db.size == 0:
+        raise BigIntGPUError(-1, "bgpu_divmod_digits (empty input)")
+    u32p = C.POINTER(C.c_uint32)
+    qcap, rcap = max(da.size - db.size + 2, 1), max(db.size, 1) + 1
+    for _ in range(2):
+        q, r = np.empty(qcap, dtype=np.uint32), np.empty(rcap, dtype=np.uint32)
+        nq, nr, qn, rn = C.c_size_t(0), C.c_size_t(0), C.c_int(0), C.c_int(0)
+        rc = lib.bgpu_divmod_digits(da.ctypes.data_as(u32p), da.size, int(bool(a_neg)), db.ctypes.data_as(u32p),
+                                    db.size, int(bool(b_neg)), int(mode), int(bool(check)),
+                                    q.ctypes.data_as(u32p), qcap, C.byref(nq), C.byref(qn),
+                                    r.ctypes.data_as(u32p), rcap, C.byref(nr), C.byref(rn))
+        if rc != -5:
+            break
+        qcap, rcap = max(qcap, nq.value), max(rcap, nr.value)
+    _check(rc, "bgpu_divmod_digits")
+    return (q[: nq.value], bool(qn.value)), (r[: nr.value], bool(rn.value))
 
 
 def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, stream: int = 0,

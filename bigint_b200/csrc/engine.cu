@@ -6,6 +6,7 @@
 //                                                       src/mul/ntt_multithread.cpp:444-530)
 //   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
 //   bgpu_reciprocal_digits <- BigFloat::reciprocal      (src/bigint.cpp:1044-1071)
+//   bgpu_divmod_digits     <- BigInt::divmod            (src/bigint.cpp:625-673)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,8 +47,8 @@ struct Engine {
     size_t io_bytes = 0;
     TreeArena tree;  // product-tree values, descriptors and scratch
     // digit buffers of the device-resident reciprocal (one per live value)
-    uint32_t* rs[11] = {};
-    size_t rs_bytes[11] = {};
+    uint32_t* rs[19] = {};
+    size_t rs_bytes[19] = {};
     // block products of the decomposition beyond the largest transform
     void* d_huge = nullptr;
     size_t huge_bytes = 0;
@@ -872,7 +873,11 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
 // shifts.  Only the starting value 1 / b.to_double() (two or three digits)
 // is formed on the host, from b's top three digits, as the reference does.
 
-enum RecipSlot { kRsIn, kRsB, kRsX0, kRsX1, kRsT1, kRsT2, kRsT3, kRsOut, kRsScratch, kRsSmall, kRsOne };
+enum RecipSlot {
+    kRsIn, kRsB, kRsX0, kRsX1, kRsT1, kRsT2, kRsT3, kRsOut, kRsScratch, kRsSmall, kRsOne,
+    // divmod: the operands, the quotient estimate, Q, Q * b, R and the adjusted Q and R
+    kRsDivA, kRsDivB, kRsDivP, kRsDivQ, kRsDivQB, kRsDivR, kRsDivQ2, kRsDivR2, kRsSlots
+};
 
 constexpr uint32_t kDigitMask = (1u << 28) - 1u;
 
@@ -886,6 +891,8 @@ struct DVal {
     int slot = -1;                // buffer holding the digits (-1: none)
     bool zero() const { return n == 1 && top == 0; }
 };
+
+static_assert(kRsSlots == sizeof(Engine::rs) / sizeof(Engine::rs[0]), "one buffer per slot");
 
 uint32_t* rslot(int k, size_t words, int* rc) {
     *rc = ensure(reinterpret_cast<void**>(&g.rs[k]), &g.rs_bytes[k], std::max<size_t>(words, 4) * 4);
@@ -1218,6 +1225,7 @@ int upload_digits(int slot, const std::vector<uint32_t>& v, int64_t pp, bool neg
 
 int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool neg, size_t precision,
                      uint32_t* out, size_t out_cap, size_t* out_len, int64_t* out_pp, int* out_neg);
+int reciprocal_val(const DVal& in, size_t precision, DVal* res);
 
 // A failed step-by-step call reports a device-side error (sticky, e.g. a
 // carry-scan timeout in one of its products) in preference to what the
@@ -1242,7 +1250,6 @@ int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool n
         if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
     if (digits[n - 1] == 0) return BGPU_ERR_INVALID_ARG;  // a leading zero digit, or the value zero
     if (precision == 0) precision = n;
-    const int64_t exponent = 28 * ((int64_t)n - 1 - point_pos) + (32 - __builtin_clz(digits[n - 1]));
     int rc;
     uint32_t* din = rslot(kRsIn, n, &rc);
     if (rc != BGPU_OK) return rc;
@@ -1251,6 +1258,22 @@ int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool n
     size_t tz = 0;
     while (digits[tz] == 0) ++tz;
     const DVal in{din, n, point_pos, neg, tz, digits[n - 1], kRsIn};
+    DVal r;
+    rc = reciprocal_val(in, precision, &r);
+    if (rc != BGPU_OK) return rc;
+    *out_len = r.n;
+    *out_pp = r.pp;
+    *out_neg = r.neg ? 1 : 0;
+    if (r.n > out_cap) return BGPU_ERR_OUT_CAPACITY;
+    rc = device_to_host(out, r.d, r.n * 4, g.stream);
+    return check_device_error(rc);
+}
+
+// in.reciprocal(precision) with the value's digits on the device; the result
+// lies in one of the reciprocal's own slots (kRsX0, kRsX1 or kRsOut).
+int reciprocal_val(const DVal& in, size_t precision, DVal* res) {
+    const int64_t exponent = 28 * ((int64_t)in.n - 1 - in.pp) + (32 - __builtin_clz(in.top));
+    int rc;
 
     // b = *this >> exponent; b.remove_tail_zero()
     DVal b;
@@ -1302,16 +1325,201 @@ int reciprocal_steps(const uint32_t* digits, size_t n, int64_t point_pos, bool n
     }
 
     // x >>= exponent
-    DVal r;
     if (x.zero()) return BGPU_ERR_CUDA;
-    rc = shift_val(x, -exponent, kRsOut, &r);
+    return shift_val(x, -exponent, kRsOut, res);
+}
+
+// ---- BigInt::divmod (src/bigint.cpp:625-673) ----------------------------------
+// The reference divides through its own reciprocal:
+//   Q = BigInt(BigFloat::mul(BigFloat(a), BigFloat(b).reciprocal(n_a + 16), n_a + 16), mode);
+//   R = a - Q * b;
+//   one adjustment by +-1 when R breaks the mode's bound (check = true).
+// Replayed step by step on the device like the reciprocal: the estimate, Q * b
+// and the exact sums and differences are device kernels; the host follows
+// lengths, point positions and signs, and reads one compare word per test.
+
+enum DivMode : uint32_t { kTruncate = 0, kFloor = 1, kCeil = 2, kRoundHalfUp = 3 };
+
+// sign(|a| - |b|) of two integer values (point positions <= 0).
+int cmp_abs(const DVal& a, const DVal& b, int* out) {
+    if (a.zero() || b.zero()) {
+        *out = a.zero() ? (b.zero() ? 0 : -1) : 1;
+        return BGPU_OK;
+    }
+    const int64_t pp = std::max(a.pp - (int64_t)a.tz, b.pp - (int64_t)b.tz);
+    const int64_t len = std::max((int64_t)a.n - a.pp, (int64_t)b.n - b.pp) + pp;
+    if (len <= 0 || len >= ((int64_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    FrameOp f{a.d, pp - a.pp, (uint32_t)a.n, b.d, pp - b.pp, (uint32_t)b.n, (uint32_t)len, 0, nullptr};
+    unsigned long long* dr = nullptr;
+    int rc = result_block(&dr);
+    if (rc == BGPU_OK) rc = cuda_status(launch_frame_cmp(f, dr, g.stream));
+    unsigned long long w = 0;
+    if (rc == BGPU_OK) rc = read_back(reinterpret_cast<const uint32_t*>(dr), reinterpret_cast<uint32_t*>(&w), 2);
     if (rc != BGPU_OK) return rc;
-    *out_len = r.n;
-    *out_pp = r.pp;
-    *out_neg = r.neg ? 1 : 0;
-    if (r.n > out_cap) return BGPU_ERR_OUT_CAPACITY;
-    rc = device_to_host(out, r.d, r.n * 4, g.stream);
-    return check_device_error(rc);
+    *out = w == 0 ? 0 : ((w & 3u) == 1u ? 1 : -1);
+    return BGPU_OK;
+}
+
+// The exact product of two integer values into `slot`.
+int int_product(const DVal& a, const DVal& b, int slot, DVal* out) {
+    if (a.zero() || b.zero()) {
+        *out = DVal{};
+        return BGPU_OK;
+    }
+    const size_t nres = a.n + b.n + 1;
+    if (nres > ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    int rc;
+    uint32_t* dres = rslot(slot, nres, &rc);
+    unsigned long long* dr = nullptr;
+    if (rc == BGPU_OK) rc = digits_product(a, 0, b, 0, dres, nres);
+    if (rc == BGPU_OK) rc = result_block(&dr);
+    uint32_t r[4];
+    if (rc == BGPU_OK) rc = extent(dr, dres, nres, 0, 0, r);
+    if (rc != BGPU_OK) return rc;
+    if (r[0] == 0 || r[1] >= r[0]) return BGPU_ERR_CUDA;  // a product of nonzero values is nonzero
+    *out = DVal{dres + r[1], r[0] - r[1], a.pp + b.pp - (int64_t)r[1], a.neg != b.neg, 0, r[3], slot};
+    return BGPU_OK;
+}
+
+// BigInt(const BigFloat&, mode) (src/bigint.cpp:1142-1147, convert_from_BigFloat
+// :1156-1172, _round :1072-1110) of the estimate P, whose bottom digit is
+// nonzero (BigFloat::mul removes tail zeros).  Digits below the point are
+// dropped; Floor and Ceil raise |Q| by one when the sign asks for it (a
+// dropped digit is always nonzero here), RoundHalfUp when the top dropped bit
+// is set.  When every digit lies below the point and none is added, the
+// reference is left with an empty digit vector (undefined behaviour, reached
+// for 2^-28 <= |P| < 1); the engine returns the value that truncation means,
+// zero.
+int estimate_to_int(const DVal& p, uint32_t mode, const DVal& one_pos, const DVal& one_neg, DVal* q) {
+    if (p.zero() || p.pp > (int64_t)p.n) {
+        *q = DVal{};
+        return BGPU_OK;
+    }
+    if (p.pp <= 0) {  // an integer already: -pp zero digits below
+        *q = p;
+        return BGPU_OK;
+    }
+    const size_t k = (size_t)p.pp;  // dropped digits d[0..k)
+    bool inc = false;
+    if (mode == kFloor) {
+        inc = p.neg;
+    } else if (mode == kCeil) {
+        inc = !p.neg;
+    } else if (mode == kRoundHalfUp) {
+        uint32_t top_dropped = 0;
+        const int rc = read_back(p.d + (k - 1), &top_dropped, 1);
+        if (rc != BGPU_OK) return rc;
+        inc = (top_dropped >> 27) != 0;
+    }
+    if (k == p.n) {  // nothing above the point
+        *q = inc ? (p.neg ? one_neg : one_pos) : DVal{};
+        return BGPU_OK;
+    }
+    const DVal kept{p.d + k, p.n - k, 0, p.neg, 0, p.top, p.slot};
+    if (!inc) {
+        *q = kept;
+        return BGPU_OK;
+    }
+    return add_or_sub(kept, p.neg ? one_neg : one_pos, false, kRsDivQ, q);  // |Q| + 1
+}
+
+// An integer value as Digits (zero: {0}) into a host buffer.
+int int_out(const DVal& v, uint32_t* out, size_t cap, size_t* len, int* neg) {
+    if (v.zero()) {
+        *len = 1;
+        *neg = 0;
+        if (cap < 1) return BGPU_ERR_OUT_CAPACITY;
+        out[0] = 0;
+        return BGPU_OK;
+    }
+    if (v.pp > 0) return BGPU_ERR_CUDA;  // not an integer
+    const size_t low = (size_t)(-v.pp);
+    *len = v.n + low;
+    *neg = v.neg ? 1 : 0;
+    if (*len > cap) return BGPU_ERR_OUT_CAPACITY;
+    if (low) memset(out, 0, low * 4);
+    return device_to_host(out + low, v.d, v.n * 4, g.stream);
+}
+
+// A host integer (Digits, no leading zeros) on the device as BigFloat(x): tail
+// zeros removed, point position -tz.
+int upload_int(int slot, const uint32_t* digits, size_t n, bool neg, DVal* out) {
+    if (n == 1 && digits[0] == 0) {
+        *out = DVal{};
+        return BGPU_OK;
+    }
+    size_t tz = 0;
+    while (digits[tz] == 0) ++tz;
+    int rc;
+    uint32_t* d = rslot(slot, n - tz, &rc);
+    if (rc == BGPU_OK) rc = host_to_device(d, digits + tz, (n - tz) * 4, g.stream, nullptr);
+    if (rc != BGPU_OK) return rc;
+    *out = DVal{d, n - tz, -(int64_t)tz, neg, 0, digits[n - 1], slot};
+    return BGPU_OK;
+}
+
+int divmod_steps(const uint32_t* a, size_t na, bool a_neg, const uint32_t* b, size_t nb, bool b_neg,
+                 uint32_t mode, bool check, uint32_t* q, size_t q_cap, size_t* q_len, int* q_neg,
+                 uint32_t* r, size_t r_cap, size_t* r_len, int* r_neg) {
+    for (const auto& [d, n] : {std::pair{a, na}, std::pair{b, nb}}) {
+        if (n >= ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+        for (size_t i = 0; i < n; ++i)
+            if (d[i] >> 28) return BGPU_ERR_INVALID_ARG;
+        if (n > 1 && d[n - 1] == 0) return BGPU_ERR_INVALID_ARG;  // a leading zero digit
+    }
+    if (nb == 1 && b[0] == 0) return BGPU_ERR_INVALID_ARG;  // division by zero (std::domain_error)
+    if (mode > kRoundHalfUp) mode = kTruncate;            // the reference's default branch
+    DVal A, B, Q, R;
+    int rc = upload_int(kRsDivA, a, na, a_neg && !(na == 1 && a[0] == 0), &A);
+    if (rc == BGPU_OK) rc = upload_int(kRsDivB, b, nb, b_neg, &B);
+    if (rc != BGPU_OK) return rc;
+    if (!A.zero()) {
+        const size_t precision = na + 16;  // PROTECT_PRECISION
+        DVal inv, p, one_pos, one_neg, qb;
+        rc = reciprocal_val(B, precision, &inv);
+        if (rc == BGPU_OK) rc = mul_trunc(A, inv, precision, kRsDivP, &p);
+        if (rc == BGPU_OK) rc = upload_digits(kRsOne, std::vector<uint32_t>{1u}, 0, false, &one_pos);
+        if (rc != BGPU_OK) return rc;
+        one_neg = one_pos;
+        one_neg.neg = true;
+        rc = estimate_to_int(p, mode, one_pos, one_neg, &Q);
+        if (rc == BGPU_OK) rc = int_product(Q, B, kRsDivQB, &qb);
+        if (rc == BGPU_OK) rc = add_or_sub(A, qb, true, kRsDivR, &R);  // R = a - Q * b
+        if (rc != BGPU_OK) return rc;
+        if (check && !R.zero()) {
+            bool adjust;
+            int c = 0;
+            if (mode == kRoundHalfUp) {
+                DVal r2;
+                rc = add_or_sub(R, R, false, kRsDivR2, &r2);
+                if (rc == BGPU_OK) rc = cmp_abs(r2, B, &c);
+                adjust = c > 0 || (c == 0 && R.neg == a_neg);
+            } else {
+                rc = cmp_abs(R, B, &c);
+                const bool over = c >= 0;
+                if (mode == kFloor) adjust = (R.neg != b_neg) || over;
+                else if (mode == kCeil) adjust = (R.neg == b_neg) || over;
+                else adjust = (R.neg != a_neg) || over;
+            }
+            if (rc != BGPU_OK) return rc;
+            if (adjust) {
+                DVal q2, r2;
+                const bool down = R.neg != b_neg;  // R += b, --Q; else R -= b, ++Q
+                rc = add_or_sub(R, B, !down, kRsDivR2, &r2);
+                if (rc == BGPU_OK) rc = add_or_sub(Q, one_pos, down, kRsDivQ2, &q2);
+                if (rc != BGPU_OK) return rc;
+                Q = q2;
+                R = r2;
+            }
+        }
+    }
+    const int rq = int_out(Q, q, q_cap, q_len, q_neg);
+    if (rq != BGPU_OK && rq != BGPU_ERR_OUT_CAPACITY) return rq;
+    const int rr = int_out(R, r, r_cap, r_len, r_neg);
+    if (rr != BGPU_OK && rr != BGPU_ERR_OUT_CAPACITY) return rr;
+    rc = check_device_error(BGPU_OK);
+    if (rc != BGPU_OK) return rc;
+    return rq != BGPU_OK ? rq : rr;
 }
 
 }  // namespace
@@ -1384,6 +1592,19 @@ int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, 
     cudaSetDevice(g.device);
     return reciprocal_locked(digits, n, point_pos, is_neg != 0, precision, out, out_cap, out_len,
                              out_point_pos, out_is_neg);
+}
+
+int bgpu_divmod_digits(const uint32_t* a, size_t na, int a_neg, const uint32_t* b, size_t nb, int b_neg,
+                       uint32_t mode, int check, uint32_t* q, size_t q_cap, size_t* q_len, int* q_neg,
+                       uint32_t* r, size_t r_cap, size_t* r_len, int* r_neg) {
+    if (!a || !b || na == 0 || nb == 0 || !q_len || !q_neg || !r_len || !r_neg || (!q && q_cap) ||
+        (!r && r_cap) || mode > 255)
+        return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return with_device_status(divmod_steps(a, na, a_neg != 0, b, nb, b_neg != 0, mode, check != 0, q, q_cap,
+                                           q_len, q_neg, r, r_cap, r_len, r_neg));
 }
 
 int bgpu_selftest_wait(uint32_t spin_limit, int set_flag) {

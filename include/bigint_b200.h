@@ -172,6 +172,23 @@ int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, 
                            size_t precision, uint32_t* out, size_t out_cap, size_t* out_len,
                            int64_t* out_point_pos, int* out_is_neg);
 
+/* Quotient and remainder: the reference's BigInt::divmod(b, mode, check)
+ * (src/bigint.cpp:625-673) on +-A and +-B given as Digits (28-bit, no leading
+ * zeros; zero is the single digit 0) and signs.  The reference's steps run on
+ * the GPU: the estimate BigFloat::mul(A, B.reciprocal(n_a + 16), n_a + 16)
+ * rounded by `mode` (0 Truncate, 1 Floor, 2 Ceil, 3 RoundHalfUp; other values
+ * below 256 act as Truncate, as in the reference), R = A - Q * B, and with
+ * `check` one adjustment by +-1 when R breaks the mode's bound.  Writes Q's
+ * and R's Digits and signs, identical to the reference's.  Where the
+ * reference's conversion of the estimate is undefined (2^-28 <= |estimate| <
+ * 1 with nothing added by the rounding), Q starts from zero.  B = 0 (the
+ * reference throws std::domain_error), digits >= 2^28, a leading zero digit or
+ * mode >= 256 give BGPU_ERR_INVALID_ARG; BGPU_ERR_OUT_CAPACITY when a buffer
+ * is too small (*q_len and *r_len = the lengths needed). */
+int bgpu_divmod_digits(const uint32_t* a, size_t na, int a_neg, const uint32_t* b, size_t nb, int b_neg,
+                       uint32_t mode, int check, uint32_t* q, size_t q_cap, size_t* q_len, int* q_neg,
+                       uint32_t* r, size_t r_cap, size_t* r_len, int* r_neg);
+
 /* Device-resident product (no host copies, asynchronous on `stream`, a
  * cudaStream_t; 0 is the legacy default stream): d_out receives exactly
  * na + nb limbs (zero padded).  d_a == d_b with na == nb squares.  Errors

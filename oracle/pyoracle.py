@@ -161,6 +161,12 @@ class Reference(_Lib):
         if self.has_to_dec:
             L.ref_to_dec_string.argtypes = [_u64p, C.c_size_t, C.c_char_p, C.c_size_t, _szp]
             L.ref_to_dec_string.restype = C.c_int
+        self.has_divmod = hasattr(L, "ref_divmod")
+        if self.has_divmod:
+            L.ref_divmod.argtypes = [_u64p, C.c_size_t, C.c_int, _u64p, C.c_size_t, C.c_int, C.c_uint32,
+                                     C.c_int, _u32p, C.c_size_t, _szp, C.POINTER(C.c_int), _u32p,
+                                     C.c_size_t, _szp, C.POINTER(C.c_int)]
+            L.ref_divmod.restype = C.c_int
         self.has_from_dec = hasattr(L, "ref_from_dec_string")
         if self.has_from_dec:
             L.ref_from_dec_string.argtypes = [C.c_char_p, C.c_size_t, _u32p, C.c_size_t, _szp,
@@ -232,6 +238,22 @@ class Reference(_Lib):
             raise OracleError(f"ref_bigfloat_reciprocal returned {rc}")
         return ((din[: nin.value].copy(), int(ppin.value), bool(neg)),
                 (out[: nout.value].copy(), int(pp.value), bool(oneg.value)))
+
+    def divmod(self, a_limbs, a_neg: bool, b_limbs, b_neg: bool, mode: int = 0, check: bool = True):
+        """(+-A).divmod(+-B, mode, check) for A, B given by little-endian u64
+        limbs: ((Q Digits, Q negative), (R Digits, R negative)).  |A / B| must
+        stay out of [2^-28, 1] (the reference's conversion is undefined there)."""
+        la, lb = _limbs(a_limbs), _limbs(b_limbs)
+        qcap = max(la.size - lb.size + 2, 1) * 3 + 8
+        rcap = max(la.size, lb.size) * 3 + 8
+        q, r = np.zeros(qcap, dtype=np.uint32), np.zeros(rcap, dtype=np.uint32)
+        nq, nr, qn, rn = C.c_size_t(0), C.c_size_t(0), C.c_int(0), C.c_int(0)
+        rc = self.lib.ref_divmod(_p64(la), la.size, int(bool(a_neg)), _p64(lb), lb.size, int(bool(b_neg)),
+                                 int(mode), int(bool(check)), _p32(q), qcap, C.byref(nq), C.byref(qn),
+                                 _p32(r), rcap, C.byref(nr), C.byref(rn))
+        if rc != 0:
+            raise OracleError(f"ref_divmod returned {rc}")
+        return ((q[: nq.value].copy(), bool(qn.value)), (r[: nr.value].copy(), bool(rn.value)))
 
     def to_dec_string(self, limbs) -> str:
         """Decimal text of the integer with little-endian u64 ``limbs``

@@ -1,6 +1,6 @@
 // C-ABI shim over the UNMODIFIED reference multiply path (Looading99/BigInt),
 // compiled together with the reference's own sources into
-// oracle/_ref/libbigint_ref.so by oracle/build_ref.sh.  It is test
+// oracle/_ref/libbigint_ref.so by oracle/build.py (build_ref).  It is test
 // infrastructure: the parity tests, the golden-vector generator and the
 // bench's CPU reference arm load it; the product never does.
 //
@@ -17,6 +17,7 @@
 //   ref_bigfloat_reciprocal -> the same on BigFloat(x, offset), negated on request
 //   ref_to_dec_string -> BigInt::print (decimal)  src/bigint.cpp:175-247
 //   ref_from_dec_string -> BigInt(std::string)     src/bigint.cpp:25-124
+//   ref_divmod      -> BigInt::divmod             src/bigint.cpp:625-673
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -192,6 +193,32 @@ int ref_from_dec_string(const char* s, size_t len, uint32_t* out, size_t cap, si
     const bigint::BigInt x(std::string(s, len), false);
     *neg = x.sign() < 0 ? 1 : 0;
     return copy_out32(x.get_data(), out, cap, out_len);
+}
+
+// a.divmod(b, mode, check) (src/bigint.cpp:625-673) for A and B given by
+// little-endian u64 limbs (built through the hex-string constructor) and
+// signs: the quotient's and the remainder's Digits and signs.  The caller
+// keeps |A / B| away from [2^-28, 1], where the reference's conversion of the
+// quotient estimate leaves an empty digit vector (undefined behaviour).
+int ref_divmod(const uint64_t* a, size_t na, int a_neg, const uint64_t* b, size_t nb, int b_neg,
+               uint32_t mode, int check, uint32_t* q, size_t q_cap, size_t* q_len, int* q_neg,
+               uint32_t* r, size_t r_cap, size_t* r_len, int* r_neg) {
+    static const char hexd[] = "0123456789abcdef";
+    auto make = [](const uint64_t* limbs, size_t n, int neg) {
+        std::string hex;
+        hex.reserve(16 * n);
+        for (size_t i = n; i-- > 0;)
+            for (int k = 15; k >= 0; --k) hex.push_back(hexd[(limbs[i] >> (4 * k)) & 15]);
+        bigint::BigInt x(hex, true);
+        return neg ? -x : x;
+    };
+    const bigint::BigInt A = make(a, na, a_neg), B = make(b, nb, b_neg);
+    const auto [Q, R] = A.divmod(B, static_cast<bigint::RoundMode>(mode), check != 0);
+    *q_neg = Q.sign() < 0 ? 1 : 0;
+    *r_neg = R.sign() < 0 ? 1 : 0;
+    const int rq = copy_out32(Q.get_data(), q, q_cap, q_len);
+    const int rr = copy_out32(R.get_data(), r, r_cap, r_len);
+    return rq != 0 || rr != 0 ? -1 : 0;
 }
 
 // fast_pow over BigInt, as the reference's benchmark example calls it
