@@ -12,7 +12,11 @@ replay the reference's BigFloat::reciprocal (src/bigint.cpp:1044-1071):
 * ``add_or_sub`` -- BigFloat::add_or_sub (src/bigint.cpp:849-936) as the exact
   sum or difference in the reference's frame, leading and bottom zeros
   removed;
-* ``shift``, ``to_double``, ``from_double`` -- src/bigint.cpp:681-812.
+* ``shift``, ``to_double``, ``from_double`` -- src/bigint.cpp:681-812;
+* ``divmod`` -- BigInt::divmod (src/bigint.cpp:625-673) as the engine replays
+  it for ``bgpu_divmod_digits``: the estimate through ``reciprocal`` and
+  ``mul_trunc``, its rounding to an integer (BigInt(const BigFloat&, mode),
+  src/bigint.cpp:1072-1172), R = a - Q * b and the single adjustment.
 
 tests/test_oracle_bigfloat.py pins this model against the reference's own
 reciprocal; the GPU tests pin the device against the reference.  Only the
@@ -173,3 +177,60 @@ def reciprocal(digits, pp: int, neg: bool, precision: int) -> Val:
         t3 = mul_trunc(x, t2, cur + 1)
         x = add_or_sub(x, t3, False)
     return shift(x, -expo)
+
+
+def _bigfloat_of_int(d, neg: bool) -> Val:
+    """BigFloat(BigInt) (include/bigint/bigint.h:382-388): tail zeros removed."""
+    d = [int(x) for x in d]
+    if len(d) == 1 and d[0] == 0:
+        return Val([0], 0, False)
+    t = 0
+    while d[t] == 0:
+        t += 1
+    return Val(d[t:], -t, neg)
+
+
+def _signed(v: Val) -> int:
+    """The integer value of a Val whose point position is <= 0."""
+    if v.zero():
+        return 0
+    return (-1 if v.neg else 1) * (_int(v.d) << (28 * -v.pp))
+
+
+def divmod(a, a_neg: bool, b, b_neg: bool, mode: int, check: bool = True):
+    """(Q, R) as Python integers.  mode: 0 Truncate, 1 Floor, 2 Ceil,
+    3 RoundHalfUp (others act as Truncate).  Where the reference's rounding
+    of the estimate leaves no digits (2^-28 <= |estimate| < 1, nothing added),
+    Q starts from zero, as on the device."""
+    A, B = _bigfloat_of_int(a, a_neg), _bigfloat_of_int(b, b_neg)
+    if B.zero():
+        raise ZeroDivisionError("division by zero")
+    if A.zero():
+        return 0, 0
+    prec = len(a) + 16
+    p = mul_trunc(A, reciprocal(B.d, B.pp, B.neg, prec), prec)
+    if p.zero() or p.pp > len(p.d):
+        q = 0
+    elif p.pp <= 0:
+        q = _signed(p)
+    else:
+        k = p.pp  # digits below the point; p.d[0] != 0
+        inc = {1: p.neg, 2: not p.neg, 3: bool(p.d[k - 1] >> 27)}.get(mode, False)
+        mag = (_int(p.d[k:]) if k < len(p.d) else 0) + int(inc)
+        q = -mag if p.neg else mag
+    av, bv = _signed(A), _signed(B)
+    r = av - q * bv
+    if check and r != 0:
+        rn, bn, an = r < 0, bv < 0, av < 0
+        if mode == 3:
+            c = (abs(2 * r) > abs(bv)) - (abs(2 * r) < abs(bv))
+            adjust = c > 0 or (c == 0 and rn == an)
+        else:
+            over = abs(r) >= abs(bv)
+            adjust = {1: rn != bn or over, 2: rn == bn or over}.get(mode, rn != an or over)
+        if adjust:
+            if rn != bn:
+                r, q = r + bv, q - 1
+            else:
+                r, q = r - bv, q + 1
+    return q, r
