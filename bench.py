@@ -627,6 +627,48 @@ def divmod_form(bb, port, cpu: bool = True, reps: int = 5):
     return res
 
 
+def bigfloat_print_form(bb, cpu: bool = True, reps: int = 5):
+    """BigFloat::print (src/bigint.cpp:972-1041) of a 2^22-bit value with the
+    point in the middle and the default fraction length (all its fraction
+    Digits: 631 306 decimals), through bgpu_bigfloat_to_decimal (5^d, the
+    scaled fraction, its rounding and both decimal conversions on the device);
+    the reference's own print on the host cores beside it (one run), texts
+    compared."""
+    rng = np.random.default_rng(SEED + 11)
+    limbs = rng.integers(0, 2**64, (1 << 22) // 64, dtype=np.uint64)
+    limbs[-1] |= np.uint64(1 << 63)
+    limbs[0] |= np.uint64(1)  # no zero digit at the bottom: the fields below are BigFloat(X, offset)'s
+    digits = limbs_to_digits28_np(limbs)
+    offset = -28 * (digits.size // 2)
+    pp = digits.size // 2
+    bb.bigfloat_to_decimal(digits, pp)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        text = bb.bigfloat_to_decimal(digits, pp)
+        times.append(time.perf_counter() - t0)
+    res = {"bits": 1 << 22, "point_pos": pp, "chars": len(text), "s": statistics.median(times),
+           "api": "bgpu_bigfloat_to_decimal (host Digits in, host text out)"}
+    from oracle.pyoracle import Reference, have_reference
+
+    if cpu and have_reference() and Reference().has_bigfloat_print:
+        ref = Reference()
+        ref.init_thread_pool(host_cores())
+        t0 = time.perf_counter()
+        (din, ppin), want = ref.bigfloat_print(limbs, offset, False, 0)
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+                                "call": "BigFloat::print"}
+        if not (np.array_equal(din, digits) and ppin == pp and text == want):
+            raise SystemExit("bench BigFloat print: text differs from the reference's")
+        res["verified"] = "identical text"
+    else:
+        head, frac = text.split(".")
+        if bb.to_decimal(digits[pp:]) != head or len(frac) != int(28 * pp * 0.30102999566398120):
+            raise SystemExit("bench BigFloat print: integer part or fraction length wrong")
+        res["verified"] = "integer part equals bgpu_to_decimal's; fraction length"
+    return res
+
+
 def decimal_print_form(bb, cpu: bool = True):
     """Decimal text of a 2^22-bit integer (1.26 M digits): bgpu_to_decimal
     (the whole conversion on the GPU, host Digits in, host text out); the
@@ -1077,6 +1119,7 @@ def run_gpu_arm(args) -> None:
                  "mul_digits_2p24": mul_digits_form(bb, port, cpu=not args.no_cpu_baseline),
                  "reciprocal_2p24": reciprocal_form(bb, cpu=not args.no_cpu_baseline),
                  "divmod_2p24": divmod_form(bb, port, cpu=not args.no_cpu_baseline),
+                 "bigfloat_print_2p22": bigfloat_print_form(bb, cpu=not args.no_cpu_baseline),
                  "decimal_print_2p22": decimal_print_form(bb, cpu=not args.no_cpu_baseline),
                  "decimal_parse_5m": decimal_parse_form(bb, cpu=not args.no_cpu_baseline),
                  "batched_4096": batched_form(bb, torch, device, port),
@@ -1128,7 +1171,7 @@ def run_gpu_arm(args) -> None:
 
 
 FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
-         "divmod_2p24", "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
+         "divmod_2p24", "bigfloat_print_2p22", "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
          "product_tree_2p20")
 
 
@@ -1162,6 +1205,8 @@ def run_single_form(args) -> None:
         res = reciprocal_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "divmod_2p24":
         res = divmod_form(bb, port, cpu=not args.no_cpu_baseline)
+    elif name == "bigfloat_print_2p22":
+        res = bigfloat_print_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_print_2p22":
         res = decimal_print_form(bb, cpu=not args.no_cpu_baseline)
     elif name == "decimal_parse_5m":

@@ -18,6 +18,7 @@ this package           reference                                       C-ABI
 ``divmod_digits``      ``BigInt::divmod`` (bigint.cpp:625-673)          ``bgpu_divmod_digits``
 ``from_decimal(text)`` ``BigInt(const std::string&)`` (bigint.cpp:25-124) ``bgpu_from_decimal``
 ``to_decimal(d, neg)`` ``BigInt::print`` (bigint.cpp:175-247)          ``bgpu_to_decimal``
+``bigfloat_to_decimal`` ``BigFloat::print`` (bigint.cpp:972-1041)       ``bgpu_bigfloat_to_decimal``
 ``init(device)``       ``bigint::init_thread_pool`` (bigint.h:35-38)   ``bgpu_init``
 =====================  ==============================================  =========================
 
@@ -49,6 +50,7 @@ from ._lib import (  # noqa: F401
     ROUND_TRUNCATE,
     BatchPlan,
     BigIntGPUError,
+    bigfloat_to_decimal,
     Stats,
     brute_mul,
     device_status,

@@ -114,6 +114,9 @@ def _load() -> C.CDLL:
                                      u32p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int), u32p,
                                      C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
     L.bgpu_divmod_digits.restype = C.c_int
+    L.bgpu_bigfloat_to_decimal.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, C.c_char_p,
+                                           C.c_size_t, C.POINTER(C.c_size_t)]
+    L.bgpu_bigfloat_to_decimal.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_uint32, C.c_void_p]
     L.bgpu_mul_u64_device.restype = C.c_int
@@ -445,6 +448,32 @@ def reciprocal_digits(digits, point_pos: int = 0, neg: bool = False, precision: 
         cap = n.value
     _check(rc, "bgpu_reciprocal_digits")
     return out[: n.value], int(pp.value), bool(ng.value)
+
+
+def bigfloat_to_decimal(digits, point_pos: int = 0, neg: bool = False, dec_digits: int = 0) -> str:
+    """``BigFloat::print(out, dec_digits)`` (src/bigint.cpp:972-1041) on the GPU.
+
+    The input is a BigFloat's fields: 28-bit Digits without a leading zero
+    digit, the point position (value = digits * 2^(-28 point_pos)) and the
+    sign.  Returns the reference's text, "[-]int.frac" with the fraction
+    rounded half up to ``dec_digits`` digits (0: as many as its Digits hold)
+    (``bgpu_bigfloat_to_decimal``)."""
+    _ensure_init()
+    d = _as_digits(digits)
+    if d.size == 0:
+        raise BigIntGPUError(-1, "bgpu_bigfloat_to_decimal (empty input)")
+    u32p = C.POINTER(C.c_uint32)
+    cap = int(d.size * 28 * 0.30103) + abs(int(point_pos)) * 9 + int(dec_digits) + 64
+    for _ in range(2):
+        out = C.create_string_buffer(cap)
+        n = C.c_size_t(0)
+        rc = lib.bgpu_bigfloat_to_decimal(d.ctypes.data_as(u32p), d.size, int(point_pos), int(bool(neg)),
+                                          int(dec_digits), out, cap, C.byref(n))
+        if rc != -5:
+            break
+        cap = n.value
+    _check(rc, "bgpu_bigfloat_to_decimal")
+    return out.raw[: n.value].decode()
 
 
 ROUND_TRUNCATE, ROUND_FLOOR, ROUND_CEIL, ROUND_HALF_UP = 0, 1, 2, 3  # the reference's RoundMode

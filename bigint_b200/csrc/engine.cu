@@ -7,6 +7,7 @@
 //   bgpu_mul_digits  <- bigint::mul::mul_digits        (include/bigint/mul.h:223-318)
 //   bgpu_reciprocal_digits <- BigFloat::reciprocal      (src/bigint.cpp:1044-1071)
 //   bgpu_divmod_digits     <- BigInt::divmod            (src/bigint.cpp:625-673)
+//   bgpu_bigfloat_to_decimal <- BigFloat::print         (src/bigint.cpp:972-1041)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,8 +48,8 @@ struct Engine {
     size_t io_bytes = 0;
     TreeArena tree;  // product-tree values, descriptors and scratch
     // digit buffers of the device-resident reciprocal (one per live value)
-    uint32_t* rs[19] = {};
-    size_t rs_bytes[19] = {};
+    uint32_t* rs[23] = {};
+    size_t rs_bytes[23] = {};
     // block products of the decomposition beyond the largest transform
     void* d_huge = nullptr;
     size_t huge_bytes = 0;
@@ -876,7 +877,9 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
 enum RecipSlot {
     kRsIn, kRsB, kRsX0, kRsX1, kRsT1, kRsT2, kRsT3, kRsOut, kRsScratch, kRsSmall, kRsOne,
     // divmod: the operands, the quotient estimate, Q, Q * b, R and the adjusted Q and R
-    kRsDivA, kRsDivB, kRsDivP, kRsDivQ, kRsDivQB, kRsDivR, kRsDivQ2, kRsDivR2, kRsSlots
+    kRsDivA, kRsDivB, kRsDivP, kRsDivQ, kRsDivQB, kRsDivR, kRsDivQ2, kRsDivR2,
+    // small powers (BigFloat::print's 5^d): running base and result, two each
+    kRsPowB0, kRsPowB1, kRsPowR0, kRsPowR1, kRsSlots
 };
 
 constexpr uint32_t kDigitMask = (1u << 28) - 1u;
@@ -1969,18 +1972,20 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
 // floors of the same real, squared), one Newton step from below brings it
 // within a few units, and single correction steps make it exact.  Leaves of
 // 128 limbs print 2432 characters per thread.
-static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* out, size_t out_cap,
-                             size_t* out_len) {
-    for (size_t i = 0; i < n; ++i)
-        if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
-    n = strip32(digits, n);
-    if (n == 0) {  // the reference prints zero as "0", without a sign
-        *out_len = 1;
-        if (out_cap < 1) return BGPU_ERR_OUT_CAPACITY;
-        out[0] = '0';
+// Decimal text (no sign, no leading zeros) of the integer whose Digits are n
+// digits at hsrc (host) or dsrc (device), the top one `top` (nonzero), above
+// `low` zero digits: h[first..) on return.
+static int dec_chars(const uint32_t* hsrc, const uint32_t* dsrc, size_t low, size_t n, uint32_t top,
+                     std::vector<char>* hv, size_t* first_out) {
+    std::vector<char>& h = *hv;
+    if (n == 0) {
+        h.assign(1, '0');
+        *first_out = 0;
         return BGPU_OK;
     }
-    const uint64_t bits = 28 * (uint64_t)(n - 1) + (32 - __builtin_clz(digits[n - 1]));
+    const size_t nsrc = n;
+    n += low;
+    const uint64_t bits = 28 * (uint64_t)(n - 1) + (32 - __builtin_clz(top));
     const uint64_t dmax = (uint64_t)std::ceil((double)bits * 0.30102999566398120) + 1;  // >= decimal digits
     const int J = ceil_log2((dmax + 18) / 19);
     if (J > 25) return BGPU_ERR_CAPACITY;
@@ -2009,9 +2014,13 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
     cudaStream_t st = g.stream;
 
     // the value, as NL limbs; the powers of ten and their reciprocals
-    rc = host_to_device(ddig, digits, n * 4, st, nullptr);
+    cudaError_t e = low ? cudaMemsetAsync(ddig, 0, low * 4, st) : cudaSuccess;
+    rc = cuda_status(e);
+    if (rc == BGPU_OK)
+        rc = hsrc ? host_to_device(ddig + low, hsrc, nsrc * 4, st, nullptr)
+                  : cuda_status(cudaMemcpyAsync(ddig + low, dsrc, nsrc * 4, cudaMemcpyDeviceToDevice, st));
     if (rc != BGPU_OK) return rc;
-    cudaError_t e = launch_digits28_to_limbs(ddig, (uint32_t)n, lvl[0], (uint32_t)NL, st);
+    e = launch_digits28_to_limbs(ddig, (uint32_t)n, lvl[0], (uint32_t)NL, st);
     if (e != cudaSuccess) return cuda_status(e);
     uint32_t nl = 0;
     rc = ensure_powers(J, J > jleaf, st, &nl);
@@ -2044,20 +2053,182 @@ static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* o
     const uint64_t nleaf = std::min<uint64_t>(NL / w0, (dmax + 19 * w0 - 1) / (19 * w0));
     e = launch_dec_print_leaves(lvl[cur], w0, nleaf, chars, st);
     if (e != cudaSuccess) return cuda_status(e);
-    std::vector<char> h(19 * w0 * nleaf);
+    h.resize(19 * w0 * nleaf);
     rc = device_to_host(h.data(), chars, h.size(), st);
     rc = check_device_error(rc);
     if (rc != BGPU_OK) return rc;
     size_t first = 0;
     while (first + 1 < h.size() && h[first] == '0') ++first;
+    *first_out = first;
+    g.last_launches = nl;
+    return BGPU_OK;
+}
+
+static int to_decimal_locked(const uint32_t* digits, size_t n, bool neg, char* out, size_t out_cap,
+                             size_t* out_len) {
+    for (size_t i = 0; i < n; ++i)
+        if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    n = strip32(digits, n);
+    if (n == 0) {  // the reference prints zero as "0", without a sign
+        *out_len = 1;
+        if (out_cap < 1) return BGPU_ERR_OUT_CAPACITY;
+        out[0] = '0';
+        return BGPU_OK;
+    }
+    std::vector<char> h;
+    size_t first = 0;
+    const int rc = dec_chars(digits, nullptr, 0, n, digits[n - 1], &h, &first);
+    if (rc != BGPU_OK) return rc;
     const size_t len = (h.size() - first) + (neg ? 1 : 0);
     *out_len = len;
-    g.last_launches = nl;
     if (len > out_cap) return BGPU_ERR_OUT_CAPACITY;
     size_t o = 0;
     if (neg) out[o++] = '-';
     memcpy(out + o, h.data() + first, h.size() - first);
     return BGPU_OK;
+}
+
+// ---- BigFloat::print (src/bigint.cpp:972-1041) --------------------------------
+
+// base^e (e >= 1) as a device value by the reference's fast_pow
+// (include/bigint/bigint_base.h:60-69): multiply on a set bit, then square.
+static int small_pow_val(uint32_t base, uint32_t e, DVal* out) {
+    DVal b, r;
+    int rc = upload_digits(kRsPowB0, std::vector<uint32_t>{base}, 0, false, &b);
+    if (rc != BGPU_OK) return rc;
+    bool have_r = false;
+    int cb = 0, cr = 0;
+    for (; e; e >>= 1) {
+        if (e & 1) {
+            if (!have_r) {  // res = 1 * base: a copy
+                uint32_t* d = rslot(kRsPowR0 + cr, b.n, &rc);
+                if (rc == BGPU_OK)
+                    rc = cuda_status(cudaMemcpyAsync(d, b.d, b.n * 4, cudaMemcpyDeviceToDevice, g.stream));
+                if (rc != BGPU_OK) return rc;
+                r = b;
+                r.d = d;
+                r.slot = kRsPowR0 + cr;
+                have_r = true;
+            } else {
+                DVal t;
+                rc = int_product(r, b, kRsPowR0 + (cr ^ 1), &t);
+                if (rc != BGPU_OK) return rc;
+                cr ^= 1;
+                r = t;
+            }
+        }
+        if (e > 1) {  // the reference's last squaring does not change the result
+            DVal t;
+            rc = int_product(b, b, kRsPowB0 + (cb ^ 1), &t);
+            if (rc != BGPU_OK) return rc;
+            cb ^= 1;
+            b = t;
+        }
+    }
+    *out = r;
+    return BGPU_OK;
+}
+
+// The reference's print of a BigFloat (digits, point position, sign) with
+// dec_digits fraction digits (0: as many as the fraction's Digits hold):
+//   int part = the digits above the point; frac = the digits below it;
+//   F = BigInt(BigFloat(frac * 5^d, d - 28 pp), RoundHalfUp)   (= frac 10^d, rounded)
+//   F == 10^d: F = 0, ++int part;
+//   "-"? int "." F padded to d digits.
+// The product, shift, rounding and comparison run as device steps; both
+// parts are printed by the device decimal conversion.  Where the reference's
+// rounding leaves no digits (2^-28 <= frac 10^d < 1/2; undefined behaviour),
+// F is zero.
+static int bigfloat_print_steps(const uint32_t* digits, size_t n, int64_t pp, bool neg, size_t dec_digits,
+                                char* out, size_t out_cap, size_t* out_len) {
+    if (n >= ((size_t)1 << 31)) return BGPU_ERR_CAPACITY;
+    for (size_t i = 0; i < n; ++i)
+        if (digits[i] >> 28) return BGPU_ERR_INVALID_ARG;
+    if (n > 1 && digits[n - 1] == 0) return BGPU_ERR_INVALID_ARG;  // a leading zero digit
+    const int64_t sn = (int64_t)n;
+    // int part: digits [max(pp, 0), n) above -pp zero digits; {0} when pp >= n
+    const size_t ilo = pp > 0 ? (size_t)pp : 0, ilow = pp < 0 ? (size_t)(-pp) : 0;
+    size_t icount = pp < sn ? strip32(digits + ilo, n - ilo) : 0;
+    // frac: digits [0, min(pp, n)); the default d counts them before leading zeros go
+    const size_t fsize = pp > 0 ? (size_t)std::min(pp, sn) : 0;
+    if (dec_digits == 0) dec_digits = (size_t)std::floor((double)(fsize * 28) * std::log10(2.0));
+    if (dec_digits > ((size_t)1 << 28)) return BGPU_ERR_CAPACITY;
+    const size_t fcount = strip32(digits, fsize);
+    DVal F;  // zero
+    bool carry = false;
+    int rc = BGPU_OK;
+    if (dec_digits && fcount) {
+        DVal frac, K, X, S, T, one_pos, one_neg;
+        rc = upload_int(kRsDivB, digits, fcount, false, &frac);
+        if (rc == BGPU_OK) rc = small_pow_val(5, (uint32_t)dec_digits, &K);
+        if (rc == BGPU_OK) rc = int_product(frac, K, kRsDivQB, &X);
+        // BigFloat(X, -offset) with offset = 28 pp - d: X << (d - 28 pp), tail zeros removed
+        if (rc == BGPU_OK) rc = shift_val(X, (int64_t)dec_digits - 28 * pp, kRsDivR, &S);
+        if (rc != BGPU_OK) return rc;
+        S.d += S.tz;
+        S.n -= S.tz;
+        S.pp -= (int64_t)S.tz;
+        S.tz = 0;
+        rc = upload_digits(kRsOne, std::vector<uint32_t>{1u}, 0, false, &one_pos);
+        if (rc != BGPU_OK) return rc;
+        one_neg = one_pos;
+        one_neg.neg = true;
+        rc = estimate_to_int(S, kRoundHalfUp, one_pos, one_neg, &F);
+        // F == 10^d = 5^d << d ?
+        if (rc == BGPU_OK && !F.zero()) rc = shift_val(K, (int64_t)dec_digits, kRsDivR2, &T);
+        int c = 1;
+        if (rc == BGPU_OK && !F.zero()) rc = cmp_abs(F, T, &c);
+        if (rc != BGPU_OK) return rc;
+        if (c == 0) {
+            F = DVal{};
+            carry = true;
+        }
+    }
+    std::vector<char> ti, tf;
+    size_t fi = 0, ff = 0;
+    if (carry) {  // ++int part on the device
+        DVal I, I1, one;
+        rc = upload_digits(kRsOne, std::vector<uint32_t>{1u}, 0, false, &one);
+        if (rc == BGPU_OK && icount) {
+            uint32_t* d = rslot(kRsDivA, icount, &rc);
+            if (rc == BGPU_OK) rc = host_to_device(d, digits + ilo, icount * 4, g.stream, nullptr);
+            I = DVal{d, icount, -(int64_t)ilow, false, 0, digits[ilo + icount - 1], kRsDivA};
+        }
+        if (rc == BGPU_OK) rc = add_or_sub(I, one, false, kRsDivQ2, &I1);
+        if (rc == BGPU_OK) rc = dec_chars(nullptr, I1.d, (size_t)(-I1.pp), I1.n, I1.top, &ti, &fi);
+    } else {
+        rc = dec_chars(digits + ilo, nullptr, icount ? ilow : 0, icount, icount ? digits[ilo + icount - 1] : 0,
+                       &ti, &fi);
+    }
+    if (rc == BGPU_OK && dec_digits) {
+        if (F.zero()) rc = dec_chars(nullptr, nullptr, 0, 0, 0, &tf, &ff);
+        else rc = F.pp > 0 ? BGPU_ERR_CUDA : dec_chars(nullptr, F.d, (size_t)(-F.pp), F.n, F.top, &tf, &ff);
+    }
+    if (rc != BGPU_OK) return rc;
+    const size_t li = ti.size() - fi, lf = dec_digits ? tf.size() - ff : 0;
+    if (lf > dec_digits) return BGPU_ERR_CUDA;  // F < 10^d
+    const size_t len = (neg ? 1 : 0) + li + 1 + dec_digits;
+    *out_len = len;
+    if (len > out_cap) return BGPU_ERR_OUT_CAPACITY;
+    size_t o = 0;
+    if (neg) out[o++] = '-';
+    memcpy(out + o, ti.data() + fi, li);
+    o += li;
+    out[o++] = '.';
+    memset(out + o, '0', dec_digits - lf);
+    o += dec_digits - lf;
+    if (lf) memcpy(out + o, tf.data() + ff, lf);
+    return check_device_error(BGPU_OK);
+}
+
+int bgpu_bigfloat_to_decimal(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
+                             size_t dec_digits, char* out, size_t out_cap, size_t* out_len) {
+    if (!digits || n == 0 || !out_len || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g.device < 0) return BGPU_ERR_NOT_INIT;
+    cudaSetDevice(g.device);
+    return with_device_status(
+        bigfloat_print_steps(digits, n, point_pos, is_neg != 0, dec_digits, out, out_cap, out_len));
 }
 
 int bgpu_to_decimal(const uint32_t* digits, size_t n, int is_neg, char* out, size_t out_cap, size_t* out_len) {

@@ -172,6 +172,20 @@ int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, 
                            size_t precision, uint32_t* out, size_t out_cap, size_t* out_len,
                            int64_t* out_point_pos, int* out_is_neg);
 
+/* Decimal text of a BigFloat: the reference's BigFloat::print(out, dec_digits)
+ * (src/bigint.cpp:972-1041) on the BigFloat's fields (Digits, point position,
+ * sign).  The integer part prints as it is; the fraction f becomes
+ * round_half_up(f * 10^d), with d = dec_digits (0: floor(28 * (fraction
+ * digits) * log10 2), as in the reference), carried into the integer part when
+ * it reaches 10^d, and prints padded to d digits: "[-]int.frac" (just "int."
+ * when d is 0), identical to the reference's text, not NUL-terminated.  5^d,
+ * the product, the shift, the rounding and both decimal conversions run on
+ * the GPU.  Where the reference's rounding is undefined (2^-28 <= f * 10^d <
+ * 1/2) the fraction prints as zeros.  BGPU_ERR_OUT_CAPACITY when out_cap is
+ * too small (*out_len = needed). */
+int bgpu_bigfloat_to_decimal(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
+                             size_t dec_digits, char* out, size_t out_cap, size_t* out_len);
+
 /* Quotient and remainder: the reference's BigInt::divmod(b, mode, check)
  * (src/bigint.cpp:625-673) on +-A and +-B given as Digits (28-bit, no leading
  * zeros; zero is the single digit 0) and signs.  The reference's steps run on

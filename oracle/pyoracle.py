@@ -167,6 +167,12 @@ class Reference(_Lib):
                                      C.c_int, _u32p, C.c_size_t, _szp, C.POINTER(C.c_int), _u32p,
                                      C.c_size_t, _szp, C.POINTER(C.c_int)]
             L.ref_divmod.restype = C.c_int
+        self.has_bigfloat_print = hasattr(L, "ref_bigfloat_print")
+        if self.has_bigfloat_print:
+            L.ref_bigfloat_print.argtypes = [_u64p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, _u32p,
+                                             C.c_size_t, _szp, C.POINTER(C.c_int64), C.c_char_p,
+                                             C.c_size_t, _szp]
+            L.ref_bigfloat_print.restype = C.c_int
         self.has_from_dec = hasattr(L, "ref_from_dec_string")
         if self.has_from_dec:
             L.ref_from_dec_string.argtypes = [C.c_char_p, C.c_size_t, _u32p, C.c_size_t, _szp,
@@ -254,6 +260,21 @@ class Reference(_Lib):
         if rc != 0:
             raise OracleError(f"ref_divmod returned {rc}")
         return ((q[: nq.value].copy(), bool(qn.value)), (r[: nr.value].copy(), bool(rn.value)))
+
+    def bigfloat_print(self, limbs, offset: int, neg: bool, dec_digits: int = 0):
+        """(+-BigFloat(X, offset)).print(out, dec_digits) for X with
+        little-endian u64 ``limbs``: ((in_digits, in_point_pos), text)."""
+        leaves = _limbs(limbs)
+        in_cap = (leaves.size * 64) // 28 + 8
+        cap = int(in_cap * 9 + abs(int(offset)) * 0.31 + int(dec_digits)) + 64
+        din = np.zeros(in_cap, dtype=np.uint32)
+        out = C.create_string_buffer(cap)
+        nin, nout, ppin = C.c_size_t(0), C.c_size_t(0), C.c_int64(0)
+        rc = self.lib.ref_bigfloat_print(_p64(leaves), leaves.size, int(offset), int(bool(neg)), int(dec_digits),
+                                         _p32(din), in_cap, C.byref(nin), C.byref(ppin), out, cap, C.byref(nout))
+        if rc != 0:
+            raise OracleError(f"ref_bigfloat_print returned {rc}")
+        return (din[: nin.value].copy(), int(ppin.value)), out.raw[: nout.value].decode()
 
     def to_dec_string(self, limbs) -> str:
         """Decimal text of the integer with little-endian u64 ``limbs``

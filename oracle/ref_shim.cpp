@@ -18,6 +18,7 @@
 //   ref_to_dec_string -> BigInt::print (decimal)  src/bigint.cpp:175-247
 //   ref_from_dec_string -> BigInt(std::string)     src/bigint.cpp:25-124
 //   ref_divmod      -> BigInt::divmod             src/bigint.cpp:625-673
+//   ref_bigfloat_print -> BigFloat::print          src/bigint.cpp:972-1041
 //   ref_init_thread_pool -> bigint::init_thread_pool (ntt_multithread.cpp:407)
 // Results are copied into caller buffers; return 0 on success, -1 when the
 // caller's buffer is too small (out_len then holds the needed size).
@@ -219,6 +220,31 @@ int ref_divmod(const uint64_t* a, size_t na, int a_neg, const uint64_t* b, size_
     const int rq = copy_out32(Q.get_data(), q, q_cap, q_len);
     const int rr = copy_out32(R.get_data(), r, r_cap, r_len);
     return rq != 0 || rr != 0 ? -1 : 0;
+}
+
+// BigFloat::print(out, dec_digits) (src/bigint.cpp:972-1041) of
+// +-BigFloat(X, offset) (X * 2^offset, tail zeros removed; X by its
+// little-endian u64 limbs through the hex-string constructor).  Returns the
+// input BigFloat's digits and point position as well, and the text.
+int ref_bigfloat_print(const uint64_t* limbs, size_t n, int64_t offset, int neg, size_t dec_digits,
+                       uint32_t* in_out, size_t in_cap, size_t* in_len, int64_t* in_point_pos, char* out,
+                       size_t cap, size_t* out_len) {
+    static const char hexd[] = "0123456789abcdef";
+    std::string hex;
+    hex.reserve(16 * n);
+    for (size_t i = n; i-- > 0;)
+        for (int k = 15; k >= 0; --k) hex.push_back(hexd[(limbs[i] >> (4 * k)) & 15]);
+    bigint::BigFloat v(bigint::BigInt(hex, true), offset);
+    if (neg) v = -v;
+    *in_point_pos = v.get_point_pos();
+    if (copy_out32(v.get_data(), in_out, in_cap, in_len) != 0) return -1;
+    std::ostringstream os;
+    v.print(os, dec_digits);
+    const std::string s = os.str();
+    *out_len = s.size();
+    if (s.size() > cap) return -1;
+    std::memcpy(out, s.data(), s.size());
+    return 0;
 }
 
 // fast_pow over BigInt, as the reference's benchmark example calls it

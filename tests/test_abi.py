@@ -38,7 +38,8 @@ def test_header_declares_entry_points():
     names = declared_functions()
     for must in ("bgpu_init", "bgpu_shutdown", "bgpu_strerror", "bgpu_mul_u64", "bgpu_mul_digits",
                  "bgpu_mul_u64_device", "bgpu_device_status", "bgpu_mul_u64_many", "bgpu_pow_u64",
-                 "bgpu_reciprocal_digits", "bgpu_from_decimal", "bgpu_to_decimal", "bgpu_divmod_digits"):
+                 "bgpu_reciprocal_digits", "bgpu_from_decimal", "bgpu_to_decimal", "bgpu_divmod_digits",
+                 "bgpu_bigfloat_to_decimal"):
         assert must in names
 
 
@@ -94,6 +95,7 @@ def test_calls_before_init_report_not_initialized(lib):
     n2, neg2 = C.c_size_t(0), C.c_int(0)
     assert lib.bgpu_divmod_digits(pd, 4, 0, pd, 2, 0, 0, 1, pd, 4, C.byref(n), C.byref(neg), pd, 4,
                                   C.byref(n2), C.byref(neg2)) == -8
+    assert lib.bgpu_bigfloat_to_decimal(pd, 4, 0, 0, 0, buf, 16, C.byref(n)) == -8
 
 
 def test_new_entry_points_reject_bad_arguments_on_host(lib):
@@ -120,3 +122,6 @@ def test_new_entry_points_reject_bad_arguments_on_host(lib):
     assert divmod_rc(mode=256) == -1
     assert divmod_rc(qlen=None) == -1
     assert divmod_rc(rlen=None) == -1
+    assert lib.bgpu_bigfloat_to_decimal(None, 4, 0, 0, 0, buf, 16, C.byref(n)) == -1
+    assert lib.bgpu_bigfloat_to_decimal(pd, 0, 0, 0, 0, buf, 16, C.byref(n)) == -1
+    assert lib.bgpu_bigfloat_to_decimal(pd, 4, 0, 0, 0, buf, 16, None) == -1
