@@ -62,9 +62,9 @@ def test_concurrent_host_threads(bb, port):
 
 def test_concurrent_mixed_entry_points(bb, port):
     """Threads calling different entry points at once (u64 and Digits
-    products through the staged host copies, the reciprocal, decimal parse and
-    print, fast_pow) share the engine's buffers; each result must equal the
-    same call made alone."""
+    products through the staged host copies, the reciprocal, divmod, decimal
+    parse and print, BigFloat print, fast_pow) share the engine's buffers; each
+    result must equal the same call made alone."""
     import threading
 
     rng = np.random.default_rng(SEED + 82)
@@ -72,6 +72,9 @@ def test_concurrent_mixed_entry_points(bb, port):
     d = rng.integers(0, 1 << 28, 150000, dtype=np.uint32)
     d[-1] |= 1
     text = "".join(map(str, rng.integers(0, 10, 60000)))
+    na, nb, nf = d[:60000].copy(), d[:25000].copy(), d[:30000].copy()
+    for x in (na, nb, nf):
+        x[-1] |= 1  # no leading zero digit
     calls = [
         lambda: bb.mul(a, b),
         lambda: bb.mul_digits(d, d[:70000].copy()),
@@ -79,6 +82,8 @@ def test_concurrent_mixed_entry_points(bb, port):
         lambda: bb.from_decimal(text)[0],
         lambda: bb.to_decimal(d[:40000]),
         lambda: bb.fast_pow(7, 1000003),
+        lambda: np.concatenate([x for (x, _) in bb.divmod_digits(na, nb, True, False, 1)]),
+        lambda: bb.bigfloat_to_decimal(nf, 12000, False, 0),
     ]
     alone = [c() for c in calls]
     got = [[None] * len(calls) for _ in range(3)]
