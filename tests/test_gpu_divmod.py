@@ -179,3 +179,38 @@ def test_large_identity(bb):
     assert not qn and not rn
     assert (mod_m61(q) * mod_m61(b) + mod_m61(r)) % M61 == mod_m61(a)
     assert r.size < b.size or (r.size == b.size and r[::-1].tolist() < b[::-1].tolist())
+
+
+def test_small_output_buffers_report_the_lengths_needed(bb):
+    """BGPU_ERR_OUT_CAPACITY with *q_len and *r_len set, then a call with
+    those capacities succeeds."""
+    import ctypes as C
+
+    rng = np.random.default_rng(SEED + 807)
+    a, b = rand_int_digits(rng, 300), rand_int_digits(rng, 120)
+    (wq, _), (wr, _) = bb.divmod_digits(a, b)
+    u32p = C.POINTER(C.c_uint32)
+    q, r = np.zeros(4, np.uint32), np.zeros(4, np.uint32)
+    nq, nr, qn, rn = C.c_size_t(0), C.c_size_t(0), C.c_int(0), C.c_int(0)
+    rc = bb.lib.bgpu_divmod_digits(a.ctypes.data_as(u32p), a.size, 0, b.ctypes.data_as(u32p), b.size, 0, 0, 1,
+                                   q.ctypes.data_as(u32p), q.size, C.byref(nq), C.byref(qn),
+                                   r.ctypes.data_as(u32p), r.size, C.byref(nr), C.byref(rn))
+    assert rc == -5 and nq.value == wq.size and nr.value == wr.size
+    q, r = np.zeros(nq.value, np.uint32), np.zeros(nr.value, np.uint32)
+    rc = bb.lib.bgpu_divmod_digits(a.ctypes.data_as(u32p), a.size, 0, b.ctypes.data_as(u32p), b.size, 0, 0, 1,
+                                   q.ctypes.data_as(u32p), q.size, C.byref(nq), C.byref(qn),
+                                   r.ctypes.data_as(u32p), r.size, C.byref(nr), C.byref(rn))
+    assert rc == 0 and np.array_equal(q, wq) and np.array_equal(r, wr)
+    text = bb.bigfloat_to_decimal(a, 100, True, 30)
+    buf, n = C.create_string_buffer(8), C.c_size_t(0)
+    rc = bb.lib.bgpu_bigfloat_to_decimal(a.ctypes.data_as(u32p), a.size, 100, 1, 30, buf, 8, C.byref(n))
+    assert rc == -5 and n.value == len(text)
+
+
+def test_invalid_digits_are_rejected(bb):
+    with pytest.raises(bb.BigIntGPUError):
+        bb.divmod_digits(np.array([1 << 28], np.uint32), np.array([3], np.uint32))
+    with pytest.raises(bb.BigIntGPUError):
+        bb.divmod_digits(np.array([5, 0], np.uint32), np.array([3], np.uint32))  # a leading zero digit
+    with pytest.raises(bb.BigIntGPUError):
+        bb.bigfloat_to_decimal(np.array([3, 0], np.uint32), 1)
