@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kAddThreads) k_seg_divstep(const uint64_t* cur
 __global__ void k_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nseg, char* out) {
     const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nseg) return;
-    uint32_t x[2 * kLeafLimbs];
+    uint32_t x[2 * kPrintLeafLimbs];
     const uint32_t nw = 2 * w;
     for (uint32_t i = 0; i < w; ++i) {
         const uint64_t v = in[p * w + i];
@@ -294,6 +294,7 @@ cudaError_t launch_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t, ui
 }
 
 cudaError_t launch_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nseg, char* out, cudaStream_t st) {
+    if (w > kPrintLeafLimbs) return cudaErrorInvalidValue;
     k_dec_print_leaves<<<(uint32_t)((nseg + 63) / 64), 64, 0, st>>>(in, w, nseg, out);
     return cudaGetLastError();
 }

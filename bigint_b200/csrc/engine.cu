@@ -1971,7 +1971,8 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
 // device.  The reciprocals are a chain: V_k^2 is at most V_(k+1) (both are
 // floors of the same real, squared), one Newton step from below brings it
 // within a few units, and single correction steps make it exact.  Leaves of
-// 128 limbs print 2432 characters per thread.
+// kPrintLeafLimbs limbs print 19 * kPrintLeafLimbs characters per thread.
+
 // Decimal text (no sign, no leading zeros) of the integer whose Digits are n
 // digits at hsrc (host) or dsrc (device), the top one `top` (nonzero), above
 // `low` zero digits: h[first..) on return.
@@ -1990,7 +1991,7 @@ static int dec_chars(const uint32_t* hsrc, const uint32_t* dsrc, size_t low, siz
     const int J = ceil_log2((dmax + 18) / 19);
     if (J > 25) return BGPU_ERR_CAPACITY;
     const uint64_t NL = (uint64_t)1 << J;
-    const uint32_t w0 = (uint32_t)std::min<uint64_t>(128, NL);
+    const uint32_t w0 = (uint32_t)std::min<uint64_t>(kPrintLeafLimbs, NL);  // limbs per printed leaf
     int jleaf = 0;
     while ((1u << jleaf) < w0) ++jleaf;
     auto mk = pow_mk;
