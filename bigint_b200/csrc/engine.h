@@ -258,7 +258,7 @@ cudaError_t launch_shift_digits(const uint32_t* v, uint32_t n, uint32_t s, bool 
 constexpr uint64_t kHugeBlockLimbs = (uint64_t)1 << 24;
 // Limbs per leaf of the decimal printer: one thread prints a leaf by repeated
 // division by 10^9, its work growing with the square of the leaf.
-constexpr uint32_t kPrintLeafLimbs = 64;
+constexpr uint32_t kPrintLeafLimbs = 32;
 uint32_t accumulate_blocks(uint64_t L);
 cudaError_t launch_accumulate(uint64_t* out, uint64_t L, const uint64_t* add, uint64_t nadd, uint32_t* agg,
                               uint32_t* cin, cudaStream_t st);

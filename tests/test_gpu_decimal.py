@@ -104,10 +104,10 @@ def test_print_small_and_edges(bb, ref):
 
 
 def test_print_sizes_across_levels(bb, ref):
-    """Values whose decimal length crosses the printed leaves (1216 digits)
+    """Values whose decimal length crosses the printed leaves (608 digits)
     and each division level."""
     rng = np.random.default_rng(SEED + 610)
-    for decimal_len in [100, 1215, 1216, 1217, 2431, 2432, 2433, 4865, 9729, 20000, 77824, 77825, 155649,
+    for decimal_len in [100, 607, 608, 609, 1215, 1216, 1217, 2431, 2432, 2433, 4865, 9729, 20000, 77824, 77825, 155649,
                         400000]:
         nd = int(decimal_len / 0.30103 / 28) + 1
         d = rng.integers(0, 1 << 28, nd, dtype=np.uint32)
