@@ -6,7 +6,7 @@
 //   segment_{j+1}[p] = segment_j[2p+1] * 10^(19 * 2^j) + segment_j[2p].
 // A level-j segment is below 10^(19 * 2^j) < 2^(64 * 2^j), so it fits in
 // 2^j limbs and every level is one array of the same 2^J limbs.  The first
-// levels (segments of up to 128 limbs, 2432 digits) are built in one kernel
+// levels (segments of up to kParseLeafLimbs = 32 limbs, 608 digits) are built in one kernel
 // by Horner's rule per segment; each later level is one batch of equal-size
 // products (the engine's batch plans) and one segmented carry add of the low
 // halves.
@@ -20,19 +20,18 @@ namespace bgpu {
 namespace {
 
 constexpr uint64_t kTen19 = 10000000000000000000ull;
-constexpr uint32_t kLeafLimbs = 128;  // limbs per segment built by Horner's rule
 constexpr int kAddThreads = 256;
 constexpr int kAddPer = 8;
 constexpr uint32_t kAddTile = kAddThreads * kAddPer;
 
-// Segment s (w limbs, w <= kLeafLimbs) from decimal positions
+// Segment s (w limbs, w <= kParseLeafLimbs) from decimal positions
 // [19 w s, 19 w (s+1)) counted from the least significant digit of dig[0..D)
 // (most significant first, values 0..9), by Horner's rule over its w groups
 // of 19 digits.
 __global__ void k_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64_t nseg, uint64_t* out) {
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nseg) return;
-    uint64_t v[kLeafLimbs];
+    uint64_t v[kParseLeafLimbs];
     for (uint32_t i = 0; i < w; ++i) v[i] = 0;
     for (int g = (int)w - 1; g >= 0; --g) {
         // the 19 digits of group g, most significant first
@@ -301,6 +300,7 @@ cudaError_t launch_dec_print_leaves(const uint64_t* in, uint32_t w, uint64_t nse
 
 cudaError_t launch_dec_leaves(const uint8_t* dig, uint64_t D, uint32_t w, uint64_t nseg, uint64_t* out,
                               cudaStream_t st) {
+    if (w > kParseLeafLimbs) return cudaErrorInvalidValue;
     k_dec_leaves<<<(uint32_t)((nseg + 127) / 128), 128, 0, st>>>(dig, D, w, nseg, out);
     return cudaGetLastError();
 }

@@ -1898,7 +1898,7 @@ static int from_decimal_locked(const char* s, size_t len, uint32_t* out, size_t 
     const int J = ceil_log2(leaves);
     if (J > 25) return BGPU_ERR_CAPACITY;  // the top level's product is the largest general transform
     const uint64_t NL = (uint64_t)1 << J;  // limbs of every level
-    const uint32_t w0 = (uint32_t)std::min<uint64_t>(128, NL);  // segments built per thread (decimal.cu)
+    const uint32_t w0 = (uint32_t)std::min<uint64_t>(kParseLeafLimbs, NL);  // limbs of a leaf built per thread
     int j0 = 0;
     while ((1u << j0) < w0) ++j0;
     const uint64_t nd = (64 * NL + 27) / 28;  // Digits of the result, before stripping

@@ -259,6 +259,9 @@ constexpr uint64_t kHugeBlockLimbs = (uint64_t)1 << 24;
 // Limbs per leaf of the decimal printer: one thread prints a leaf by repeated
 // division by 10^9, its work growing with the square of the leaf.
 constexpr uint32_t kPrintLeafLimbs = 32;
+// Limbs per leaf of the decimal parser: one thread builds a leaf from its
+// decimal digits by Horner's rule, its work growing with the square of the leaf.
+constexpr uint32_t kParseLeafLimbs = 32;
 uint32_t accumulate_blocks(uint64_t L);
 cudaError_t launch_accumulate(uint64_t* out, uint64_t L, const uint64_t* add, uint64_t nadd, uint32_t* agg,
                               uint32_t* cin, cudaStream_t st);

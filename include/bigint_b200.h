@@ -141,7 +141,7 @@ int bgpu_pow_u64(const uint64_t* base, size_t nbase, uint32_t exponent, uint64_t
  * text ('-' for a negative nonzero value, no leading zeros, "0" for zero),
  * identical to the reference's, not NUL-terminated.  The conversion runs on
  * the GPU: halves by 10^(19 * 2^k) top down, with exact reciprocals and
- * batched products, and leaves of 2432 digits.  BGPU_ERR_OUT_CAPACITY when
+ * batched products, and leaves of 608 digits.  BGPU_ERR_OUT_CAPACITY when
  * out_cap is too small (*out_len = needed). */
 int bgpu_to_decimal(const uint32_t* digits, size_t n, int is_neg, char* out, size_t out_cap, size_t* out_len);
 
