@@ -23,6 +23,8 @@ constexpr uint64_t kTen19 = 10000000000000000000ull;
 constexpr int kAddThreads = 256;
 constexpr int kAddPer = 8;
 constexpr uint32_t kAddTile = kAddThreads * kAddPer;
+constexpr int kWideAddThreads = 1024;
+constexpr uint32_t kWideDivstepLimbs = 4096;  // w at which a level's divide step uses 1024-thread blocks
 
 // Segment s (w limbs, w <= kParseLeafLimbs) from decimal positions
 // [19 w s, 19 w (s+1)) counted from the least significant digit of dig[0..D)
@@ -134,10 +136,12 @@ __global__ void __launch_bounds__(kAddThreads) k_seg_add_low(uint64_t* out, cons
 // once more and adds 1 to q.
 
 // Block-wide sum or difference of two limb runs with the carry (or borrow)
-// carried across tiles; out may alias x.  Returns the carry out.
+// carried across tiles of T * kAddPer limbs (T = the block's threads); out
+// may alias x.  Returns the carry out.
+template <int T>
 __device__ uint32_t block_addsub(uint64_t* out, const uint64_t* x, uint32_t nx, const uint64_t* y, uint32_t ny,
                                  uint32_t n, bool sub, uint32_t cin) {
-    for (uint32_t t0 = 0; t0 < n; t0 += kAddTile) {
+    for (uint32_t t0 = 0; t0 < n; t0 += (uint32_t)T * kAddPer) {
         const uint32_t j0 = t0 + threadIdx.x * kAddPer;
         uint64_t a[kAddPer], b[kAddPer];
         uint32_t st = 2u;
@@ -201,19 +205,19 @@ __device__ bool block_geq(const uint64_t* x, uint32_t nx, const uint64_t* y, uin
 // Segment p of the level above (2w limbs at cur + 2 w p) with U_p = q * Q
 // (2w limbs at u + 2 w p) and q (w limbs at t + (2w + m) p + 2w) written as
 // the two halves of the level below: next[2 w p ..] = r, next[2 w p + w ..] = q.
-__global__ void __launch_bounds__(kAddThreads) k_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t,
-                                                             uint32_t tstride, const uint64_t* q_pow, uint32_t w,
-                                                             uint64_t* next) {
+template <int T>
+__global__ void __launch_bounds__(T) k_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t, uint32_t tstride,
+                                                   const uint64_t* q_pow, uint32_t w, uint64_t* next) {
     const uint64_t p = blockIdx.x;
     const uint64_t* s = cur + 2 * (uint64_t)w * p;
     uint64_t* r = u + 2 * (uint64_t)w * p;
     uint64_t* q = t + (uint64_t)tstride * p + 2 * w;
-    block_addsub(r, s, 2 * w, r, 2 * w, 2 * w, true, 0);  // r = s - q Q, in place of U
+    block_addsub<T>(r, s, 2 * w, r, 2 * w, 2 * w, true, 0);  // r = s - q Q, in place of U
     __syncthreads();
     if (block_geq(r, 2 * w, q_pow, w)) {  // q was one short
-        block_addsub(r, r, 2 * w, q_pow, w, 2 * w, true, 0);
+        block_addsub<T>(r, r, 2 * w, q_pow, w, 2 * w, true, 0);
         __syncthreads();
-        block_addsub(q, q, w, nullptr, 0, w, false, 1);
+        block_addsub<T>(q, q, w, nullptr, 0, w, false, 1);
         __syncthreads();
     }
     uint64_t* lo = next + 2 * (uint64_t)w * p;
@@ -266,9 +270,9 @@ __global__ void __launch_bounds__(kAddThreads) k_fix_step(uint64_t* r, uint32_t 
                                                           uint64_t* v, uint32_t nv, uint32_t* flag) {
     const bool ge = block_geq(r, nr, q, nq);
     if (ge) {
-        block_addsub(r, r, nr, q, nq, nr, true, 0);
+        block_addsub<kAddThreads>(r, r, nr, q, nq, nr, true, 0);
         __syncthreads();
-        block_addsub(v, v, nv, nullptr, 0, nv, false, 1);
+        block_addsub<kAddThreads>(v, v, nv, nullptr, 0, nv, false, 1);
     }
     if (threadIdx.x == 0) *flag = ge ? 1u : 0u;
 }
@@ -288,7 +292,12 @@ cudaError_t launch_fix_step(uint64_t* r, uint32_t nr, const uint64_t* q, uint32_
 
 cudaError_t launch_seg_divstep(const uint64_t* cur, uint64_t* u, uint64_t* t, uint32_t tstride, const uint64_t* q_pow,
                                uint32_t w, uint64_t nseg, uint64_t* next, cudaStream_t st) {
-    k_seg_divstep<<<(uint32_t)nseg, kAddThreads, 0, st>>>(cur, u, t, tstride, q_pow, w, next);
+    // long segments (the top levels: few of them, one block each) walk their
+    // limbs in 4x wider tiles
+    if (w >= kWideDivstepLimbs)
+        k_seg_divstep<kWideAddThreads><<<(uint32_t)nseg, kWideAddThreads, 0, st>>>(cur, u, t, tstride, q_pow, w, next);
+    else
+        k_seg_divstep<kAddThreads><<<(uint32_t)nseg, kAddThreads, 0, st>>>(cur, u, t, tstride, q_pow, w, next);
     return cudaGetLastError();
 }
 
