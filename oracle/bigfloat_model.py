@@ -16,10 +16,15 @@ replay the reference's BigFloat::reciprocal (src/bigint.cpp:1044-1071):
 * ``divmod`` -- BigInt::divmod (src/bigint.cpp:625-673) as the engine replays
   it for ``bgpu_divmod_digits``: the estimate through ``reciprocal`` and
   ``mul_trunc``, its rounding to an integer (BigInt(const BigFloat&, mode),
-  src/bigint.cpp:1072-1172), R = a - Q * b and the single adjustment.
+  src/bigint.cpp:1072-1172), R = a - Q * b and the single adjustment;
+* ``bigfloat_print`` -- BigFloat::print (src/bigint.cpp:972-1041) as the engine
+  replays it for ``bgpu_bigfloat_to_decimal``: the fraction times 5^d, the
+  shift by d - 28 pp, the rounding half up and the carry into the integer
+  part.
 
 tests/test_oracle_bigfloat.py pins this model against the reference's own
-reciprocal; the GPU tests pin the device against the reference.  Only the
+reciprocal, divmod and print; the GPU tests pin the device against the
+reference.  Only the
 tests import this module.
 """
 from __future__ import annotations
@@ -234,3 +239,51 @@ def divmod(a, a_neg: bool, b, b_neg: bool, mode: int, check: bool = True):
             else:
                 r, q = r - bv, q + 1
     return q, r
+
+
+def _round_half_up_to_int(p: Val) -> int:
+    """BigInt(const BigFloat&, RoundHalfUp) of a Val whose bottom digit is
+    nonzero, as the device computes it; zero where the reference's rounding
+    leaves no digit."""
+    if p.zero() or p.pp > len(p.d):
+        return 0
+    if p.pp <= 0:
+        return _signed(p)
+    k = p.pp
+    mag = (_int(p.d[k:]) if k < len(p.d) else 0) + (p.d[k - 1] >> 27)
+    return -mag if p.neg else mag
+
+
+def bigfloat_print(digits, pp: int, neg: bool, dec_digits: int = 0) -> str:
+    """The text of BigFloat::print(out, dec_digits) for a BigFloat's fields."""
+    import math
+    import sys
+
+    d = [int(x) for x in digits]
+    n = len(d)
+    int_part = (_int(d[max(pp, 0):]) << (28 * max(-pp, 0))) if pp < n else 0
+    fsize = min(pp, n) if pp > 0 else 0
+    if dec_digits == 0:
+        dec_digits = math.floor(float(fsize * 28) * math.log10(2))
+    frac = _int(d[:fsize])
+    f = 0
+    if dec_digits and frac:
+        x = frac * 5 ** dec_digits
+        xd = _digits(x, (x.bit_length() + 27) // 28)
+        t = 0
+        while xd[t] == 0:
+            t += 1
+        s = shift(Val(xd[t:], -t, False), dec_digits - 28 * pp)
+        t = s.tz()
+        f = _round_half_up_to_int(Val(s.d[t:], s.pp - t, False))
+        if f == 10 ** dec_digits:
+            f, int_part = 0, int_part + 1
+    old = sys.get_int_max_str_digits()
+    sys.set_int_max_str_digits(0)
+    try:
+        text = ("-" if neg else "") + str(int_part) + "."
+        if dec_digits:
+            text += str(f).rjust(dec_digits, "0")
+    finally:
+        sys.set_int_max_str_digits(old)
+    return text
