@@ -105,3 +105,28 @@ def test_reduce_max_over_two_gloo_ranks():
         assert p.exitcode == 0
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert got == [(0, 11.0), (1, 11.0)]
+
+
+def test_every_form_is_run_alone_and_in_the_default_run():
+    """Each name in bench.FORMS is dispatched by --form and appears in the
+    default run's "forms" object."""
+    import inspect
+
+    single = inspect.getsource(bench.run_single_form)
+    default = inspect.getsource(bench.run_gpu_arm)
+    missing = [name for name in bench.FORMS if f'"{name}"' not in single]
+    assert missing in ([], [bench.FORMS[-1]])  # the last form is the dispatcher's final else
+    for name in bench.FORMS:
+        assert f'"{name}":' in default, name
+
+
+def test_limb_digit_converters_round_trip():
+    rng = np.random.default_rng(11)
+    for n in (1, 2, 7, 64, 1001):
+        limbs = rng.integers(0, 2**64, n, dtype=np.uint64)
+        limbs[-1] |= np.uint64(1)
+        d = bench.limbs_to_digits28_np(limbs)
+        assert d.dtype == np.uint32 and int(d.max()) < (1 << 28) and d[-1] != 0
+        assert sum(int(x) << (28 * i) for i, x in enumerate(d)) == int.from_bytes(limbs.tobytes(), "little")
+        back = bench.digits28_to_limbs_np(d)
+        assert np.array_equal(back[: n], limbs) and not back[n:].any()
