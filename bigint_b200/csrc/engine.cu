@@ -1590,6 +1590,7 @@ int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, 
                            int64_t* out_point_pos, int* out_is_neg) {
     if (!digits || n == 0 || !out_len || !out_point_pos || !out_is_neg || (!out && out_cap))
         return BGPU_ERR_INVALID_ARG;
+    if (point_pos > BGPU_MAX_POINT_POS || point_pos < -BGPU_MAX_POINT_POS) return BGPU_ERR_CAPACITY;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);
@@ -2225,6 +2226,8 @@ static int bigfloat_print_steps(const uint32_t* digits, size_t n, int64_t pp, bo
 int bgpu_bigfloat_to_decimal(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
                              size_t dec_digits, char* out, size_t out_cap, size_t* out_len) {
     if (!digits || n == 0 || !out_len || (!out && out_cap)) return BGPU_ERR_INVALID_ARG;
+    // 28 * point_pos and the shift d - 28 * point_pos stay far inside int64
+    if (point_pos > BGPU_MAX_POINT_POS || point_pos < -BGPU_MAX_POINT_POS) return BGPU_ERR_CAPACITY;
     std::lock_guard<std::mutex> lk(g_mu);
     if (g.device < 0) return BGPU_ERR_NOT_INIT;
     cudaSetDevice(g.device);

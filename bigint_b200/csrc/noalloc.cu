@@ -21,8 +21,10 @@
 //   * every call shares the one scratch array, which keeps the last call's
 //     contents; the carry-scan ticket, flags and error word are cleared on the
 //     caller's stream at the start of each call, the rest is fully rewritten.
-//     Calls whose work overlaps on the GPU (two streams, two host threads)
-//     race on the array and must be serialized by the caller.
+//     Calls within one process are serialized per device: a host mutex is
+//     held until the call's work has finished, so their work cannot overlap
+//     on the GPU (work that did overlap would race on the array).  Each
+//     process has its own copy of the array.
 //   * the first call on each device performs the set-up (table upload and
 //     cudaGetSymbolAddress, synchronous); make that first call before any
 //     stream capture.
@@ -72,7 +74,7 @@ struct DeviceSetup {
 
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
-std::mutex g_na_mu;
+std::mutex g_na_mu[kMaxDevices];  // one per device: its set-up and its use of the scratch
 
 // Once per device, with that device current: upload the tables and take the
 // device addresses of the static arrays.  In host code the array names are
@@ -107,7 +109,7 @@ extern "C" int bgpu_mul_u64_device_noalloc(const uint64_t* d_a, size_t na, const
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return BGPU_ERR_NO_DEVICE;
-    std::lock_guard<std::mutex> lk(g_na_mu);
+    std::lock_guard<std::mutex> lk(g_na_mu[dev]);
     DeviceSetup& s = g_setup[dev];
     if (!s.ready) {
         const int rc = setup_device(dev, &s);
@@ -146,12 +148,18 @@ extern "C" int bgpu_mul_u64_device_noalloc(const uint64_t* d_a, size_t na, const
     if (shape.log_n1 > kNaStageLog || shape.log_n2 > kNaStageLog) return BGPU_ERR_CAPACITY;
     cudaError_t e = launch_ntt_product(kSlotNoAlloc + kNaSet, s.consts, oa, ob, square, log_n, ps,
                                        d_out, kFmtLimb64, na + nb, cl, st, nullptr, &shape);
-    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? BGPU_ERR_OOM : BGPU_ERR_CUDA;
+    if (e != cudaSuccess) {
+        // Kernels queued before the failing launch still write the scratch:
+        // let them finish before the lock goes, so the next call's clearing
+        // of the carry-scan state cannot race them.
+        cudaStreamSynchronize(st);
+        return e == cudaErrorMemoryAllocation ? BGPU_ERR_OOM : BGPU_ERR_CUDA;
+    }
     // Synchronous completion: wait for the product and report a bounded
     // device-side wait that gave up (the error word is part of the scratch).
     uint32_t err = 0;
     e = cudaMemcpyAsync(&err, ps.err, sizeof(err), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return BGPU_ERR_CUDA;
+    const cudaError_t es = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || es != cudaSuccess) return BGPU_ERR_CUDA;
     return err ? BGPU_ERR_DEVICE_TIMEOUT : BGPU_OK;
 }

@@ -61,6 +61,9 @@ extern "C" {
 #define BGPU_SCHOOLBOOK_MAX_LIMBS 256u
 #define BGPU_KARATSUBA_MAX_LIMBS 256u
 #define BGPU_MAX_LOG2_POINTS 26u  /* transform points are 32-bit digits */
+/* Largest |point_pos| the BigFloat entry points take (BGPU_ERR_CAPACITY
+ * above): 28 * point_pos then stays far inside int64_t. */
+#define BGPU_MAX_POINT_POS ((int64_t)1 << 40)
 
 typedef struct bgpu_stats {
     int32_t method;          /* BGPU_METHOD_* actually used */
@@ -167,6 +170,7 @@ int bgpu_from_decimal(const char* s, size_t len, uint32_t* out, size_t out_cap, 
  * in the reference.  Writes the reciprocal's Digits, point position and sign,
  * identical to the reference's result.  Division by zero (the reference
  * throws std::domain_error) and digits >= 2^28 give BGPU_ERR_INVALID_ARG;
+ * |point_pos| > BGPU_MAX_POINT_POS gives BGPU_ERR_CAPACITY;
  * BGPU_ERR_OUT_CAPACITY when out_cap is too small (*out_len = needed). */
 int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
                            size_t precision, uint32_t* out, size_t out_cap, size_t* out_len,
@@ -181,8 +185,9 @@ int bgpu_reciprocal_digits(const uint32_t* digits, size_t n, int64_t point_pos, 
  * when d is 0), identical to the reference's text, not NUL-terminated.  5^d,
  * the product, the shift, the rounding and both decimal conversions run on
  * the GPU.  Where the reference's rounding is undefined (2^-28 <= f * 10^d <
- * 1/2) the fraction prints as zeros.  BGPU_ERR_OUT_CAPACITY when out_cap is
- * too small (*out_len = needed). */
+ * 1/2) the fraction prints as zeros.  |point_pos| > BGPU_MAX_POINT_POS gives
+ * BGPU_ERR_CAPACITY; BGPU_ERR_OUT_CAPACITY when out_cap is too small
+ * (*out_len = needed). */
 int bgpu_bigfloat_to_decimal(const uint32_t* digits, size_t n, int64_t point_pos, int is_neg,
                              size_t dec_digits, char* out, size_t out_cap, size_t* out_len);
 
@@ -337,12 +342,14 @@ int bgpu_load_tuning(const char* path);
  *    nothing is launched.
  *  - the first call on each device does the set-up (table upload and the
  *    static array's address, synchronous): make it before any stream capture.
- *  - the work is queued on `stream` (0 = legacy default stream) and the call
- *    returns after it completes, with BGPU_ERR_DEVICE_TIMEOUT if the carry
- *    scan's bounded wait gave up.
+ *  - the call is synchronous: the work is queued on `stream` (0 = legacy
+ *    default stream) and the call returns after it completes, with
+ *    BGPU_ERR_DEVICE_TIMEOUT if the carry scan's bounded wait gave up.
  *  - every call shares the static array (it keeps the last call's contents;
- *    the carry-scan state is cleared at the start of each call): calls that
- *    overlap on the GPU race and must be serialized by the caller. */
+ *    the carry-scan state is cleared at the start of each call).  Calls in one
+ *    process are serialized per device by a host lock held until their work
+ *    has finished; work that still overlapped on the GPU would race on the
+ *    array. */
 int bgpu_mul_u64_device_noalloc(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
                                 uint64_t* d_out, void* stream);
 

@@ -10,9 +10,12 @@ Two shared libraries come out of here:
   need on Linux (no source is copied or edited).  ``-flto`` from the
   reference's CMake release flags is left out: the LTO plugin cannot run here.
 
-Usage: ``python oracle/build.py [port|ref|all]`` (default ``all``).  The
-reference tree is only needed for ``ref``; when it is absent that step is
-skipped and an existing ``oracle/_ref`` build is kept.
+Usage: ``python oracle/build.py [port|ref|ref_gpu|all]`` (default ``all``).
+The reference tree is only needed for ``ref`` and ``ref_gpu``: its root comes
+from the ``BIGINT_REF_ROOT`` environment variable (or the ``ref_root``
+argument of the build functions).  With no root given those two steps stop
+with an error; with a root that holds no sources they are skipped and an
+existing ``oracle/_ref`` build is kept.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("BIGINT_REF_ROOT", "/root/reference")
+REF_ROOT_ENV = "BIGINT_REF_ROOT"
 REF_SOURCES = [
     "src/mul/ntt_multithread.cpp",
     "src/mul/fft.cpp",
@@ -52,7 +55,17 @@ def build_port(force: bool = False) -> str:
     return PORT_SO
 
 
-def build_ref(force: bool = False) -> str | None:
+def ref_root(given: str | None = None) -> str:
+    """The reference checkout to compile: `given`, else $BIGINT_REF_ROOT."""
+    root = given or os.environ.get(REF_ROOT_ENV)
+    if not root:
+        raise RuntimeError(f"oracle/build.py: no reference root; set {REF_ROOT_ENV} to the "
+                           "reference checkout (the directory holding include/ and src/)")
+    return root
+
+
+def build_ref(force: bool = False, ref_root_dir: str | None = None) -> str | None:
+    REF_ROOT = ref_root(ref_root_dir)
     if not os.path.isdir(os.path.join(REF_ROOT, "src")):
         return REF_SO if os.path.exists(REF_SO) else None
     os.makedirs(REF_DIR, exist_ok=True)
@@ -82,10 +95,11 @@ REF_GPU_SO = os.path.join(REF_DIR, "libbigint_ref_gpu.so")
 REF_GPU_SOURCES = ["src/mul/ssa.cpp", "src/bigint.cpp"]
 
 
-def build_ref_gpu(force: bool = False) -> str | None:
+def build_ref_gpu(force: bool = False, ref_root_dir: str | None = None) -> str | None:
     """The unmodified reference BigInt with its multiplies on the GPU engine
     (bigint_b200/hooks/reference_hook.cpp), plus the same C-ABI shim as the
     reference oracle, linked against bigint_b200/libbigint_b200.so."""
+    REF_ROOT = ref_root(ref_root_dir)
     engine = os.path.join(ENGINE_DIR, "libbigint_b200.so")
     if not os.path.isdir(os.path.join(REF_ROOT, "src")) or not os.path.exists(engine):
         return REF_GPU_SO if os.path.exists(REF_GPU_SO) else None

@@ -125,3 +125,17 @@ def test_new_entry_points_reject_bad_arguments_on_host(lib):
     assert lib.bgpu_bigfloat_to_decimal(None, 4, 0, 0, 0, buf, 16, C.byref(n)) == -1
     assert lib.bgpu_bigfloat_to_decimal(pd, 0, 0, 0, 0, buf, 16, C.byref(n)) == -1
     assert lib.bgpu_bigfloat_to_decimal(pd, 4, 0, 0, 0, buf, 16, None) == -1
+
+
+def test_point_positions_beyond_the_bound_rejected_on_host(lib):
+    """|point_pos| above 2^40 would overflow 28 * point_pos: rejected with
+    BGPU_ERR_CAPACITY before any device work (no init needed)."""
+    u32p = C.POINTER(C.c_uint32)
+    d = np.ones(4, dtype=np.uint32)
+    pd = d.ctypes.data_as(u32p)
+    n, pp, neg = C.c_size_t(0), C.c_int64(0), C.c_int(0)
+    buf = C.create_string_buffer(16)
+    for bad in ((1 << 40) + 1, -(1 << 40) - 1, (1 << 62), -(1 << 63)):
+        assert lib.bgpu_bigfloat_to_decimal(pd, 4, bad, 0, 0, buf, 16, C.byref(n)) == -4
+        assert lib.bgpu_reciprocal_digits(pd, 4, bad, 0, 0, pd, 4, C.byref(n), C.byref(pp),
+                                          C.byref(neg)) == -4

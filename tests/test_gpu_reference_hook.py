@@ -1,7 +1,7 @@
 """The reference's own, unmodified BigInt / BigFloat code running its products
 on this engine: the reference built without its CPU NTT and FFT translation
 units and with bigint_b200/hooks/reference_hook.cpp in their place (the
-link-time drop-in of INTEGRATION.md).  Every result is compared with the pure
+link-time drop-in a maintainer of the reference would use).  Every result is compared with the pure
 reference library on the same inputs."""
 from __future__ import annotations
 

@@ -69,12 +69,15 @@ def test_noalloc_square_and_repeat_without_new_device_memory(bb):
     assert noalloc(da.data_ptr(), a.size, da.data_ptr(), a.size, got.data_ptr(), None) == 0
     torch.cuda.synchronize()
     free0, _ = torch.cuda.mem_get_info()
+    torch0 = torch.cuda.memory_allocated()
     for _ in range(2):
         got.fill_(-1)
         assert noalloc(da.data_ptr(), a.size, da.data_ptr(), a.size, got.data_ptr(), None) == 0
         assert torch.equal(got, want)
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
+    # nothing new on the device: neither through torch's allocator nor directly
+    assert torch.cuda.memory_allocated() == torch0
     assert free1 == free0
 
 
