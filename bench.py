@@ -66,10 +66,44 @@ def pairs_beyond_l2(bits: int) -> int:
 
 
 def host_cores() -> int:
+    """Logical CPUs this process may run on."""
     try:
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def physical_cores() -> int:
+    """Physical cores among the CPUs this process may run on (SMT siblings
+    counted once), from the kernel's CPU topology; the logical count when the
+    topology is not readable."""
+    try:
+        cpus = sorted(os.sched_getaffinity(0))
+    except AttributeError:
+        cpus = list(range(os.cpu_count() or 1))
+    cores = set()
+    for c in cpus:
+        base = f"/sys/devices/system/cpu/cpu{c}/topology/"
+        try:
+            pkg = open(base + "physical_package_id").read().strip()
+            core = open(base + "core_id").read().strip()
+        except OSError:
+            return len(cpus)
+        cores.add((pkg, core))
+    return max(1, len(cores))
+
+
+def ref_pool_threads() -> int:
+    """Thread count of the reference's pool inside this process (it is sized
+    once per process): the physical cores, as the reference recommends."""
+    return physical_cores()
+
+
+def cpu_thread_counts() -> list[int]:
+    """Thread counts the reference's CPU multiply is timed at: the physical
+    cores (SMT siblings excluded, as the reference recommends for its pool),
+    8 (the reference's own examples), and every logical CPU."""
+    return sorted({physical_cores(), 8, host_cores()})
 
 
 def workload_name(bits: int) -> str:
@@ -249,9 +283,13 @@ def profiled_traffic(kernel: str) -> float | None:
 
 # ---- CPU baseline ----------------------------------------------------------------
 
-def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int):
+def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int, min_reps: int = 1,
+                       warmup: int = 1):
     """Products/s of the reference CPU multiply (or the C port when the
-    reference library was not built), over a bounded sample."""
+    reference library was not built), over a bounded sample: at least
+    `min_reps` products and then until `seconds` or `max_reps`.  The
+    reference's thread pool is sized once per process, so each thread count
+    runs in a process of its own (`cpu_reference_rates`)."""
     from oracle.pyoracle import Port, Reference, have_reference
 
     if have_reference():
@@ -262,15 +300,43 @@ def cpu_reference_rate(a, b, seconds: float, max_reps: int, threads: int):
         impl, kind, cores = Port(), "port", 1
         fn = impl.ntt_mul
     fn(a[:1024], b[:1024])  # warm the pool
-    fn(a, b)  # and the full-size path: the reference's first large products run slower
+    for _ in range(max(1, warmup)):
+        fn(a, b)  # and the full-size path: the reference's first large products run slower
     reps, t0 = 0, time.perf_counter()
     while True:
         fn(a, b)
         reps += 1
         el = time.perf_counter() - t0
-        if el >= seconds or reps >= max_reps:
+        if reps >= min_reps and (el >= seconds or reps >= max_reps):
             break
     return reps / el, kind, cores, reps, el
+
+
+def cpu_reference_rates(bits: int, seconds: float, max_reps: int, min_reps: int = 1,
+                        warmup: int = 1) -> list[dict]:
+    """`cpu_reference_rate` at every thread count of `cpu_thread_counts()`,
+    each in a fresh process (the reference sizes its pool once per process).
+    The pool's threads are the host's; nothing here touches a GPU."""
+    import subprocess
+
+    out = []
+    for p in cpu_thread_counts():
+        cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", str(p), "--bits", str(bits),
+               "--cpu-seconds", str(seconds), "--cpu-max-reps", str(max_reps),
+               "--cpu-min-reps", str(min_reps), "--warmup", str(max(3, warmup))]
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1200)
+        if r.returncode != 0:
+            raise SystemExit(f"bench: CPU reference worker ({p} threads) failed: {r.stderr[-400:]}")
+        out.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    return out
+
+
+def run_cpu_worker(args) -> None:
+    a, b = make_operands(args.bits)
+    rate, kind, cores, reps, el = cpu_reference_rate(a, b, args.cpu_seconds, args.cpu_max_reps, args.cpu_worker,
+                                                     min_reps=args.cpu_min_reps, warmup=args.warmup)
+    print(json.dumps({"threads": cores, "kind": kind, "rate": rate, "reps": reps, "seconds": el}))
 
 
 # ---- the other configurations, reported beside the headline -----------------------
@@ -327,7 +393,7 @@ def plain_2p20_form(bb, torch, device, port, cpu: bool = True):
 
     if have_reference():
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         for _ in range(3):  # the pool's threads and first-touch pages warm up over the first calls
             want = ref.ntt_mul(a, b)
         if cpu:
@@ -336,7 +402,7 @@ def plain_2p20_form(bb, torch, device, port, cpu: bool = True):
                 t0 = time.perf_counter()
                 ref.ntt_mul(a, b)
                 ts.append(time.perf_counter() - t0)
-            res["cpu_reference"] = {"ms": statistics.median(ts) * 1e3, "threads": host_cores(),
+            res["cpu_reference"] = {"ms": statistics.median(ts) * 1e3, "threads": ref_pool_threads(),
                                     "call": "bigint::mul::ntt::mul (median of 7 after 3 warm-up calls)"}
         res["verified"] = "limb-exact vs the reference's ntt::mul"
     else:
@@ -358,6 +424,12 @@ def sweep_form(bb, torch, device, port):
     M = (1 << 61) - 1
     rng = np.random.default_rng(SEED + 2)
     rows = []
+    from oracle.pyoracle import Reference, have_reference
+
+    ref = None
+    if have_reference():  # products up to 2^27 bits also limb-exact vs ntt::mul (at most ~1 s each)
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
     cases = [(1 << b, 1 << b, "square") for b in range(16, 31, 2)]
     cases += [(1 << 24, 1 << 21, "1:8"), (1 << 20, 1 << 14, "1:64")]
     # beyond the largest transform (2^31 product bits): blocks of 2^30-bit NTT products
@@ -392,12 +464,18 @@ def sweep_form(bb, torch, device, port):
             ok = port.mod_m61(a) * port.mod_m61(b) % M == port.mod_m61(c)
             if not ok:
                 raise SystemExit(f"bench sweep: residue check failed at {abits}x{bbits} {fill}")
+            verified = "residue mod 2^61-1"
+            if ref is not None and abits + bbits <= 1 << 27:
+                want = ref.ntt_mul(a) if kind == "square" else ref.ntt_mul(a, b)
+                if not np.array_equal(np.trim_zeros(c, "b"), want):
+                    raise SystemExit(f"bench sweep: {abits}x{bbits} {fill} differs from the reference's ntt::mul")
+                verified += "; limb-exact vs the reference's ntt::mul"
             model = reference_model_bytes(na, nb)
             rows.append({"a_bits": abits, "b_bits": bbits, "kind": kind, "limbs": fill,
                          "ms": ms, "products_per_s": 1e3 / ms,
                          "log2_points": (2 * na + 2 * nb - 2).bit_length(),
                          "reference_model_frac": model / (ms * 1e-3) / 1e9 / measured_peaks()[0],
-                         "verified": "residue mod 2^61-1"})
+                         "verified": verified})
             del da, db, out
     return rows
 
@@ -463,10 +541,10 @@ def mul_digits_form(bb, port, cpu: bool = True, reps: int = 20):
 
     if cpu and have_reference():
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
         want = ref.mul_digits(a, b)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                 "call": "bigint::mul::mul_digits"}
         if not np.array_equal(got, want):
             raise SystemExit("bench mul_digits: product differs from the reference")
@@ -530,10 +608,10 @@ def fast_pow_form(bb, port, cpu: bool = True):
                                         "fft::mul hooked to bgpu_mul_u64", "identical": same}
     if cpu and have_reference() and Reference().has_fast_pow:
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
         ref.fast_pow_digits(base, e)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                 "call": "bigint::fast_pow<BigInt>"}
     return res
 
@@ -562,10 +640,10 @@ def reciprocal_form(bb, cpu: bool = True, reps: int = 5):
 
     if cpu and have_reference() and Reference().has_bigfloat_reciprocal:
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
         (din, ppin, _), (want, wpp, wneg) = ref.bigfloat_reciprocal(limbs, 0, False, 0)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                 "call": "BigFloat::reciprocal"}
         if not (np.array_equal(din, digits) and ppin == pp_in and np.array_equal(got, want) and pp == wpp
                 and neg == wneg):
@@ -608,10 +686,10 @@ def divmod_form(bb, port, cpu: bool = True, reps: int = 5):
 
     if cpu and have_reference() and Reference().has_divmod:
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
         (wq, wqn), (wr, wrn) = ref.divmod(la, False, lb, False, 0, True)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                 "call": "BigInt::divmod"}
         if not (np.array_equal(q, wq) and qn == wqn and np.array_equal(r, wr) and rn == wrn):
             raise SystemExit("bench divmod: result differs from the reference's")
@@ -653,10 +731,10 @@ def bigfloat_print_form(bb, cpu: bool = True, reps: int = 5):
 
     if cpu and have_reference() and Reference().has_bigfloat_print:
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
         (din, ppin), want = ref.bigfloat_print(limbs, offset, False, 0)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                 "call": "BigFloat::print"}
         if not (np.array_equal(din, digits) and ppin == pp and text == want):
             raise SystemExit("bench BigFloat print: text differs from the reference's")
@@ -727,11 +805,11 @@ def decimal_print_form(bb, cpu: bool = True):
         raise SystemExit("bench decimal: bgpu_to_decimal and the hooked reference print different text")
     if cpu and have_reference():
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         ref.to_dec_string(limbs[:4096])
         t0 = time.perf_counter()
         s_cpu = ref.to_dec_string(limbs)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(), "call": "BigInt::print"}
+        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(), "call": "BigInt::print"}
         if s_cpu != s_gpu:
             raise SystemExit("bench decimal: hooked reference prints a different number")
         res["verified"] = "identical decimal text (native, hooked reference, pure reference)"
@@ -762,13 +840,13 @@ def decimal_parse_form(bb, cpu: bool = True):
 
     if have_reference() and Reference().has_from_dec:
         ref = Reference()
-        ref.init_thread_pool(host_cores())
+        ref.init_thread_pool(ref_pool_threads())
         ref.from_dec_string(text[:100000])
         if cpu:
             t0 = time.perf_counter()
         want, wneg = ref.from_dec_string(text)
         if cpu:
-            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
                                     "call": "BigInt(const std::string&)"}
         if not (np.array_equal(got, want) and neg == wneg):
             raise SystemExit("bench decimal parse: result differs from the reference's")
@@ -792,18 +870,49 @@ def limbs_to_digits28_np(limbs) -> np.ndarray:
     return d[:n]
 
 
-def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
-    """Config "batched uneven": 4096 products, operand lengths log-uniform in
-    [2^10, 2^22] bits, one graph launch per batch vs one plain NTT call per
-    product (same inputs, device resident, > L2 in total)."""
-    rng = np.random.default_rng(SEED + 3)
+BATCH_SEED = SEED + 3
+
+
+def batched_sizes(nprod: int = 4096, seed: int = BATCH_SEED):
+    """Operand lengths (u64 limbs) of the batched uneven workload: each
+    operand's bit length log-uniform in [2^10, 2^22], drawn independently."""
+    rng = np.random.default_rng(seed)
     na = np.maximum(1, (np.exp2(rng.uniform(10, 22, nprod)) // 64).astype(np.int64))
     nb = np.maximum(1, (np.exp2(rng.uniform(10, 22, nprod)) // 64).astype(np.int64))
+    return na, nb
+
+
+def batched_operands(i: int, na: int, nb: int, seed: int = BATCH_SEED):
+    """Operands of product i of the batched workload: uniform limbs, top bit
+    set, from a stream of their own (so any product can be rebuilt alone)."""
+    rng = np.random.default_rng([seed, i])
+    a = rng.integers(0, 2**64, int(na), dtype=np.uint64, endpoint=False)
+    b = rng.integers(0, 2**64, int(nb), dtype=np.uint64, endpoint=False)
+    a[-1] |= np.uint64(1 << 63)
+    b[-1] |= np.uint64(1 << 63)
+    return a, b
+
+
+def batched_inputs(nprod: int = 4096, seed: int = BATCH_SEED):
+    """The whole batched workload in one array: (big, offs_a, na, offs_b, nb)."""
+    na, nb = batched_sizes(nprod, seed)
     offs_a = np.concatenate([[0], np.cumsum(na)[:-1]])
     offs_b = np.concatenate([[0], np.cumsum(nb)[:-1]]) + na.sum()
-    big = rng.integers(0, 2**64, int(na.sum() + nb.sum()), dtype=np.uint64, endpoint=False)
-    big[offs_a + na - 1] |= np.uint64(1 << 63)
-    big[offs_b + nb - 1] |= np.uint64(1 << 63)
+    big = np.empty(int(na.sum() + nb.sum()), dtype=np.uint64)
+    for i in range(nprod):
+        a, b = batched_operands(i, na[i], nb[i], seed)
+        big[offs_a[i]:offs_a[i] + na[i]] = a
+        big[offs_b[i]:offs_b[i] + nb[i]] = b
+    return big, offs_a, na, offs_b, nb
+
+
+def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5, ref_every: int = 64):
+    """Config "batched uneven": 4096 products, operand lengths log-uniform in
+    [2^10, 2^22] bits, one graph launch per batch vs one plain NTT call per
+    product (same inputs, device resident, > L2 in total).  Every product is
+    checked by its residue and against the one-call-per-product output; every
+    `ref_every`-th product also limb-exact against the reference's _mul."""
+    big, offs_a, na, offs_b, nb = batched_inputs(nprod)
     dbig = _dev_limbs(torch, device, big)
     outn = na + nb
     offs_o = np.concatenate([[0], np.cumsum(outn)[:-1]])
@@ -834,12 +943,28 @@ def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
         for i in range(nprod):
             a_ptr, n_a, b_ptr, n_b, o_ptr = prods[i]
             bb.mul_device(a_ptr, n_a, b_ptr, n_b, o_ptr, stream=sp, method=bb.BGPU_METHOD_NTT)
+    dout.zero_()
     one_by_one(0)
     bb.device_status(sp)
+    if not np.array_equal(dout.cpu().numpy().view(np.uint64), host):
+        raise SystemExit("bench batched: the batch differs from one plain NTT call per product")
     ms_single = _event_ms(torch, stream, one_by_one, 1)
     bb.device_status(sp)
     launches = plan.launches
     plan.close()
+    verified = "residue mod 2^61-1 and identical to one plain NTT call, every product"
+    from oracle.pyoracle import Reference, have_reference
+
+    if have_reference() and ref_every:
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
+        for i in range(0, nprod, ref_every):
+            a = big[offs_a[i]:offs_a[i] + na[i]]
+            b = big[offs_b[i]:offs_b[i] + nb[i]]
+            c = np.trim_zeros(host[offs_o[i]:offs_o[i] + outn[i]], "b")
+            if not np.array_equal(c, ref.mul(a, b)):
+                raise SystemExit(f"bench batched: product {i} differs from the reference's _mul")
+        verified += f"; every {ref_every}th product limb-exact vs the reference's _mul"
     return {"products": nprod, "operand_bits": "log-uniform [2^10, 2^22]",
             "batched": {"ms_per_batch": ms_batch, "products_per_s": nprod / (ms_batch * 1e-3),
                         "launches_per_batch": launches, "graph_launches": 1,
@@ -847,7 +972,7 @@ def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5):
             "one_plain_ntt_launch_per_product": {"ms": ms_single,
                                                  "products_per_s": nprod / (ms_single * 1e-3),
                                                  "launches": 4 * nprod},
-            "speedup": ms_single / ms_batch, "verified": "residue mod 2^61-1, every product"}
+            "speedup": ms_single / ms_batch, "verified": verified}
 
 
 def batched_same_size_form(bb, torch, device, port, A, B, count: int = 32, runs: int = 10):
@@ -912,15 +1037,19 @@ def tree_form(bb, torch, device, port, nleaves: int = 1 << 20, reps: int = 3, cp
            "ms": 1e3 * statistics.median(times), "products_per_s": (nleaves - 1) / statistics.median(times),
            "result_bits": int(np.count_nonzero(got) and (len(np.trim_zeros(got, "b")) * 64)),
            "verified": "residue mod 2^61-1 of the product of all leaves"}
-    if cpu:
-        from oracle.pyoracle import Reference, have_reference
+    from oracle.pyoracle import Reference, have_reference
 
-        if have_reference():
-            ref = Reference()
-            ref.init_thread_pool(host_cores())
-            t0 = time.perf_counter()
-            ref.product_tree_digits(leaves)
-            res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": host_cores(),
+    if have_reference():
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
+        t0 = time.perf_counter()
+        want = ref.product_tree_digits(leaves)
+        t_ref = time.perf_counter() - t0
+        if not np.array_equal(limbs_to_digits28_np(got), want):
+            raise SystemExit("bench tree: the product differs from the reference's BigInt tree")
+        res["verified"] += "; limb-exact vs the reference's BigInt tree"
+        if cpu:
+            res["cpu_reference"] = {"s": t_ref, "threads": ref_pool_threads(),
                                     "call": "BigInt::operator* pairwise tree"}
     return res
 
@@ -928,38 +1057,32 @@ def tree_form(bb, torch, device, port, nleaves: int = 1 << 20, reps: int = 3, cp
 # ---- arms --------------------------------------------------------------------------
 
 def run_reference_arm(args) -> None:
+    """The reference's own CPU multiply (`_mul`, from oracle/_ref) on the host
+    cores: K products after W warm-up products at each thread count of
+    `cpu_thread_counts()`, each count in a process of its own; the line's
+    value is the fastest count, and every count is listed."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
-    a, b = make_operands(args.bits)
-    threads = host_cores()
-    from oracle.pyoracle import Port, Reference, have_reference
-
-    if have_reference():
-        impl, kind, cores = Reference(), "reference", threads
-        impl.init_thread_pool(threads)
-        fn = impl.mul
-    else:
-        impl, kind, cores = Port(), "port", 1
-        fn = impl.ntt_mul
-    for _ in range(args.warmup):
-        fn(a, b)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        fn(a, b)
-    el = time.perf_counter() - t0
-    value = args.steps / el
+    rows = cpu_reference_rates(args.bits, seconds=0.0, max_reps=args.steps, min_reps=args.steps,
+                               warmup=args.warmup)
+    best = max(rows, key=lambda r: r["rate"])
+    value, cores, kind = best["rate"], best["threads"], best["kind"]
     line = {
         "impl": "reference",
         "metric": "bit-exact products/s (2^24 x 2^24-bit multiply)",
         "value": value, "unit": "products/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name(args.bits), "call": "bigint::mul::_mul",
-                   "threads": cores, "parallelism": "host threads (init_thread_pool)"},
+                   "threads": cores, "parallelism": "host threads (init_thread_pool)",
+                   "thread_counts": {str(r["threads"]): {"products_per_s": r["rate"], "reps": r["reps"]}
+                                     for r in rows},
+                   "physical_cores": physical_cores(), "logical_cpus": host_cores()},
         "cpu_baseline": {"value": value, "unit": "products/s", "cores": cores, "kind": kind,
-                         "sample": f"{args.steps} products of the full workload after "
-                                   f"{args.warmup} warm-up products"},
+                         "sample": f"{args.steps} products of the full workload after {args.warmup} "
+                                   f"warm-up products, at {', '.join(str(r['threads']) for r in rows)} "
+                                   f"threads (value: the fastest, {cores})"},
         "e2e": {"value": value, "unit": "products/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -1004,38 +1127,49 @@ def run_gpu_arm(args) -> None:
     bb.device_status(sptr)
     launches_per_step = bb.last_launch_count()
 
-    # Timed region: K back-to-back products on one stream.  Step i uses operand
+    # Timed region: windows of exactly K back-to-back products on one stream,
+    # each bracketed by a barrier and a device synchronize on both sides and
+    # timed with CUDA events on the launching stream.  Step i uses operand
     # pair i mod npairs; all pairs together exceed L2, so no step finds its
-    # inputs cached by the previous one.
+    # inputs cached by the previous one.  The window repeats until about
+    # `--window-seconds` of device time (at least 5 windows) so the clock
+    # sampler sees the whole run; the reported time is the median window.
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dOut.zero_()  # every output checked below comes from the timed products
-    barrier(world, device)
-    torch.cuda.synchronize(device)
-    with ClockSampler(pci_bus_id(device)) as clk:
+
+    def window(flags, first_step):
+        barrier(world, device)
+        torch.cuda.synchronize(device)
         with torch.cuda.stream(stream):
+            h0 = time.perf_counter()
             t0.record(stream)
             for i in range(args.steps):
-                step(args.warmup + i)
+                step(first_step + i, flags)
             t1.record(stream)
+            issue_s = time.perf_counter() - h0
         torch.cuda.synchronize(device)
-    barrier(world, device)
+        barrier(world, device)
+        return t0.elapsed_time(t1), issue_s
+
+    first_ms, _ = window(bb.BGPU_INDEPENDENT, args.warmup)
+    nwin = int(reduce_max(float(min(2000, max(5, round(args.window_seconds * 1e3 / max(first_ms, 1e-3))))),
+                          world, device))
+    win_ms, issue = [], []
+    with ClockSampler(pci_bus_id(device)) as clk:
+        for w in range(nwin):
+            ms, iss = window(bb.BGPU_INDEPENDENT, args.warmup + w * args.steps)
+            win_ms.append(ms)
+            issue.append(iss)
     bb.device_status(sptr)
-    total_ms = reduce_max(t0.elapsed_time(t1), world, device)
+    total_ms = reduce_max(statistics.median(win_ms), world, device)
     clocks = clk.summary()
     out_timed = dOut.cpu().numpy().view(np.uint64)
 
     # The same K products without the flag: every product fully after the
     # previous one (what a caller gets without promising independence).
-    barrier(world, device)
-    torch.cuda.synchronize(device)
-    with torch.cuda.stream(stream):
-        t0.record(stream)
-        for i in range(args.steps):
-            step(args.warmup + i, 0)
-        t1.record(stream)
-    torch.cuda.synchronize(device)
+    seq_win = [window(0, args.warmup + w * args.steps)[0] for w in range(max(5, nwin // 4))]
     bb.device_status(sptr)
-    seq_ms = reduce_max(t0.elapsed_time(t1), world, device)
+    seq_ms = reduce_max(statistics.median(seq_win), world, device)
 
     # Roofline pass: the same K products again with CUDA events recorded on
     # the launching stream between the kernels of every product (kept out of
@@ -1050,17 +1184,29 @@ def run_gpu_arm(args) -> None:
     bb.set_kernel_timing(False)
     bb.device_status(sptr)
 
-    # correctness of every timed output (the overlapped pass) and of the
-    # last pass: residue identity mod 2^61-1, and the two passes agree
+    # correctness of every output slot the timed windows wrote (the
+    # overlapped pass) and of the last pass: residue identity mod 2^61-1, and
+    # the two passes agree; one timed product limb-exact against the
+    # reference's own _mul (oracle/_ref), outside every timed region
     port = Port()
     M = (1 << 61) - 1
     out_host = dOut.cpu().numpy().view(np.uint64)
-    written = sorted({(args.warmup + i) % npairs for i in range(args.steps)})
+    written = sorted({(args.warmup + i) % npairs for i in range(args.steps * nwin)})
     for k in written:
         if (port.mod_m61(A[k]) * port.mod_m61(B[k])) % M != port.mod_m61(out_timed[k]):
             raise SystemExit(f"bench: timed product {k} failed the mod 2^61-1 residue check")
         if not np.array_equal(out_timed[k], out_host[k]):
             raise SystemExit(f"bench: product {k} differs between the overlapped and the plain pass")
+    verified = "residue mod 2^61-1, every output slot of the timed windows"
+    from oracle.pyoracle import Reference, have_reference
+
+    if have_reference() and rank == 0:
+        k = written[0]
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
+        if not np.array_equal(out_timed[k], ref.mul(A[k], B[k])):
+            raise SystemExit(f"bench: timed product {k} differs from the reference's _mul")
+        verified += f"; product {k} limb-exact vs the reference's bigint::mul::_mul"
 
     # e2e through the public host API from pinned buffers: bgpu_mul_u64_many,
     # which pipelines a list of host-resident products (every product copies
@@ -1074,11 +1220,14 @@ def run_gpu_arm(args) -> None:
     pairs = [(pA[i % npairs], pB[i % npairs]) for i in range(e2e_steps)]
     outs = [pOut[i % npairs] for i in range(e2e_steps)]
     bb.mul_many(pairs[:4], outs[:4])  # warm-up
-    torch.cuda.synchronize(device)
-    barrier(world, device)
-    te = time.perf_counter()
-    bb.mul_many(pairs, outs)
-    e2e_s = reduce_max(time.perf_counter() - te, world, device)
+    e2e_win = []
+    for _ in range(5):  # five windows of the K host-resident products; the median one
+        torch.cuda.synchronize(device)
+        barrier(world, device)
+        te = time.perf_counter()
+        bb.mul_many(pairs, outs)
+        e2e_win.append(time.perf_counter() - te)
+    e2e_s = reduce_max(statistics.median(e2e_win), world, device)
     for k in written:
         if k < e2e_steps and not np.array_equal(pOut[k], out_host[k]):
             raise SystemExit("bench: host-API product differs from the device-resident product")
@@ -1128,11 +1277,14 @@ def run_gpu_arm(args) -> None:
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        rate, kind, cores, reps, el = cpu_reference_rate(A[0], B[0], args.cpu_seconds, 50,
-                                                         host_cores())
-        cpu = {"value": rate, "unit": "products/s", "cores": cores, "kind": kind,
-               "sample": f"{reps} full 2^24 x 2^24-bit products in {el:.1f} s "
-                         f"({'bigint::mul::_mul' if kind == 'reference' else 'C port ntt_mul'})"}
+        rows = cpu_reference_rates(args.bits, args.cpu_seconds / len(cpu_thread_counts()), 50)
+        best = max(rows, key=lambda r: r["rate"])
+        cpu = {"value": best["rate"], "unit": "products/s", "cores": best["threads"], "kind": best["kind"],
+               "sample": "; ".join(f"{r['threads']} threads: {r['reps']} full 2^24 x 2^24-bit products in "
+                                   f"{r['seconds']:.1f} s ({r['rate']:.2f}/s)" for r in rows) +
+                         f" ({'bigint::mul::_mul' if best['kind'] == 'reference' else 'C port ntt_mul'}; "
+                         f"value: the fastest count)",
+               "physical_cores": physical_cores(), "logical_cpus": host_cores()}
 
     value = world * args.steps / (total_ms * 1e-3)
     line = {
@@ -1144,14 +1296,24 @@ def run_gpu_arm(args) -> None:
                    "transform_points": 1 << log_n, "digit_bits": 32,
                    "l2": f"inputs larger than L2: {npairs} distinct operand pairs "
                          f"({npairs * 2 * na * 8 >> 20} MiB) cycled, steps back to back",
-                   "parallelism": f"replicas x{world}", "verified": "residue mod 2^61-1, every output",
+                   "parallelism": f"replicas x{world}", "verified": verified,
                    "pipelining": "independent products (BGPU_INDEPENDENT): each product's forward "
-                                 "transform starts under the previous product's carry scan"},
+                                 "transform starts under the previous product's carry scan",
+                   "timing": f"median of {nwin} windows of exactly K={args.steps} products, each window "
+                             "bracketed by barrier + synchronize, CUDA events on the launching stream; "
+                             "max over ranks",
+                   "windows_ms": {"median": statistics.median(win_ms), "min": min(win_ms),
+                                  "max": max(win_ms), "count": nwin},
+                   "host_issue_us_per_product": statistics.median(issue) / args.steps * 1e6,
+                   "host_issue_note": "host time to enqueue one product (4 launches through the C-ABI); "
+                                      "below the device time per product, the launches are hidden"},
         "sequential": {"ms_per_step": seq_ms / args.steps, "value": world * args.steps / (seq_ms * 1e-3),
-                       "note": "the same products without BGPU_INDEPENDENT, each after the previous"},
+                       "note": "the same products without BGPU_INDEPENDENT, each after the previous "
+                               f"(median of {len(seq_win)} windows)"},
         "e2e": {"value": world * e2e_steps / e2e_s, "unit": "products/s",
                 "h2d_bytes_per_step": (na + nb) * 8, "d2h_bytes_per_step": (na + nb) * 8,
-                "api": f"bgpu_mul_u64_many over {e2e_steps} host-resident products (pinned)",
+                "api": f"bgpu_mul_u64_many over {e2e_steps} host-resident products (pinned), "
+                       "median of 5 calls",
                 "single_call": {"value": world * single_steps / single_s, "unit": "products/s",
                                 "api": "bgpu_mul_u64, one synchronous call per product"}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
@@ -1226,6 +1388,11 @@ def main(argv=None) -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--bits", type=int, default=OPERAND_BITS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--window-seconds", type=float, default=0.25,
+                    help="device time the K-product window is repeated for (median window reported)")
+    ap.add_argument("--cpu-worker", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-max-reps", type=int, default=50, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-min-reps", type=int, default=1, help=argparse.SUPPRESS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the other configurations (size sweep, FFT form, batch, tree)")
@@ -1234,6 +1401,9 @@ def main(argv=None) -> None:
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.cpu_worker:
+        run_cpu_worker(args)
+        return
     if args.form:
         run_single_form(args)
         return

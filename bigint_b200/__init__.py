@@ -78,6 +78,7 @@ from ._lib import (  # noqa: F401
     product_tree_device,
     reciprocal_digits,
     set_batch_split,
+    set_block_limbs,
     set_split,
     set_kernel_timing,
     set_tuning,

@@ -117,6 +117,8 @@ def _load() -> C.CDLL:
     L.bgpu_bigfloat_to_decimal.argtypes = [u32p, C.c_size_t, C.c_int64, C.c_int, C.c_size_t, C.c_char_p,
                                            C.c_size_t, C.POINTER(C.c_size_t)]
     L.bgpu_bigfloat_to_decimal.restype = C.c_int
+    L.bgpu_set_block_limbs.argtypes = [C.c_uint64]
+    L.bgpu_set_block_limbs.restype = C.c_int
     L.bgpu_mul_u64_device.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_uint32, C.c_void_p]
     L.bgpu_mul_u64_device.restype = C.c_int
@@ -530,6 +532,13 @@ def device_status(stream: int = 0) -> None:
 
 def last_launch_count() -> int:
     return int(lib.bgpu_last_launch_count())
+
+
+def set_block_limbs(limbs: int) -> None:
+    """Operand block of the products beyond the largest transform (a power of
+    two in [64, 2^24] limbs; 0 = the default 2^24).  A test hook: with a small
+    block, products above 4 * limbs points take the block path."""
+    _check(lib.bgpu_set_block_limbs(int(limbs)), "bgpu_set_block_limbs")
 
 
 def set_split(log2_points: int, log2_column: int) -> None:

@@ -82,6 +82,9 @@ struct Engine {
     bool kernel_timing = false;
     std::vector<cudaEvent_t> kev;  // kTimingRing * (kNttLaunches + 1)
     uint64_t kev_count = 0;
+    // operand block of products beyond the largest transform (a power of
+    // two; kHugeBlockLimbs unless a test shrinks it with bgpu_set_block_limbs)
+    uint64_t huge_block = kHugeBlockLimbs;
 };
 
 constexpr uint64_t kTimingRing = 1024;  // products whose kernel times are kept
@@ -274,8 +277,13 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
 
 // True when a product of na x nb limbs needs more points than the largest
 // transform.
+// Largest transform a single product uses: a block pair of huge_block limbs
+// each fills 2^(log2(huge_block) + 2) points, exactly the largest transform
+// for the default block.
+int transform_cap_log() { return ceil_log2(g.huge_block) + 2; }
+
 bool beyond_transform(size_t na, size_t nb) {
-    return ceil_log2(2 * (uint64_t)(na + nb) - 1) > kMaxLogN;
+    return ceil_log2(2 * (uint64_t)(na + nb) - 1) > transform_cap_log();
 }
 
 // Product beyond the largest transform (huge.cu): both operands in blocks of
@@ -284,7 +292,7 @@ bool beyond_transform(size_t na, size_t nb) {
 // square computes each off-diagonal block pair once and adds it twice.
 int huge_product(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, uint64_t* dout, bool square,
                  cudaStream_t st) {
-    const uint64_t S = kHugeBlockLimbs, L = na + nb;
+    const uint64_t S = g.huge_block, L = na + nb;
     const size_t acc = align256((size_t)accumulate_blocks(L) * 4);
     int rc = ensure(&g.d_huge, &g.huge_bytes, 2 * S * 8 + 2 * acc);
     if (rc != BGPU_OK) return rc;
@@ -798,7 +806,7 @@ int mul_digits_locked(const uint32_t* a, size_t na, const uint32_t* b, size_t nb
     // transform (blocks of NTT products, huge.cu).
     const uint32_t sm = small_method(flags, la64, lb64);
     const uint64_t n32 = (bits28(pa, la) + 31) / 32 + (bits28(pb, lb) + 31) / 32;
-    const bool huge = !sm && ceil_log2(n32 - 1) > kMaxLogN;
+    const bool huge = !sm && ceil_log2(n32 - 1) > transform_cap_log();
     if (sm || huge) {
         uint64_t* la_d = reinterpret_cast<uint64_t*>(io + l_off);
         uint64_t* lb_d = square ? la_d : la_d + align256((la64 + 1) * 8) / 8;
@@ -1098,7 +1106,7 @@ int digits_product(const DVal& a, size_t off_a, const DVal& b, size_t off_b, uin
     const uint64_t bits_a = 28 * (uint64_t)(la - 1) + (32 - __builtin_clz(a.top));
     const uint64_t bits_b = 28 * (uint64_t)(lb - 1) + (32 - __builtin_clz(b.top));
     const uint32_t sm = small_method(BGPU_METHOD_AUTO, la64, lb64);
-    const bool huge = !sm && ceil_log2((bits_a + 31) / 32 + (bits_b + 31) / 32 - 1) > kMaxLogN;
+    const bool huge = !sm && ceil_log2((bits_a + 31) / 32 + (bits_b + 31) / 32 - 1) > transform_cap_log();
     if (sm || huge) {  // on u64 limbs: the small kernels, or NTT blocks beyond the largest transform
         int rc;
         uint32_t* scr = rslot(kRsScratch, 2 * ((la64 + 1) + (lb64 + 1) + (la64 + lb64)), &rc);
@@ -2337,6 +2345,14 @@ int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_
         if (len > out_cap) return BGPU_ERR_OUT_CAPACITY;
         memcpy(out, dst, len * 8);
     }
+    return BGPU_OK;
+}
+
+int bgpu_set_block_limbs(uint64_t limbs) {
+    if (limbs == 0) limbs = kHugeBlockLimbs;
+    if (limbs < 64 || limbs > kHugeBlockLimbs || (limbs & (limbs - 1))) return BGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g.huge_block = limbs;
     return BGPU_OK;
 }
 

@@ -112,6 +112,17 @@ cudaError_t launch_ntt_product(int slot, const NttConsts& host, const OperandDes
 constexpr int kNttLaunches = 4;
 extern const char* const kNttKernelNames[kNttLaunches];
 
+// Carry-scan blocks: kCarryThreads threads, each resolving kCarryPer
+// consecutive 8-coefficient chunks.
+#ifndef BGPU_CARRY_THREADS
+#define BGPU_CARRY_THREADS 256
+#endif
+#ifndef BGPU_CARRY_PER
+#define BGPU_CARRY_PER 4
+#endif
+constexpr int kCarryThreads = BGPU_CARRY_THREADS;
+constexpr int kCarryPer = BGPU_CARRY_PER;
+constexpr uint32_t kCarryChunksPerBlock = (uint32_t)(kCarryThreads * kCarryPer);
 uint32_t carry_blocks(uint32_t nchunks);
 
 // Diagnostic launch of the carry scan's bounded wait on one flag word.

@@ -48,7 +48,7 @@ constexpr size_t kOffY = 0;
 constexpr size_t kOffChunks = kOffY + al256(2 * (size_t)kNumPrimes * kNaPoints * 4);
 constexpr size_t kOffSpill = kOffChunks + al256(kNaPoints / 2 * 8);
 constexpr size_t kOffFlags = kOffSpill + al256(kNaPoints / 8 * 8);
-constexpr size_t kFlagWords = (kNaPoints / 8 + 1 + 255) / 256;  // carry-scan blocks
+constexpr size_t kFlagWords = (kNaPoints / 8 + kCarryChunksPerBlock) / kCarryChunksPerBlock;  // carry-scan blocks
 constexpr size_t kOffTicket = kOffFlags + al256(kFlagWords * 8);
 constexpr size_t kOffErr = kOffTicket + 256;
 constexpr size_t kScratchBytes = kOffErr + 256;

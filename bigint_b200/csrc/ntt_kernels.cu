@@ -626,8 +626,6 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
 
 // ---- kernel 4: carry scan with decoupled look-back ----------------------------
 
-constexpr int kCarryThreads = 256;
-constexpr int kCarryPer = 4;  // consecutive chunks per thread
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait, then error exit
 
 struct CarryArgs {
@@ -945,7 +943,10 @@ static constexpr int mid_threads(int l1) { return l1 >= 12 ? 256 : (l1 >= 9 ? (1
 template <int PS, int L2>
 static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, uint32_t tiles,
                                 int count, cudaStream_t st) {
-    constexpr int T = 256, TP = 128;
+#ifndef BGPU_INV_TP
+#define BGPU_INV_TP 128
+#endif
+    constexpr int T = 256, TP = BGPU_INV_TP;
     if (f) {
         auto k = k_fwd_cols<PS, L2, T>;
         const size_t sm = smem_fwd_cols(L2);
@@ -1016,8 +1017,7 @@ static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint3
 }
 
 uint32_t carry_blocks(uint32_t nchunks) {
-    constexpr uint32_t per_block = kCarryThreads * kCarryPer;
-    return (nchunks + 1 + per_block - 1) / per_block;
+    return (nchunks + 1 + kCarryChunksPerBlock - 1) / kCarryChunksPerBlock;
 }
 
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }

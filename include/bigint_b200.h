@@ -287,6 +287,16 @@ int bgpu_product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out
 int bgpu_product_tree_u64(const uint64_t* leaves, size_t n, uint64_t* out, size_t out_cap,
                           size_t* out_len);
 
+/* Test hook for the products beyond the largest transform (the size range
+ * the reference gives to ssa::mul, src/mul/ssa.cpp:383-401 via
+ * include/bigint/mul.h:208-220).  Such products cut both operands into blocks
+ * of `limbs` u64 limbs and run every block pair as one NTT product; by default
+ * the block is 2^24 limbs, whose block pairs fill the largest transform.  A
+ * smaller power of two in [64, 2^24] makes every product above 4 * limbs
+ * 32-bit points take the block path, so tests can check it against the
+ * oracle at small sizes; 0 restores the default. */
+int bgpu_set_block_limbs(uint64_t limbs);
+
 /* Transform split used for 2^log2_points-point products: the column pass
  * length 2^log2_column (the row pass gets the rest).  Set by the autotuner
  * (bigint_b200/autotune.py); log2_column = 0 restores the built-in choice.

@@ -6,7 +6,8 @@ pair on the NTT and adds the block products into the result with a device
 carry scan.  At these sizes the CPU oracle takes minutes, so the checks are
 size-independent: the residue identity mod 2^61-1, the low limb, operand
 order, and the all-ones closed form, whose carries cross every block
-boundary."""
+boundary.  The block path itself is also run with small blocks (the
+bgpu_set_block_limbs test hook) and compared limb-exact with the oracle."""
 from __future__ import annotations
 
 import numpy as np
@@ -125,3 +126,49 @@ def test_pipelined_host_api_with_a_huge_product(bb, port):
     outs = bb.mul_many(pairs)
     for (a, b), c in zip(pairs, outs):
         check_product(port, a, b, c)
+
+
+@pytest.fixture
+def small_blocks(bb):
+    bb.set_block_limbs(1 << 10)
+    yield 1 << 10
+    bb.set_block_limbs(0)
+
+
+@pytest.mark.parametrize("na,nb", [(4096, 4096), (3000, 5000), (1025, 9000), (1 << 13, 1 << 13),
+                                   (10000, 1500), (2049, 2049)])
+def test_block_path_small_blocks_vs_oracle(bb, port, small_blocks, na, nb):
+    """Blocks of 2^10 limbs: every product above 2^12 points runs as block
+    products plus carry-scan accumulation; ragged last blocks, unbalanced
+    block counts and squares, limb-exact against the oracle."""
+    rng = np.random.default_rng(SEED + 300 + na + 3 * nb)
+    a, b = rand_limbs(rng, na), rand_limbs(rng, nb)
+    assert np.array_equal(bb.ntt_mul(a, b), port.mul(a, b))
+    assert np.array_equal(bb.ntt_mul(a), port.mul(a))
+
+
+def test_block_path_small_blocks_all_ones_and_device_entry(bb, port, small_blocks):
+    """All-ones operands (carries across every block boundary) through the
+    host API, the device entry and Digits, against the oracle."""
+    torch = pytest.importorskip("torch")
+    a = np.full(5000, ONES)
+    b = np.full(3333, ONES)
+    want = port.mul(a, b)
+    assert np.array_equal(bb.ntt_mul(a, b), want)
+    assert np.array_equal(bb.ntt_mul(a), port.mul(a))
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    out = torch.full((a.size + b.size,), -1, dtype=torch.int64, device="cuda")
+    bb.mul_device(da.data_ptr(), a.size, db.data_ptr(), b.size, out.data_ptr(), method=bb.BGPU_METHOD_NTT)
+    bb.device_status(0)
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
+    rng = np.random.default_rng(SEED + 310)
+    da_, db_ = rand_digits(rng, 9000), rand_digits(rng, 7000)
+    assert np.array_equal(bb.mul_digits(da_, db_), port.mul_digits(da_, db_))
+
+
+def test_block_limbs_hook_rejects_bad_sizes(bb):
+    for bad in (63, 100, (1 << 24) + 1, 1 << 25):
+        with pytest.raises(bb.BigIntGPUError):
+            bb.set_block_limbs(bad)
+    bb.set_block_limbs(0)
