@@ -34,8 +34,11 @@ namespace bgpu {
 // shortens the hand-over from the column pass under programmatic dependent
 // launch (measured at 2^20 points: the isolated kernel time is unchanged, the
 // product 7 us shorter).  Longer rows need more registers and keep the default.
+#ifndef BGPU_MID_THREADS_PER_SM
+#define BGPU_MID_THREADS_PER_SM 1280
+#endif
 __host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
-    return (l1 <= 11 && threads >= 64) ? 1280 / threads : 1;
+    return (l1 <= 11 && threads >= 64) ? BGPU_MID_THREADS_PER_SM / threads : 1;
 }
 
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
@@ -48,14 +51,15 @@ cudaError_t upload_consts(int slot, const NttConsts& c) {
 
 // ---- register-resident butterflies ------------------------------------------
 
-// DIF stages for pair bits HI..LO on the 2^R elements base + (j << LO).
+// DIF stages for pair bits HI..LO on the 2^R elements base + (j << LO),
+// starting at stage T0 (the stages before it already done by the caller).
 // Element pair (i, i+h): (a, b) -> (a+b, (a-b) * omega_{2h}^(i mod h)).
-template <bool LAZY, int R, int HI, int LO>
+template <bool LAZY, int R, int HI, int LO, int T0 = 0>
 __device__ __forceinline__ void dif_regs(uint32_t (&x)[1 << R], uint32_t base_low,
                                          const uint2* __restrict__ tw, uint32_t p) {
     const uint2* twb = tw + base_low;  // every twiddle below is twb[compile-time offset]
 #pragma unroll
-    for (int t = 0; t < R; ++t) {
+    for (int t = T0; t < R; ++t) {
         const uint32_t h = 1u << (HI - t);
         const int dist = 1 << (R - 1 - t);
 #pragma unroll
@@ -171,17 +175,6 @@ __device__ __forceinline__ uint32_t bitrev(uint32_t v, int bits) {
     return bits == 0 ? 0u : (__brev(v) >> (32 - bits));
 }
 
-// 32-bit digit n of an operand (0 beyond its length).
-__device__ __forceinline__ uint32_t load_digit32(const OperandDesc& in, uint32_t n) {
-    if (n >= in.nd32) return 0u;
-    if (in.fmt == kFmtLimb64) return __ldg(static_cast<const uint32_t*>(in.ptr) + n);
-    const uint32_t* d = static_cast<const uint32_t*>(in.ptr);
-    const uint32_t bit = n * 32u;
-    const uint32_t i0 = bit / 28u, sh = bit - i0 * 28u;  // sh in {0,4,...,24}
-    uint32_t v = __ldg(d + i0) >> sh;
-    if (i0 + 1 < in.nsrc) v |= __ldg(d + i0 + 1) << (28u - sh);
-    return v;
-}
 
 // ---- kernel 1: forward column pass ------------------------------------------
 
@@ -206,8 +199,107 @@ __device__ __forceinline__ ProductDesc product(const ProductDesc* descs, const P
     return descs ? descs[p] : one;
 }
 
+// 32-bit digit n of an operand in a format known at compile time (0 beyond
+// its length).
+template <bool LIMB>
+__device__ __forceinline__ uint32_t load_digit32_fmt(const OperandDesc& in, uint32_t n) {
+    if (n >= in.nd32) return 0u;
+    if constexpr (LIMB) {
+        return __ldg(static_cast<const uint32_t*>(in.ptr) + n);
+    } else {
+        const uint32_t* d = static_cast<const uint32_t*>(in.ptr);
+        const uint32_t bit = n * 32u;
+        const uint32_t i0 = bit / 28u, sh = bit - i0 * 28u;  // sh in {0,4,...,24}
+        uint32_t v = __ldg(d + i0) >> sh;
+        if (i0 + 1 < in.nsrc) v |= __ldg(d + i0 + 1) << (28u - sh);
+        return v;
+    }
+}
+
+// Round 0 of the forward column pass: rows n2 = base + (j << LO) read from
+// the caller's digits (u64 limbs when LIMB, else 28-bit Digits), reduced into
+// [0, 2p) ([0, p) for the strict set) and transformed.  HALF: the operand
+// fills at most the lower half of the transform, so the elements of the upper
+// half (j >= 2^(R-1), rows n2 >= N2/2) are zero: they are not loaded, and the
+// first stage (a, 0) -> (a, a w) is one multiply per pair.  With a single
+// round the inter-pass twiddle and the global store follow; otherwise the
+// elements go to the shared tile.
+template <int PS, int L2, int T, bool LIMB, bool HALF>
+__device__ __forceinline__ void fwd_round0(const FwdColsArgs& a, const OperandDesc& in, const NttConsts& c,
+                                           int q, uint32_t c0, uint32_t* y, const uint2* sS, uint32_t* sm) {
+    constexpr bool LAZY = PS == 0;
+    using P2 = Plan<L2>;
+    constexpr int NR = P2::nr;
+    constexpr int RL = P2::r(NR - 1);
+    constexpr int SROW = (1 << RL) + 1;
+    using Gr = Group<L2, kCols, 0>;
+    constexpr int R = Gr::R;
+    constexpr int D = 1 << (R - 1);
+    constexpr int NL = HALF ? D : (1 << R);  // elements read from the operand
+    const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv, red = c.red[q];
+    const uint2* tw = c.stage[q][0];
+    const uint32_t stride = 1u << (Gr::LO + a.log_n1);  // digit step between a group's rows
+#pragma unroll 2
+    for (int g = threadIdx.x; g < Gr::G; g += T) {
+        const Gr gr(g);
+        uint32_t x[1 << R];
+        uint32_t any = 0;
+        uint32_t n = c0 + gr.col + (gr.base << a.log_n1);
+#pragma unroll
+        for (int j = 0; j < NL; ++j, n += stride) {
+            const uint32_t v = load_digit32_fmt<LIMB>(in, n);
+            any |= v;
+            // v - floor(v * red / 2^32) * p lies in [0, 2p) for any 32-bit v
+            const uint32_t r = v - __umulhi(v, red) * p;
+            x[j] = LAZY ? r : csub(r, p);
+        }
+        if (any) {
+            if constexpr (HALF) {
+                const uint2* twb = tw + gr.base_low;
+#pragma unroll
+                for (int j = 0; j < D; ++j) {
+                    if (Gr::LO == 0 && j == 0) {
+                        x[j + D] = x[j];  // omega^0 (base_low is 0 when LO == 0)
+                    } else {
+                        const uint2 w = __ldg(twb + (1u << Gr::HI) + ((uint32_t)j << Gr::LO));
+                        const uint32_t t = shoup_lazy(x[j], w.x, w.y, p);
+                        x[j + D] = LAZY ? t : csub(t, p);
+                    }
+                }
+                dif_regs<LAZY, R, Gr::HI, Gr::LO, 1>(x, gr.base_low, tw, p);
+            } else {
+                dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) x[j] = 0;
+        }
+        if constexpr (NR == 1) {
+            const uint32_t n1 = c0 + gr.col;
+            const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & ((1u << a.log_n) - 1u),
+                                              a.log_n, p);
+            const uint32_t bwp = bw * pinv;
+            const uint2* srow = sS + gr.col * SROW;
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j)
+                y[(gr.idx(j) << a.log_n1) + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
+        } else {
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
+        }
+    }
+}
+
+// Column tiles of 2^9 rows run 8 CTAs of 256 threads per SM (32 registers a
+// thread, a few bytes spilled): measured at 2^20 points, the product is
+// 0.4 us shorter than with the 40 registers the compiler picks on its own
+// (6 CTAs per SM).  Other heights keep the compiler's choice.
+__host__ __device__ constexpr int fwd_min_blocks(int l2, int threads) {
+    return (l2 == 9 && threads == 256) ? 8 : 1;
+}
+
 template <int PS, int L2, int T>
-__global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
+__global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const FwdColsArgs a) {
     constexpr bool LAZY = PS == 0;
     extern __shared__ __align__(16) uint32_t sm[];  // [2^L2][kCols]
     using P2 = Plan<L2>;
@@ -218,10 +310,9 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
     const OperandDesc in = opi == 0 ? pd.op[0] : pd.op[1];
-    const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
+    const uint32_t c0 = blockIdx.x * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     uint32_t* y = pd.y + ((size_t)opi * kNumPrimes + q) * nn;
-    const uint32_t red = c.red[q];
 
     // The last round's groups hold slots base + j (LO = 0) of one column n1;
     // k2 = bitrev(base) + bitrev_RL(j) << (L2-RL), so the inter-pass twiddle
@@ -242,45 +333,19 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
     if (!a.overlap) pdl_wait();
 
     // Round 0: rows n2 = base + (j << LO) read from the caller's digits.
-    {
-        using Gr = Group<L2, kCols, 0>;
-        constexpr int R = Gr::R;
-#pragma unroll 2
-        for (int g = threadIdx.x; g < Gr::G; g += T) {
-            const Gr gr(g);
-            uint32_t v[1 << R], x[1 << R];
-            uint32_t any = 0;
-#pragma unroll
-            for (int j = 0; j < (1 << R); ++j) {
-                v[j] = load_digit32(in, c0 + gr.col + n1_len * gr.idx(j));
-                any |= v[j];
-            }
-#pragma unroll
-            for (int j = 0; j < (1 << R); ++j) {
-                // v - floor(v * red / 2^32) * p lies in [0, 2p) for any 32-bit v
-                const uint32_t r = v[j] - __umulhi(v[j], red) * p;
-                x[j] = LAZY ? r : csub(r, p);
-            }
-            if (any) {
-                dif_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, tw, p);
-            } else {
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j) x[j] = 0;
-            }
-            if constexpr (NR == 1) {
-                const uint32_t n1 = c0 + gr.col;
-                const uint32_t bw = inter_twiddle(c, q, 0, (n1 * bitrev(gr.base, L2)) & (uint32_t)(nn - 1),
-                                                  a.log_n, p);
-                const uint32_t bwp = bw * pinv;
-                const uint2* srow = sS + gr.col * SROW;
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j)
-                    y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
-            } else {
-#pragma unroll
-                for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
-            }
-        }
+    // The digit format and whether the operand fills at most the lower half
+    // of the transform (then every row n2 >= N2/2 is zero) are uniform over
+    // the launch, so each combination is its own copy of the round.
+    if (in.fmt == kFmtLimb64) {
+        if (2 * (size_t)in.nd32 <= nn)
+            fwd_round0<PS, L2, T, true, true>(a, in, c, q, c0, y, sS, sm);
+        else
+            fwd_round0<PS, L2, T, true, false>(a, in, c, q, c0, y, sS, sm);
+    } else {
+        if (2 * (size_t)in.nd32 <= nn)
+            fwd_round0<PS, L2, T, false, true>(a, in, c, q, c0, y, sS, sm);
+        else
+            fwd_round0<PS, L2, T, false, false>(a, in, c, q, c0, y, sS, sm);
     }
     if constexpr (NR > 1) {
         __syncthreads();
@@ -302,7 +367,7 @@ __global__ void __launch_bounds__(T) k_fwd_cols(const FwdColsArgs a) {
             const uint2* srow = sS + gr.col * SROW;
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j)
-                y[(size_t)gr.idx(j) * n1_len + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
+                y[(gr.idx(j) << a.log_n1) + n1] = mul2<LAZY>(x[j], srow[brev_c(j, R)], bw, bwp, p);
         }
     }
     // Let the row pass launch only once this CTA's work is done: an early
@@ -526,6 +591,12 @@ __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r
     w2 = (uint32_t)hi;
 }
 
+#ifndef BGPU_INV_UNROLL
+#define BGPU_INV_UNROLL 4
+#endif
+
+constexpr int kInvUnroll = BGPU_INV_UNROLL;  // groups of the first (global-memory) round in flight per thread
+
 template <int PS, int L2, int TP>
 __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs a) {
     // Three thread groups of TP threads, one per prime, transform their
@@ -551,13 +622,13 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     {
         using Gr = Group<L2, kCols, NR - 1>;
         constexpr int R = Gr::R;
-#pragma unroll 2
+#pragma unroll kInvUnroll
         for (int g = tq; g < Gr::G; g += TP) {
             const Gr gr(g);
             uint32_t x[1 << R];
 #pragma unroll
             for (int j = 0; j < (1 << R); ++j)
-                x[j] = z[(size_t)gr.idx(j) * n1_len + c0 + gr.col];
+                x[j] = z[(gr.idx(j) << a.log_n1) + c0 + gr.col];
             dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
             if constexpr (NR == 1) {
 #pragma unroll
