@@ -272,6 +272,88 @@ def reference_model_bytes(na: int, nb: int) -> int:
     return 10 * 12 * n + 2 * (na + nb) * 8
 
 
+def _plan_rounds(l: int, maxr: int = 4) -> list[int]:
+    """Radix round sizes of a length-2^l transform (the kernels' Plan<L>)."""
+    nr = (l + maxr - 1) // maxr
+    return [l // nr + (1 if k < l % nr else 0) for k in range(nr)]
+
+
+def _bfly_muls(l: int) -> float:
+    """32-bit multiply operations (mul.lo / mul.hi) of one length-2^l transform
+    as the kernels run it: 3 per Shoup butterfly; butterflies whose twiddle is
+    1 are skipped only in the round over the lowest bits."""
+    r_last = _plan_rounds(l)[-1]
+    stages = (l - r_last) + sum(1 - 2.0 ** -k for k in range(r_last))
+    return (1 << (l - 1)) * stages * 3
+
+
+def source_mul_counts(na: int, nb: int, log_n: int, log_n1: int, log_n2: int, square: bool) -> dict:
+    """32-bit multiply operations per launch of each NTT kernel, counted from
+    the kernels' source (butterflies x 3, Montgomery products x 3, the digit
+    reduction x 2, Garner CRT x 14 per point); the compiler's own instruction
+    choice (address arithmetic, moves on the multiply pipe) is not in it."""
+    n, n1, n2 = 1 << log_n, 1 << log_n1, 1 << log_n2
+    ops = 1 if square else 2
+    half = 2 * 2 * max(na, nb) <= n  # every operand in the lower half: half the digits loaded
+    loads = n // 2 if half else n
+    fwd = ops * 3 * (n1 * _bfly_muls(log_n2) + 2 * loads + 6 * n + 4 * n // 8)
+    r0 = _plan_rounds(log_n1)[0]
+    mid = 3 * (n2 * (ops + 1) * _bfly_muls(log_n1) + 4 * n + 6 * n + 7 * n / (1 << r0))
+    inv = 3 * n1 * _bfly_muls(log_n2) + 14 * n
+    return {"k_fwd_cols": fwd, "k_mid_rows": mid, "k_inv_cols": inv, "k_carry": 0.0}
+
+
+def profiled_pipes() -> dict | None:
+    """Per-launch pipe counters of the four NTT kernels at 2^24 x 2^24 bits
+    from the committed ncu summary, if any."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "ntt_2p24_pipes.json")))
+    except (OSError, ValueError):
+        return None
+
+
+def compute_roofline(kernels_ms: dict, dom: str, prod_ms: float, sm_mhz: float | None, counts: dict) -> dict:
+    """The ceiling that binds the transform passes: the 32-bit multiply pipe
+    (fmaheavy: IMAD, IMAD.HI, IMAD.WIDE at 2 warp instructions per SM per
+    cycle, the wide and high forms taking two of those slots) and instruction
+    issue (4 warp instructions per SM per cycle).  Busy cycles per SM come
+    from the committed ncu counters (a clock-independent count); the fraction
+    divides them by the cycles of the live time at the sampled SM clock."""
+    prof = profiled_pipes()
+    res = {"bound": "int32 multiply pipe (fmaheavy)", "kernel": dom,
+           "source_mul_ops_per_launch": counts.get(dom),
+           "source_mul_ops_per_product": sum(counts.values()),
+           "source_note": "counted from the kernel source: 3 per Shoup butterfly or Montgomery product, "
+                          "2 per digit reduction, 14 per Garner CRT point"}
+    if not prof or dom not in prof or not sm_mhz:
+        res["profile"] = None
+        return res
+    clk = sm_mhz * 1e6
+    k = prof[dom]
+    live_cycles = kernels_ms[dom] * 1e-3 * clk
+    res.update({
+        "ncu_fmaheavy_warp_inst_per_launch": k["fmaheavy_warp_inst"],
+        "ncu_thread_mul_inst_per_launch": k["fmaheavy_warp_inst"] * 32,
+        "busy_cycles_per_sm": k["fmaheavy_busy_cycles_per_sm"],
+        "achieved": k["fmaheavy_busy_cycles_per_sm"] / live_cycles,
+        "peak": 1.0, "unit": "fraction of fmaheavy pipe cycles (sampled SM clock)",
+        "frac": k["fmaheavy_busy_cycles_per_sm"] / live_cycles,
+        "issue_frac": k["warp_inst"] / 148 / (4 * live_cycles),
+        "ncu_busy_pct": k["fmaheavy_busy_pct"], "ncu_issue_active_pct": k["issue_active_pct"],
+        "sm_mhz": sm_mhz,
+    })
+    names = [x for x in ("k_fwd_cols", "k_mid_rows", "k_inv_cols", "k_carry") if x in prof]
+    busy = sum(prof[x]["fmaheavy_busy_cycles_per_sm"] for x in names)
+    insts = sum(prof[x]["warp_inst"] for x in names)
+    prod_cycles = prod_ms * 1e-3 * clk
+    res["whole_product"] = {
+        "busy_cycles_per_sm": busy, "cycles_per_product": prod_cycles,
+        "frac": busy / prod_cycles, "issue_frac": insts / 148 / (4 * prod_cycles),
+        "ncu_fmaheavy_warp_inst": sum(prof[x]["fmaheavy_warp_inst"] for x in names),
+        "note": "all four kernels' multiply-pipe busy cycles per SM over the product time"}
+    return res
+
+
 def profiled_traffic(kernel: str) -> float | None:
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "ntt_2p24_traffic.json")
@@ -490,6 +572,12 @@ def fft_form(bb, torch, device, reps: int = 3):
     length or the FP64 coefficient limit) run on the NTT and say so."""
     rng = np.random.default_rng(SEED + 4)
     rows = []
+    from oracle.pyoracle import Reference, have_reference
+
+    ref = None
+    if have_reference():
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
     for k in (20, 22, 24, 26, 28):
         n = (1 << k) // 64
         a = rng.integers(0, 2**64, n, dtype=np.uint64, endpoint=False)
@@ -499,9 +587,18 @@ def fft_form(bb, torch, device, reps: int = 3):
         ones = np.full(n, np.uint64(0xFFFFFFFFFFFFFFFF))
         for fill, x, y in (("uniform", a, b), ("all-ones", ones, None)):
             args = (x,) if y is None else (x, y)
-            nt = [bb.ntt_mul(*args, stats=True)[1].device_ms for _ in range(reps + 1)][1:]
+            nt = [bb.ntt_mul(*args, stats=True) for _ in range(reps + 1)]
+            want = nt[-1][0]
+            verified = "identical to the NTT product"
+            if ref is not None and k <= 24:
+                if not np.array_equal(want, ref.mul(*args)):
+                    raise SystemExit(f"bench fft: NTT product at 2^{k} bits differs from the reference's _mul")
+                verified = "identical to the NTT product and to the reference's _mul"
             for bound, avg in (("worst_case", False), ("average", True)):
-                sts = [bb.fft_mul(*args, average_bound=avg, stats=True)[1] for _ in range(reps + 1)][1:]
+                runs = [bb.fft_mul(*args, average_bound=avg, stats=True) for _ in range(reps + 1)][1:]
+                sts = [r[1] for r in runs]
+                if not all(np.array_equal(r[0], want) for r in runs):
+                    raise SystemExit(f"bench fft: FFT-form product at 2^{k} bits ({fill}, {bound}) is not exact")
                 st = sts[-1]
                 used = "ntt (fallback)" if st.fell_back else (
                     "fft" if st.method == bb.BGPU_METHOD_FFT else "ntt (beyond fft capacity)")
@@ -509,8 +606,10 @@ def fft_form(bb, torch, device, reps: int = 3):
                              "bits_per_point": st.fft_bits or None, "log2_points": st.log2_points,
                              "method": used, "max_round_err": st.max_round_err,
                              "fell_back": bool(st.fell_back),
+                             "fallbacks": sum(1 for s_ in sts if s_.fell_back), "runs": len(sts),
                              "device_ms": statistics.fmean(s_.device_ms for s_ in sts),
-                             "ntt_device_ms": statistics.fmean(nt)})
+                             "ntt_device_ms": statistics.fmean(r[1].device_ms for r in nt[1:]),
+                             "verified": verified})
     return rows
 
 
@@ -1323,7 +1422,10 @@ def run_gpu_arm(args) -> None:
                      "kernel_timing": "events between the kernels, second pass of the same K products",
                      "reference_model": {"bytes_per_product": model_b,
                                          "achieved": model_b / (prod_ms * 1e-3) / 1e9,
-                                         "frac": model_b / (prod_ms * 1e-3) / 1e9 / peak}},
+                                         "frac": model_b / (prod_ms * 1e-3) / 1e9 / peak},
+                     "compute": compute_roofline(mean_k, dom, prod_ms, clocks.get("sm_mhz"),
+                                                 source_mul_counts(na, nb, log_n, log_n - bb.get_split(log_n),
+                                                                   bb.get_split(log_n), False))},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches_per_step * args.steps,
@@ -1335,6 +1437,34 @@ def run_gpu_arm(args) -> None:
 FORMS = ("plain_2p20", "batched_2p24", "ntt_size_sweep", "fp64_fft", "fast_pow", "mul_digits_2p24", "reciprocal_2p24",
          "divmod_2p24", "bigfloat_print_2p22", "decimal_print_2p22", "decimal_parse_5m", "batched_4096",
          "product_tree_2p20")
+
+
+def run_profile_case(args) -> None:
+    """A short, fixed run for profilers: `--profile-case K` products of the
+    headline workload (device resident, BGPU_INDEPENDENT, one stream), then
+    exit.  Prints only a status line; not a measurement."""
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    import bigint_b200 as bb
+
+    bb.init(0)
+    npairs = pairs_beyond_l2(args.bits)
+    A, B = make_operands(args.bits, pairs=npairs)
+    na = nb = A.shape[1]
+    dA = torch.from_numpy(A.view(np.int64)).to(device)
+    dB = torch.from_numpy(B.view(np.int64)).to(device)
+    dOut = torch.zeros((npairs, na + nb), dtype=torch.int64, device=device)
+    stream = torch.cuda.Stream(device)
+    with torch.cuda.stream(stream):
+        for i in range(args.profile_case):
+            k = i % npairs
+            bb.mul_device(dA[k].data_ptr(), na, dB[k].data_ptr(), nb, dOut[k].data_ptr(),
+                          stream=stream.cuda_stream, method=bb.BGPU_INDEPENDENT)
+    bb.device_status(stream.cuda_stream)
+    torch.cuda.synchronize(device)
+    print(json.dumps({"profile_case": args.profile_case, "bits": args.bits, "status": "ok"}))
 
 
 def run_single_form(args) -> None:
@@ -1390,6 +1520,8 @@ def main(argv=None) -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--window-seconds", type=float, default=0.25,
                     help="device time the K-product window is repeated for (median window reported)")
+    ap.add_argument("--profile-case", type=int, default=0,
+                    help="run this many headline products and exit (for ncu; prints no measurement)")
     ap.add_argument("--cpu-worker", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-max-reps", type=int, default=50, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-min-reps", type=int, default=1, help=argparse.SUPPRESS)
@@ -1403,6 +1535,9 @@ def main(argv=None) -> None:
         ap.error("--warmup must be >= 3")
     if args.cpu_worker:
         run_cpu_worker(args)
+        return
+    if args.profile_case:
+        run_profile_case(args)
         return
     if args.form:
         run_single_form(args)

@@ -137,7 +137,7 @@ cudaError_t launch_ntt_batch(int slot, const NttConsts& host, const ProductDesc*
                              cudaStream_t stream);
 
 // ---- FP64 complex-FFT form ----
-constexpr int kFftMaxLogN = 23;     // largest FFT transform (2^23 complex points)
+constexpr int kFftMaxLogN = 26;     // largest FFT transform (2^26 complex points)
 constexpr int kFftStageLog = 13;    // FFT stage tables cover pair distances < 2^13
 constexpr int kFftTwLog = 26, kFftTwSplit = 13;
 

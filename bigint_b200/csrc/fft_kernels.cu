@@ -22,7 +22,10 @@
 
 namespace bgpu {
 
-constexpr int kFftCols = 4;  // columns per column tile: 4 x 16 B = 64 B per row segment
+// Columns per column tile: 4 (64 B per row segment) up to 2^11 rows; 2 and 1
+// for the 2^12- and 2^13-row columns of the largest transforms, so a tile
+// stays at 128 KB of shared memory.
+__host__ __device__ constexpr int fft_cols(int l2) { return l2 <= 11 ? 4 : (l2 == 12 ? 2 : 1); }
 constexpr int kFftMaxR = 3;  // radix-8 rounds (double2 data: 16 values per thread)
 
 __constant__ FftConsts c_fft;
@@ -183,6 +186,7 @@ struct FftFwdArgs {
 
 template <int L2, int T>
 __global__ void __launch_bounds__(T) k_fft_fwd_cols(const FftFwdArgs a) {
+    constexpr int kFftCols = fft_cols(L2);
     extern __shared__ __align__(16) double2 fsm[];  // [2^L2][kFftCols]
     using P2 = Plan<L2, kFftMaxR>;
     constexpr int NR = P2::nr;
@@ -340,6 +344,7 @@ struct FftInvArgs {
 
 template <int L2, int T>
 __global__ void __launch_bounds__(T) k_fft_inv_cols(const FftInvArgs a) {
+    constexpr int kFftCols = fft_cols(L2);
     extern __shared__ __align__(16) double2 fsm[];
     __shared__ double s_err[T / 32];
     using P2 = Plan<L2, kFftMaxR>;
@@ -468,6 +473,7 @@ FftShape fft_choose_shape(int log_n) {
     int l2 = (log_n - 1) / 2;
     if (l2 > 10) l2 = 10;
     if (l2 < 2) l2 = 2;
+    if (log_n - l2 > 13) l2 = log_n - 13;  // rows stop at 2^13 points (128 KB of shared memory)
     s.log_n2 = l2;
     s.log_n1 = log_n - l2;
     return s;
@@ -476,7 +482,7 @@ FftShape fft_choose_shape(int log_n) {
 bool fft_shape_supported(int log_n) {
     if (log_n < 8 || log_n > kFftMaxLogN) return false;
     const FftShape s = fft_choose_shape(log_n);
-    return s.log_n1 >= 3 && s.log_n1 <= 13;
+    return s.log_n1 >= 3 && s.log_n1 <= 13 && s.log_n2 >= 2 && s.log_n2 <= 13;
 }
 
 static constexpr int fft_row_threads(int l1) { return l1 >= 11 ? 256 : (l1 >= 8 ? (1 << (l1 - 3)) : 32); }
@@ -484,7 +490,7 @@ static constexpr int fft_row_threads(int l1) { return l1 >= 11 ? 256 : (l1 >= 8 
 template <int L2>
 static cudaError_t fft_outer(const FftFwdArgs* f, const FftInvArgs* iv, uint32_t tiles, cudaStream_t st) {
     constexpr int T = 256;
-    const size_t sm = ((size_t)kFftCols << L2) * sizeof(double2);
+    const size_t sm = ((size_t)fft_cols(L2) << L2) * sizeof(double2);
     if (f) {
         auto k = k_fft_fwd_cols<L2, T>;
         allow_smem(k, sm);
@@ -507,6 +513,9 @@ static cudaError_t fft_dispatch_outer(int l2, const FftFwdArgs* f, const FftInvA
         case 8: return fft_outer<8>(f, iv, tiles, st);
         case 9: return fft_outer<9>(f, iv, tiles, st);
         case 10: return fft_outer<10>(f, iv, tiles, st);
+        case 11: return fft_outer<11>(f, iv, tiles, st);
+        case 12: return fft_outer<12>(f, iv, tiles, st);
+        case 13: return fft_outer<13>(f, iv, tiles, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -541,7 +550,7 @@ cudaError_t launch_fft_product(const uint64_t* a, uint32_t na, const uint64_t* b
                                int bits, int log_n, const FftScratch& s, cudaStream_t st) {
     if (!fft_shape_supported(log_n)) return cudaErrorInvalidValue;
     const FftShape sh = fft_choose_shape(log_n);
-    const uint32_t tiles = (1u << sh.log_n1) / kFftCols;
+    const uint32_t tiles = (1u << sh.log_n1) / fft_cols(sh.log_n2);
     FftFwdArgs f{a, b, na, nb, bits, s.y, log_n, sh.log_n1};
     cudaError_t e = fft_dispatch_outer(sh.log_n2, &f, nullptr, tiles, st);
     if (e != cudaSuccess) return e;

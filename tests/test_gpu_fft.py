@@ -112,3 +112,25 @@ def test_smallest_transforms(bb):
             b = np.full(nb, ONES) if fill == "ones" else rand_limbs(rng, nb)
             got = bb.fft_mul(a, b)
             assert limbs_to_int(got) == limbs_to_int(a) * limbs_to_int(b), (na, nb, fill)
+
+
+@pytest.mark.parametrize("n,average,log_points", [(1 << 20, False, 24), ((1 << 20) + 1000, False, 25),
+                                                  (1 << 20, True, 24), (1 << 22, True, 26)])
+def test_large_transforms_exact_vs_ntt(bb, n, average, log_points):
+    """The transforms beyond 2^23 complex points (2^11- to 2^13-row column
+    tiles of 4, 2 and 1 columns): 2^26- and 2^28-bit operands, exact whether
+    or not the product falls back to the NTT, with the expected length."""
+    rng = np.random.default_rng(SEED + n + average)
+    a, b = rand_limbs(rng, n), rand_limbs(rng, n)
+    got, st = bb.fft_mul(a, b, average_bound=average, stats=True)
+    assert st.method == bb.BGPU_METHOD_FFT and st.log2_points == log_points, st
+    assert np.array_equal(got, bb.ntt_mul(a, b))
+    if not average:
+        assert not st.fell_back and st.max_round_err < 0.25
+
+
+def test_large_transform_all_ones_square(bb):
+    ones = np.full(1 << 20, ONES)
+    got, st = bb.fft_mul(ones, stats=True)
+    assert st.method == bb.BGPU_METHOD_FFT and st.log2_points == 24 and not st.fell_back
+    assert np.array_equal(got, bb.ntt_mul(ones))
