@@ -705,13 +705,18 @@ def fast_pow_form(bb, port, cpu: bool = True):
             raise SystemExit("bench fast_pow: hooked reference differs from bgpu_pow_u64")
         res["reference_code_on_gpu"] = {"s": el, "call": "bigint::fast_pow<BigInt> with ntt::mul and "
                                         "fft::mul hooked to bgpu_mul_u64", "identical": same}
-    if cpu and have_reference() and Reference().has_fast_pow:
+    if have_reference() and Reference().has_fast_pow:
         ref = Reference()
         ref.init_thread_pool(ref_pool_threads())
         t0 = time.perf_counter()
-        ref.fast_pow_digits(base, e)
-        res["cpu_reference"] = {"s": time.perf_counter() - t0, "threads": ref_pool_threads(),
-                                "call": "bigint::fast_pow<BigInt>"}
+        want = ref.fast_pow_digits(base, e)
+        t_ref = time.perf_counter() - t0
+        if not np.array_equal(digits28_to_limbs_np(want), got):
+            raise SystemExit("bench fast_pow: bgpu_pow_u64 differs from the reference's fast_pow")
+        res["verified"] += "; identical to the reference's fast_pow<BigInt>"
+        if cpu:
+            res["cpu_reference"] = {"s": t_ref, "threads": ref_pool_threads(),
+                                    "call": "bigint::fast_pow<BigInt>"}
     return res
 
 
@@ -1100,12 +1105,21 @@ def batched_same_size_form(bb, torch, device, port, A, B, count: int = 32, runs:
     for i in range(count):
         if port.mod_m61(A[i]) * port.mod_m61(B[i]) % M != port.mod_m61(out[i]):
             raise SystemExit(f"bench batched 2^24: product {i} failed the residue check")
+    verified = "residue mod 2^61-1, every product"
+    from oracle.pyoracle import Reference, have_reference
+
+    if have_reference():
+        ref = Reference()
+        ref.init_thread_pool(ref_pool_threads())
+        if not np.array_equal(out[count - 1], ref.mul(A[count - 1], B[count - 1])):
+            raise SystemExit("bench batched 2^24: the last product differs from the reference's _mul")
+        verified += "; the last product limb-exact vs the reference's _mul"
     per = ms / count
     model = reference_model_bytes(na, nb)
     return {"products": count, "ms_per_batch": ms, "us_per_product": per * 1e3,
             "products_per_s": 1e3 / per, "launches_per_batch": launches,
             "reference_model_frac": model / (per * 1e-3) / 1e9 / measured_peaks()[0],
-            "verified": "residue mod 2^61-1, every product"}
+            "verified": verified}
 
 
 def tree_form(bb, torch, device, port, nleaves: int = 1 << 20, reps: int = 3, cpu: bool = True):
