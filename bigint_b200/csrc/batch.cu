@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -41,6 +42,11 @@ struct bgpu_batch_plan_s {
     int device = -1;
     size_t count = 0;
     std::vector<bgpu::BatchClass> classes;
+    // every NTT class (and the small products) run in the four mixed-length
+    // launches, one per pass
+    bool mixed = false;
+    bgpu::MixedSizes mixed_sizes{};
+    std::vector<std::array<uint32_t, 4>> mixed_begin;  // per class, per pass
     std::vector<bgpu::SchoolDesc> school;  // schoolbook products
     std::vector<bgpu::SchoolDesc> kara;    // Karatsuba products
     void* d_mem = nullptr;  // descriptors, scratch, flags, tickets
@@ -89,7 +95,8 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
         n_desc += c.members.size();
         flag_words += c.flags_words;
     }
-    const size_t school_off = al256(n_desc * sizeof(ProductDesc));
+    const size_t mixed_off = al256(n_desc * sizeof(ProductDesc));
+    const size_t school_off = mixed_off + al256((p->mixed ? p->classes.size() : 0) * sizeof(MixedClass));
     const size_t kara_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
     const size_t tick_off = kara_off + al256(p->kara.size() * sizeof(SchoolDesc));
     unsigned long long* tickets = reinterpret_cast<unsigned long long*>(base + tick_off);
@@ -102,7 +109,25 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
     for (size_t i = 0; e == cudaSuccess && i < branches.size(); ++i) e = cudaStreamWaitEvent(branches[i], fork, 0);
     if (e != cudaSuccess) return BGPU_ERR_CUDA;
     uint32_t launches = 0;
-    for (size_t ci = 0; ci < p->classes.size(); ++ci) {
+    if (p->mixed) {
+        // every class and the small products: four launches on the recording stream
+        MixedArgs m{};
+        m.classes = reinterpret_cast<const MixedClass*>(base + mixed_off);
+        m.nclasses = (int)p->classes.size();
+        for (size_t i = 0; i < p->classes.size(); ++i)
+            for (int pass = 0; pass < 4; ++pass) m.begin[pass][i] = p->mixed_begin[i][pass];
+        m.ticket = tickets;
+        m.ticket_base = 0;
+        m.epoch = 1;
+        m.err = hooks.err;
+        m.school = reinterpret_cast<const SchoolDesc*>(base + school_off);
+        m.nschool = (uint32_t)p->school.size();
+        m.kara = reinterpret_cast<const SchoolDesc*>(base + kara_off);
+        m.nkara = (uint32_t)p->kara.size();
+        if (launch_ntt_mixed(m, p->mixed_sizes, st) != cudaSuccess) return BGPU_ERR_CUDA;
+        launches += kNttLaunches;
+    }
+    for (size_t ci = 0; !p->mixed && ci < p->classes.size(); ++ci) {
         const BatchClass& c = p->classes[ci];
         const int ps = prime_set_for(c.log_n);
         CarryLaunch cl;
@@ -115,14 +140,14 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
         if (e != cudaSuccess) return BGPU_ERR_CUDA;
         launches += kNttLaunches;
     }
-    size_t bi = p->classes.size();
-    if (!p->school.empty()) {
+    size_t bi = p->mixed ? 0 : p->classes.size();
+    if (!p->school.empty() && !p->mixed) {
         const SchoolDesc* d_school = reinterpret_cast<const SchoolDesc*>(base + school_off);
         if (launch_schoolbook_batch(d_school, (uint32_t)p->school.size(), branches[bi++]) != cudaSuccess)
             return BGPU_ERR_CUDA;
         launches += 1;
     }
-    if (!p->kara.empty()) {
+    if (!p->kara.empty() && !p->mixed) {
         const SchoolDesc* d_kara = reinterpret_cast<const SchoolDesc*>(base + kara_off);
         if (launch_karatsuba_batch(d_kara, (uint32_t)p->kara.size(), branches[bi++]) != cudaSuccess)
             return BGPU_ERR_CUDA;
@@ -180,8 +205,12 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         }
         p->classes[it->second].members.push_back((uint32_t)i);
     }
-    // Layout: [ProductDesc...][SchoolDesc: schoolbook...][SchoolDesc: Karatsuba...]
-    //         [tickets][flags][scratch].
+    // Longest transforms first: in the mixed launches their CTAs, the longest
+    // of each pass, start in the first wave and the short ones fill the tail.
+    std::stable_sort(p->classes.begin(), p->classes.end(),
+                     [](const BatchClass& x, const BatchClass& y) { return x.log_n > y.log_n; });
+    // Layout: [ProductDesc...][MixedClass...][SchoolDesc: schoolbook...]
+    //         [SchoolDesc: Karatsuba...][tickets][flags][scratch].
     size_t n_desc = 0, flag_words = 0, scratch = 0;
     for (auto& c : p->classes) {
         c.desc_off = n_desc;
@@ -192,7 +221,14 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         c.scratch_off = scratch;
         scratch += c.members.size() * ntt_scratch_bytes(c.log_n, c.square);
     }
-    const size_t school_off = al256(n_desc * sizeof(ProductDesc));
+    // The mixed-length launches take every class when each qualifies.
+#ifndef BGPU_MIXED_BATCH
+#define BGPU_MIXED_BATCH 1
+#endif
+    p->mixed = BGPU_MIXED_BATCH && !p->classes.empty() && p->classes.size() <= (size_t)kMaxMixedClasses;
+    for (auto& c : p->classes) p->mixed = p->mixed && mixed_class_ok(c.log_n, c.square);
+    const size_t mixed_off = al256(n_desc * sizeof(ProductDesc));
+    const size_t school_off = mixed_off + al256((p->mixed ? p->classes.size() : 0) * sizeof(MixedClass));
     const size_t kara_off = school_off + al256(p->school.size() * sizeof(SchoolDesc));
     const size_t tick_off = kara_off + al256(p->kara.size() * sizeof(SchoolDesc));
     const size_t flags_base = tick_off + al256(std::max<size_t>(1, p->classes.size()) * 8);
@@ -225,6 +261,24 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         }
     }
     cudaError_t e = cudaMemcpy(base, descs.data(), n_desc * sizeof(ProductDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && p->mixed) {
+        std::vector<MixedClassSpec> spec(p->classes.size());
+        for (size_t i = 0; i < p->classes.size(); ++i) {
+            const BatchClass& c = p->classes[i];
+            spec[i] = MixedClassSpec{reinterpret_cast<const ProductDesc*>(base) + c.desc_off,
+                                     (uint32_t)c.members.size(), c.log_n, c.square};
+        }
+        std::vector<MixedClass> mc(p->classes.size());
+        if (mixed_fill(mc.data(), (int)mc.size(), spec.data(), kSlotEngine + 0, hooks.consts[0],
+                       &p->mixed_sizes) != 0) {
+            destroy_plan(p);
+            return BGPU_ERR_INVALID_ARG;
+        }
+        p->mixed_begin.resize(mc.size());
+        for (size_t i = 0; i < mc.size(); ++i)
+            for (int pass = 0; pass < 4; ++pass) p->mixed_begin[i][pass] = mc[i].begin[pass];
+        e = cudaMemcpy(base + mixed_off, mc.data(), mc.size() * sizeof(MixedClass), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess && !p->school.empty())
         e = cudaMemcpy(base + school_off, p->school.data(), p->school.size() * sizeof(SchoolDesc),
                        cudaMemcpyHostToDevice);
@@ -236,7 +290,8 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         return BGPU_ERR_CUDA;
     }
     // Capture the whole batch into one graph (streams and events made first).
-    const size_t nbranch = p->classes.size() + (p->school.empty() ? 0 : 1) + (p->kara.empty() ? 0 : 1);
+    const size_t nbranch = p->mixed ? 0 : p->classes.size() + (p->school.empty() ? 0 : 1) +
+                                              (p->kara.empty() ? 0 : 1);
     std::vector<cudaStream_t> branches(nbranch, nullptr);
     std::vector<cudaEvent_t> joins(nbranch, nullptr);
     cudaStream_t cap = nullptr;

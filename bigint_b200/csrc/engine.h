@@ -66,6 +66,94 @@ struct TransformShape {
     int log_n2;  // column length (outer passes)
 };
 
+// Small products, one CTA each (small_kernels.cu); out has na+nb limbs.
+struct SchoolDesc {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* out;
+    uint32_t na, nb;
+};
+constexpr uint32_t kSchoolbookMaxLimbs = 256;  // schoolbook: na + nb
+constexpr uint32_t kKaratsubaMaxLimbs = 256;   // Karatsuba: na and nb each
+
+// Per-launch argument blocks of the NTT passes: a device descriptor array
+// for batches, or the single product's descriptor inline (descs == nullptr).
+struct FwdColsArgs {
+    const ProductDesc* descs;
+    ProductDesc one;
+    int nops, log_n, log_n1, slot;
+    // 1: the operands and this pass's residue planes are free of the
+    // preceding kernel (its trigger came after the previous product's
+    // inverse pass finished), so the pass starts under that kernel's tail and
+    // waits for it only at the end -- which keeps every later kernel ordered
+    // after it, since each of them waits for this pass to complete
+    int overlap;
+};
+
+struct MidRowsArgs {
+    const ProductDesc* descs;  // y: A's planes (result in place), then B's unless squaring
+    ProductDesc one;
+    int log_n, log_n2, slot;
+    uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
+};
+
+struct InvColsArgs {
+    const ProductDesc* descs;  // y (A's planes after the middle pass), chunks, spill
+    ProductDesc one;
+    int log_n, log_n1, slot;
+};
+
+// A mixed-length batch (all its NTT classes in one launch per pass): one
+// class of products of equal transform length and squaring flag, with its
+// CTA range in each pass's launch (begin[3] is its first carry ticket).
+struct MixedClass {
+    FwdColsArgs fwd;
+    MidRowsArgs mid;
+    InvColsArgs inv;
+    uint32_t begin[4];
+    uint32_t tiles, rows, count;  // column tiles (N1 / 8), rows (N2), products
+    uint32_t nchunks, bpp;        // carry chunks and carry blocks per product
+    uint32_t mid_words;           // shared-memory words of one row in the row pass
+    int log_n1, log_n2, square;
+};
+constexpr int kMaxMixedClasses = 32;
+struct MixedArgs {
+    const MixedClass* classes;  // device array, in CTA-range order
+    int nclasses;
+    // each class's first CTA in each pass (carry: first ticket), kept in the
+    // launch's parameters so a CTA finds its class from the constant bank
+    uint32_t begin[4][kMaxMixedClasses];
+    unsigned long long* ticket;  // carry tickets of this launch, from ticket_base
+    uint64_t ticket_base;
+    uint64_t epoch;
+    uint32_t* err;
+    // small products of the same batch, one CTA each, ahead of the row
+    // pass's CTAs (schoolbook) and of the inverse pass's (Karatsuba)
+    const SchoolDesc* school;
+    uint32_t nschool;
+    const SchoolDesc* kara;
+    uint32_t nkara;
+};
+struct MixedClassSpec {
+    const ProductDesc* descs;  // device descriptors of the class's products
+    uint32_t count;
+    int log_n;
+    bool square;
+};
+struct MixedSizes {
+    uint32_t blocks[4];  // NTT CTAs of each pass's launch (carry: tickets)
+    size_t smem[4];      // dynamic shared memory of each launch's NTT CTAs
+};
+// A class the mixed launches can run (lazy prime set, column tiles of at most
+// 2^9 rows, rows of at most 2^9 points, at the batch split).
+bool mixed_class_ok(int log_n, bool square);
+// Fill the host copy of `nclasses` classes (descs already on the device) and
+// the launch sizes; -1 when a class does not qualify.
+int mixed_fill(MixedClass* classes, int nclasses, const MixedClassSpec* spec, int slot, const NttConsts& c,
+               MixedSizes* sizes);
+// The four launches of a mixed-length batch on `stream`.
+cudaError_t launch_ntt_mixed(const MixedArgs& m, const MixedSizes& sizes, cudaStream_t stream);
+
 TransformShape choose_shape(int log_n);        // the tuned split (bgpu_set_split), else the built-in one
 TransformShape choose_shape_batch(int log_n);  // batch classes (bgpu_set_batch_split), else built-in
 TransformShape builtin_shape(int log_n);       // the built-in split only
@@ -197,15 +285,6 @@ int product_tree_device(const uint64_t* d_leaves, size_t n, uint64_t* d_out, siz
                         const EngineHooks& hooks, TreeArena* arena, cudaStream_t st,
                         uint32_t* launches);
 
-// Small products, one CTA each (small_kernels.cu); out has na+nb limbs.
-struct SchoolDesc {
-    const uint64_t* a;
-    const uint64_t* b;
-    uint64_t* out;
-    uint32_t na, nb;
-};
-constexpr uint32_t kSchoolbookMaxLimbs = 256;  // schoolbook: na + nb
-constexpr uint32_t kKaratsubaMaxLimbs = 256;   // Karatsuba: na and nb each
 cudaError_t launch_schoolbook(const uint64_t* a, uint32_t na, const uint64_t* b, uint32_t nb,
                               uint64_t* out, cudaStream_t stream);
 cudaError_t launch_schoolbook_batch(const SchoolDesc* d_descs, uint32_t count, cudaStream_t stream);

@@ -24,8 +24,11 @@
 // (arith.cuh): set 0 uses lazy butterflies, set 1 strict ones.
 #include <cuda/atomic>
 
+#include <algorithm>
+
 #include "engine.h"
 #include "pass_common.cuh"
+#include "small_bodies.cuh"
 
 namespace bgpu {
 
@@ -178,19 +181,6 @@ __device__ __forceinline__ uint32_t bitrev(uint32_t v, int bits) {
 
 // ---- kernel 1: forward column pass ------------------------------------------
 
-// Per-launch argument blocks: a device descriptor array for batches, or the
-// single product's descriptor inline (descs == nullptr).
-struct FwdColsArgs {
-    const ProductDesc* descs;
-    ProductDesc one;
-    int nops, log_n, log_n1, slot;
-    // 1: the operands and this pass's residue planes are free of the
-    // preceding kernel (its trigger came after the previous product's
-    // inverse pass finished), so the pass starts under that kernel's tail and
-    // waits for it only at the end -- which keeps every later kernel ordered
-    // after it, since each of them waits for this pass to complete
-    int overlap;
-};
 
 // Returned by value: binding a reference to the kernel parameter would force
 // a copy of it into local memory.
@@ -298,19 +288,21 @@ __host__ __device__ constexpr int fwd_min_blocks(int l2, int threads) {
     return (l2 == 9 && threads == 256) ? 8 : 1;
 }
 
+// The forward column pass of one CTA: tile bx, prime by, operand and product
+// bz (block coordinates passed in, so a mixed-length launch can run it too).
 template <int PS, int L2, int T>
-__global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const FwdColsArgs a) {
+__device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx, uint32_t by, uint32_t bz,
+                                              uint32_t* sm) {  // sm: [2^L2][kCols] + column powers
     constexpr bool LAZY = PS == 0;
-    extern __shared__ __align__(16) uint32_t sm[];  // [2^L2][kCols]
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
     const NttConsts& c = c_consts[a.slot];
-    const int q = blockIdx.y, opi = blockIdx.z % a.nops;
-    const ProductDesc pd = product(a.descs, a.one, blockIdx.z / a.nops);
+    const int q = (int)by, opi = (int)(bz % (uint32_t)a.nops);
+    const ProductDesc pd = product(a.descs, a.one, bz / (uint32_t)a.nops);
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
     const OperandDesc in = opi == 0 ? pd.op[0] : pd.op[1];
-    const uint32_t c0 = blockIdx.x * kCols;
+    const uint32_t c0 = bx * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     uint32_t* y = pd.y + ((size_t)opi * kNumPrimes + q) * nn;
 
@@ -376,14 +368,14 @@ __global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const Fwd
     if (a.overlap) pdl_wait();
 }
 
+template <int PS, int L2, int T>
+__global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const __grid_constant__ FwdColsArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    fwd_cols_body<PS, L2, T>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm);
+}
+
 // ---- kernel 2: middle row pass ----------------------------------------------
 
-struct MidRowsArgs {
-    const ProductDesc* descs;  // y: A's planes (result in place), then B's unless squaring
-    ProductDesc one;
-    int log_n, log_n2, slot;
-    uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
-};
 
 // a*b*2^-32 mod p in [0, p); the 2^-32 and the inverse transform's N^-1 are
 // both cancelled by the scale N^-1 * 2^32 folded into the row's inverse
@@ -403,12 +395,22 @@ __device__ __forceinline__ uint32_t pointwise(uint32_t a, uint32_t b, uint32_t p
 template <int L1, bool SQR>
 constexpr bool kOneRowBuffer = !SQR && L1 >= 15;
 
+// Thread number within a row's group of T threads: the CTA's own thread
+// number when the CTA is one group (MULTI false: the compiler re-reads it
+// instead of holding a computed copy in a register), else the position in
+// its group (a CTA holding several rows of a mixed-length launch).
+template <int T, bool MULTI>
+__device__ __forceinline__ int sub_tid() {
+    return MULTI ? (int)(threadIdx.x & (T - 1)) : (int)threadIdx.x;
+}
+
 // Last DIF round of B (or A when squaring) fused with the pointwise product
 // and the first DIT round; with a single round also the inverse twiddle.
-template <bool LAZY, int L1, int T, bool SQR, bool SINGLE>
+template <bool LAZY, int L1, int T, bool SQR, bool SINGLE, bool MULTI>
 __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& c, uint32_t* sa,
                                          uint32_t* sb, const uint32_t* row_a, const uint32_t* row_b,
                                          uint32_t* row_out, int q, uint32_t k2, const uint2* sT) {
+    const int tid = sub_tid<T, MULTI>();
     constexpr bool ONE = kOneRowBuffer<L1, SQR>;
     using P1 = Plan<L1>;
     constexpr int K = P1::nr - 1;
@@ -421,7 +423,7 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
     const uint32_t swp = q == 0 ? a.scale_wp[0] : (q == 1 ? a.scale_wp[1] : a.scale_wp[2]);
     const uint32_t* src = (SQR || ONE) ? sa : sb;
 #pragma unroll 1
-    for (int g = threadIdx.x; g < Gr::G; g += T) {
+    for (int g = tid; g < Gr::G; g += T) {
         const Gr gr(g);
         uint32_t x[1 << R];
 #pragma unroll
@@ -452,14 +454,15 @@ __device__ __forceinline__ void mid_turn(const MidRowsArgs& a, const NttConsts& 
 
 // DIF of one row: round 0 from global into smem, then rounds 1..nr-2 (the
 // last round is done by mid_turn).
-template <bool LAZY, int L1, int T>
+template <bool LAZY, int L1, int T, bool MULTI>
 __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, const uint2* twf,
                                             uint32_t p) {
+    const int tid = sub_tid<T, MULTI>();
     using P1 = Plan<L1>;
     using Gr = Group<L1, 1, 0>;
     constexpr int R = Gr::R;
 #pragma unroll 2
-    for (int g = threadIdx.x; g < Gr::G; g += T) {
+    for (int g = tid; g < Gr::G; g += T) {
         const Gr gr(g);
         uint32_t x[1 << R];
 #pragma unroll
@@ -469,23 +472,27 @@ __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, co
         for (int j = 0; j < (1 << R); ++j) s[gr.at(j)] = x[j];
     }
     __syncthreads();
-    dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p, threadIdx.x);
+    dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p, tid);
 }
 
-template <int PS, int L1, int T, bool SQR>
-__global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const MidRowsArgs a) {
+// The row pass of one row: row slot `slot`, prime and product from `by`
+// (prime + 3 * product), run by T threads on the shared slice `sm`; every
+// thread of the CTA takes the same barriers, so a CTA may hold several rows
+// of the same length side by side (MULTI).
+template <int PS, int L1, int T, bool SQR, bool MULTI = false>
+__device__ __forceinline__ void mid_rows_body(const MidRowsArgs& a, uint32_t slot, uint32_t by,
+                                              uint32_t* sm) {  // sm: sa[2^L1] (+ sb[2^L1]) + powers
     constexpr bool LAZY = PS == 0;
     constexpr bool ONE = kOneRowBuffer<L1, SQR>;
-    extern __shared__ __align__(16) uint32_t sm[];  // sa[2^L1] (+ sb[2^L1] unless SQR or ONE)
+    const int tid = sub_tid<T, MULTI>();
     using P1 = Plan<L1>;
     constexpr int NR = P1::nr;
     static_assert(!ONE || NR > 1, "the one-buffer row pass needs several rounds");
     const NttConsts& c = c_consts[a.slot];
     uint32_t* sa = sm;
     uint32_t* sb = sm + (1u << L1);
-    const int q = blockIdx.y % kNumPrimes;
-    const ProductDesc pd = product(a.descs, a.one, blockIdx.y / kNumPrimes);
-    const uint32_t slot = blockIdx.x;
+    const int q = (int)(by % kNumPrimes);
+    const ProductDesc pd = product(a.descs, a.one, by / kNumPrimes);
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* twf = c.stage[q][0];
     const uint2* twi = c.stage[q][1];
@@ -501,7 +508,7 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
     // powers sT[j] = omega_N^-(k2 j << LO0).
     constexpr int R0 = P1::r(0), LO0 = P1::lo(0);
     uint2* sT = reinterpret_cast<uint2*>(sm + ((SQR || ONE ? 1u : 2u) << L1));
-    for (int t = threadIdx.x; t < (1 << R0); t += T) {
+    for (int t = tid; t < (1 << R0); t += T) {
         const uint32_t w = inter_twiddle(c, q, 1, ((k2 * (uint32_t)t) << LO0) & (uint32_t)(nn - 1),
                                          a.log_n, p);
         sT[t] = make_uint2(w, w * pinv);
@@ -514,7 +521,7 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
             using Gr = Group<L1, 1, 0>;
             constexpr int R = Gr::R;
 #pragma unroll 1
-            for (int g = threadIdx.x; g < Gr::G; g += T) {
+            for (int g = tid; g < Gr::G; g += T) {
                 const Gr gr(g);
                 uint32_t x[1 << R];
 #pragma unroll
@@ -525,29 +532,29 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
             }
             __syncthreads();
         }
-        mid_turn<LAZY, L1, T, SQR, true>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
+        mid_turn<LAZY, L1, T, SQR, true, MULTI>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
     } else {
-        mid_dif_row<LAZY, L1, T>(row_a, sa, twf, p);
+        mid_dif_row<LAZY, L1, T, MULTI>(row_a, sa, twf, p);
         if constexpr (ONE) {
-            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, threadIdx.x);  // A's last DIF round
+            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, tid);  // A's last DIF round
             __syncthreads();
             // park A's transform in its plane (element i at row_a[i]) ...
-            for (uint32_t i = threadIdx.x; i < (1u << L1); i += T) row_a[i] = sa[sidx<1>(i, 0)];
+            for (uint32_t i = tid; i < (1u << L1); i += T) row_a[i] = sa[sidx<1>(i, 0)];
             __syncthreads();
             // ... and transform B in the same buffer
-            mid_dif_row<LAZY, L1, T>(row_b, sa, twf, p);
+            mid_dif_row<LAZY, L1, T, MULTI>(row_b, sa, twf, p);
         } else if constexpr (!SQR) {
-            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, threadIdx.x);  // A's last DIF round
-            mid_dif_row<LAZY, L1, T>(row_b, sb, twf, p);
+            smem_round<LAZY, L1, 1, T, NR - 1, false>(sa, twf, p, tid);  // A's last DIF round
+            mid_dif_row<LAZY, L1, T, MULTI>(row_b, sb, twf, p);
         }
-        mid_turn<LAZY, L1, T, SQR, false>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
+        mid_turn<LAZY, L1, T, SQR, false, MULTI>(a, c, sa, sb, row_a, row_b, row_a, q, k2, sT);
         __syncthreads();
-        dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sa, twi, p, threadIdx.x);
+        dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sa, twi, p, tid);
         // Round 0 (top bits): DIT, inverse twiddle, store to global.
         using Gr = Group<L1, 1, 0>;
         constexpr int R = Gr::R;
 #pragma unroll 2
-        for (int g = threadIdx.x; g < Gr::G; g += T) {
+        for (int g = tid; g < Gr::G; g += T) {
             const Gr gr(g);
             uint32_t x[1 << R];
 #pragma unroll
@@ -564,13 +571,14 @@ __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const Mid
     pdl_trigger();  // late, as in the column pass
 }
 
+template <int PS, int L1, int T, bool SQR>
+__global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const __grid_constant__ MidRowsArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    mid_rows_body<PS, L1, T, SQR>(a, blockIdx.x, blockIdx.y, sm);
+}
+
 // ---- kernel 3: inverse column pass + CRT + chunk sums -------------------------
 
-struct InvColsArgs {
-    const ProductDesc* descs;  // y (A's planes after the middle pass), chunks, spill
-    ProductDesc one;
-    int log_n, log_n1, slot;
-};
 
 // Garner: residues (r0,r1,r2), each in [0, p_q) -> the coefficient as 96 bits.
 __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r1, uint32_t r2,
@@ -597,21 +605,22 @@ __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r
 
 constexpr int kInvUnroll = BGPU_INV_UNROLL;  // groups of the first (global-memory) round in flight per thread
 
+// The inverse column pass of one CTA: tile bx of product by.  Three thread
+// groups of TP threads, one per prime, transform their prime's column tile
+// side by side; then all threads do the CRT.
 template <int PS, int L2, int TP>
-__global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs a) {
-    // Three thread groups of TP threads, one per prime, transform their
-    // prime's column tile side by side; then all threads do the CRT.
+__device__ __forceinline__ void inv_cols_body(const InvColsArgs& a, uint32_t bx, uint32_t by,
+                                              uint32_t* sm) {  // sm: 3 x [2^L2][kCols]
     constexpr bool LAZY = PS == 0;
     constexpr int T = kNumPrimes * TP;
-    extern __shared__ __align__(16) uint32_t sm[];  // 3 x [2^L2][kCols]
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
     constexpr int TILE = kCols << L2;
     const NttConsts& c = c_consts[a.slot];
-    const uint32_t n1_len = 1u << a.log_n1, c0 = blockIdx.x * kCols;
+    const uint32_t n1_len = 1u << a.log_n1, c0 = bx * kCols;
     const size_t nn = (size_t)1 << a.log_n;
     const int q = threadIdx.x / TP, tq = threadIdx.x % TP;
-    const ProductDesc pd = product(a.descs, a.one, blockIdx.y);
+    const ProductDesc pd = product(a.descs, a.one, by);
     uint32_t* s = sm + q * TILE;
     const uint32_t p = c.pr[q].p;
     const uint2* twi = c.stage[q][1];
@@ -695,6 +704,12 @@ __global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs 
     }
 }
 
+template <int PS, int L2, int TP>
+__global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const __grid_constant__ InvColsArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    inv_cols_body<PS, L2, TP>(a, blockIdx.x, blockIdx.y, sm);
+}
+
 // ---- kernel 4: carry scan with decoupled look-back ----------------------------
 
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded look-back wait, then error exit
@@ -758,28 +773,18 @@ cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t 
 // 64-bit add of the (G, P) ballots; segments are chained inside the warp,
 // warps by a fold in shared memory, and blocks by a decoupled look-back in
 // ticket order.
-__global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
-    __shared__ uint32_t s_bid, s_cin;
+// Block `bid` of one product's carry scan over `nchunks` chunks, writing the
+// output in `out_fmt`; blocks of the same product must hold increasing
+// tickets of one launch (their look-back waits only on earlier blocks).
+__device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid, uint32_t nchunks, int out_fmt,
+                                            uint64_t epoch, uint32_t* err) {
+    __shared__ uint32_t s_cin;
     __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
-    if (threadIdx.x == 0) s_bid = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticket_base);
-    __syncthreads();
-    pdl_wait();
-    pdl_trigger();
-    // A ticket outside this launch means the host's ticket base and the
-    // counter disagree (an earlier launch that never ran): report, touch nothing.
-    if (s_bid >= gridDim.x) {
-        if (threadIdx.x == 0) atomicOr(a.err, 2u);
-        return;
-    }
-    // tickets enumerate (product, block) in order, so a block's predecessor
-    // within its product always holds a smaller ticket
-    const ProductDesc pd = product(a.descs, a.one, s_bid / a.bpp);
-    const uint32_t bid = s_bid % a.bpp;
     const uint64_t* chunks = pd.chunks;
     const uint64_t* spill = pd.spill;
     uint64_t* flags = pd.flags;
     const size_t out_cap = pd.out_cap;
-    const uint32_t ntot = a.nchunks + 1;
+    const uint32_t ntot = nchunks + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t wbase = (bid * kCarryThreads + (uint32_t)warp * 32) * kCarryPer;
 
@@ -788,14 +793,14 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
 #pragma unroll
     for (int i = 0; i < kCarryPer; ++i) {
         const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
-        if (cc < a.nchunks) {
+        if (cc < nchunks) {
             const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)cc * 4);
             const ulonglong2 u = src[0], v = src[1];
             S[i][0] = u.x, S[i][1] = u.y, S[i][2] = v.x, S[i][3] = v.y;
         } else {
             S[i][0] = S[i][1] = S[i][2] = S[i][3] = 0;
         }
-        sp[i] = (cc >= 1 && cc - 1 < a.nchunks) ? spill[cc - 1] : 0;
+        sp[i] = (cc >= 1 && cc - 1 < nchunks) ? spill[cc - 1] : 0;
     }
     // per-chunk (G, P) and per-segment ballots
     uint32_t gm[kCarryPer], bm[kCarryPer];
@@ -840,12 +845,12 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> self(
             *reinterpret_cast<unsigned long long*>(flags + bid));
         if (bid == 0) {
-            self.store(make_flag(a.epoch, 2, bG, 0), cuda::memory_order_release);
+            self.store(make_flag(epoch, 2, bG, 0), cuda::memory_order_release);
         } else {
-            self.store(make_flag(a.epoch, 1, bG, bP), cuda::memory_order_release);
+            self.store(make_flag(epoch, 1, bG, bP), cuda::memory_order_release);
             int k = (int)bid - 1;
             while (true) {
-                const uint64_t f = wait_flag(flags + k, a.epoch, kSpinLimit, a.err);
+                const uint64_t f = wait_flag(flags + k, epoch, kSpinLimit, err);
                 if (f == 0) break;  // gave up: error recorded, carry taken as 0
                 const uint32_t st = (uint32_t)(f >> 2) & 3u, fg = (uint32_t)(f >> 1) & 1u,
                                fp = (uint32_t)f & 1u;
@@ -863,7 +868,7 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
                 }
                 --k;  // predecessor propagates: look further back (block 0 is inclusive)
             }
-            self.store(make_flag(a.epoch, 2, bG | (bP & cin), 0), cuda::memory_order_release);
+            self.store(make_flag(epoch, 2, bG | (bP & cin), 0), cuda::memory_order_release);
         }
         s_cin = cin;
     }
@@ -887,7 +892,7 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
             S[i][k] = t;
         }
     }
-    if (a.out_fmt == kFmtLimb64) {
+    if (out_fmt == kFmtLimb64) {
         uint64_t* o = static_cast<uint64_t*>(pd.out);
         const bool vec = (reinterpret_cast<uintptr_t>(o) & 15u) == 0;  // 16-byte stores when aligned
 #pragma unroll
@@ -918,8 +923,8 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
         for (int i = 0; i < kCarryPer; ++i) {
             const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
             if (cc >= ntot) continue;
-            uint64_t nl = (cc + 1 < a.nchunks) ? chunks[(size_t)(cc + 1) * 4] : 0;
-            nl += (cc < a.nchunks ? spill[cc] : 0) + cout[i];
+            uint64_t nl = (cc + 1 < nchunks) ? chunks[(size_t)(cc + 1) * 4] : 0;
+            nl += (cc < nchunks ? spill[cc] : 0) + cout[i];
             const uint64_t bit0 = (uint64_t)cc * 256;
             uint64_t k = (bit0 + 27) / 28;
             const uint64_t kend = min((bit0 + 256 + 27) / 28, (uint64_t)out_cap);
@@ -942,6 +947,23 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
+    __shared__ uint32_t s_bid;
+    if (threadIdx.x == 0) s_bid = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticket_base);
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+    // A ticket outside this launch means the host's ticket base and the
+    // counter disagree (an earlier launch that never ran): report, touch nothing.
+    if (s_bid >= gridDim.x) {
+        if (threadIdx.x == 0) atomicOr(a.err, 2u);
+        return;
+    }
+    // tickets enumerate (product, block) in order, so a block's predecessor
+    // within its product always holds a smaller ticket
+    carry_block(product(a.descs, a.one, s_bid / a.bpp), s_bid % a.bpp, a.nchunks, a.out_fmt, a.epoch, a.err);
 }
 
 // ---- host launchers -------------------------------------------------------------
@@ -1093,6 +1115,21 @@ uint32_t carry_blocks(uint32_t nchunks) {
 
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
 
+// The row pass's scale per prime: the pointwise Montgomery product leaves a
+// factor 2^-32; the scale N^-1 * 2^32 (mod p) cancels it and applies the
+// inverse's 1/N (Montgomery pairs).
+static void set_scale(const NttConsts& c, int log_n, uint32_t* w, uint32_t* wp) {
+    for (int q = 0; q < kNumPrimes; ++q) {
+        const uint32_t p = c.pr[q].p;
+        uint64_t ninv = 1, base = (p + 1) / 2;  // 2^-1 mod p
+        for (int i = 0; i < log_n; ++i) ninv = ninv * base % p;
+        const uint64_t r = ((uint64_t)1 << 32) % p;
+        const uint64_t v = ninv * r % p;
+        w[q] = mont_of(v, p);
+        wp[q] = w[q] * c.pr[q].pinv;
+    }
+}
+
 // The four launches of `count` products (descs on the device, or `one`).
 static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDesc* descs,
                                    const ProductDesc& one, int count, bool square,
@@ -1124,17 +1161,7 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
     m.log_n = log_n;
     m.log_n2 = sh.log_n2;
     m.slot = slot;
-    for (int q = 0; q < kNumPrimes; ++q) {
-        const uint32_t p = c.pr[q].p;
-        // The pointwise Montgomery product leaves a factor 2^-32; the scale
-        // N^-1 * 2^32 (mod p) cancels it and applies the inverse's 1/N.
-        uint64_t ninv = 1, base = (p + 1) / 2;  // 2^-1 mod p
-        for (int i = 0; i < log_n; ++i) ninv = ninv * base % p;
-        const uint64_t r = ((uint64_t)1 << 32) % p;
-        const uint64_t v = ninv * r % p;
-        m.scale_w[q] = mont_of(v, p);
-        m.scale_wp[q] = m.scale_w[q] * c.pr[q].pinv;
-    }
+    set_scale(c, log_n, m.scale_w, m.scale_wp);
     e = ps == 0 ? dispatch_mid<0>(sh.log_n1, m, square, 1u << sh.log_n2, count, st)
                 : dispatch_mid<1>(sh.log_n1, m, square, 1u << sh.log_n2, count, st);
     if (e != cudaSuccess) return e;
@@ -1222,6 +1249,211 @@ cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t
     ca.epoch = cl.epoch;
     ca.err = s.err;
     return launch_k(k_carry, dim3(ca.bpp), dim3(kCarryThreads), 0, st, ca);
+}
+
+// ---- mixed-length batches: one launch per pass for every class -------------
+//
+// A batch of products of several transform lengths runs as four launches in
+// all, one per pass, instead of four per length: each CTA finds its class
+// (the classes' CTA ranges are consecutive, their first CTAs kept in the
+// launch parameters) and runs that class's pass body with block coordinates
+// computed from its place in the range.  The row pass packs 128 / T rows of T
+// threads into one 128-thread CTA.  The carry scan takes one ticket sequence
+// over all classes; a product's blocks hold consecutive tickets.  The small
+// products of the batch ride along as CTAs of their own ahead of the row pass
+// (schoolbook, 128 threads) and the inverse pass (Karatsuba, 384 threads),
+// with their shared memory carved from the launch's dynamic buffer; they wait
+// on nothing.  Classes qualify when they use the lazy prime set, column tiles
+// of at most 2^9 rows and rows of at most 2^9 points (mixed_class_ok), which
+// keeps each launch's registers near the per-length kernels'.
+
+constexpr int kMixedMidThreads = 128;
+// Register budgets of the mixed launches (each holds every length's body):
+// 6 forward CTAs of 256 threads per SM (40 registers), 7 row CTAs of 128
+// threads (72 registers, what a 2^9-point row takes on its own).
+#ifndef BGPU_MIXED_FWD_MINB
+#define BGPU_MIXED_FWD_MINB 6
+#endif
+#ifndef BGPU_MIXED_MID_MINB
+#define BGPU_MIXED_MID_MINB 7
+#endif
+
+__device__ __forceinline__ int mixed_class(const MixedArgs& m, int pass, uint32_t b) {
+    int c = 0;
+    while (c + 1 < m.nclasses && m.begin[pass][c + 1] <= b) ++c;
+    return c;
+}
+
+__global__ void __launch_bounds__(256, BGPU_MIXED_FWD_MINB) k_mixed_fwd(const __grid_constant__ MixedArgs m) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    const MixedClass& k = m.classes[mixed_class(m, 0, blockIdx.x)];
+    const uint32_t local = blockIdx.x - k.begin[0];
+    const uint32_t bx = local % k.tiles, rest = local / k.tiles;
+    const uint32_t by = rest % kNumPrimes, bz = rest / kNumPrimes;
+    switch (k.log_n2) {
+        case 2: fwd_cols_body<0, 2, 256>(k.fwd, bx, by, bz, sm); break;
+        case 3: fwd_cols_body<0, 3, 256>(k.fwd, bx, by, bz, sm); break;
+        case 4: fwd_cols_body<0, 4, 256>(k.fwd, bx, by, bz, sm); break;
+        case 5: fwd_cols_body<0, 5, 256>(k.fwd, bx, by, bz, sm); break;
+        case 6: fwd_cols_body<0, 6, 256>(k.fwd, bx, by, bz, sm); break;
+        case 7: fwd_cols_body<0, 7, 256>(k.fwd, bx, by, bz, sm); break;
+        case 8: fwd_cols_body<0, 8, 256>(k.fwd, bx, by, bz, sm); break;
+        default: fwd_cols_body<0, 9, 256>(k.fwd, bx, by, bz, sm); break;
+    }
+}
+
+template <int L1, bool SQR>
+__device__ __forceinline__ void mixed_mid_row(const MixedClass& k, uint32_t local, uint32_t* sm) {
+    constexpr int T = mid_threads(L1);
+    constexpr int RPC = kMixedMidThreads / T;  // rows per CTA
+    const uint32_t sub = threadIdx.x / T;
+    const uint32_t row = local * RPC + sub;
+    mid_rows_body<0, L1, T, SQR, (RPC > 1)>(k.mid, row % k.rows, row / k.rows, sm + sub * k.mid_words);
+}
+
+template <bool SQR>
+__device__ __forceinline__ void mixed_mid_len(const MixedClass& k, uint32_t local, uint32_t* sm) {
+    switch (k.log_n1) {
+        case 3: mixed_mid_row<3, SQR>(k, local, sm); break;
+        case 4: mixed_mid_row<4, SQR>(k, local, sm); break;
+        case 5: mixed_mid_row<5, SQR>(k, local, sm); break;
+        case 6: mixed_mid_row<6, SQR>(k, local, sm); break;
+        case 7: mixed_mid_row<7, SQR>(k, local, sm); break;
+        case 8: mixed_mid_row<8, SQR>(k, local, sm); break;
+        default: mixed_mid_row<9, SQR>(k, local, sm); break;
+    }
+}
+
+static_assert(kSbThreads == kMixedMidThreads, "schoolbook CTAs ride in the mixed row pass");
+
+__global__ void __launch_bounds__(kMixedMidThreads, BGPU_MIXED_MID_MINB)
+    k_mixed_mid(const __grid_constant__ MixedArgs m) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    if (blockIdx.x < m.nschool) {  // a schoolbook product: no wait on the column pass
+        schoolbook_body(m.school[blockIdx.x], *reinterpret_cast<SbSmem*>(sm));
+        return;
+    }
+    const uint32_t b = blockIdx.x - m.nschool;
+    const MixedClass& k = m.classes[mixed_class(m, 1, b)];
+    const uint32_t local = b - k.begin[1];
+    if (k.square)
+        mixed_mid_len<true>(k, local, sm);
+    else
+        mixed_mid_len<false>(k, local, sm);
+}
+
+static_assert(kKaThreads == kNumPrimes * 128, "Karatsuba CTAs ride in the mixed inverse pass");
+
+__global__ void __launch_bounds__(kNumPrimes * 128) k_mixed_inv(const __grid_constant__ MixedArgs m) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    if (blockIdx.x < m.nkara) {  // a Karatsuba product: no wait on the row pass
+        karatsuba_body(m.kara[blockIdx.x], *reinterpret_cast<KaSmem*>(sm));
+        return;
+    }
+    const uint32_t b = blockIdx.x - m.nkara;
+    const MixedClass& k = m.classes[mixed_class(m, 2, b)];
+    const uint32_t local = b - k.begin[2];
+    const uint32_t bx = local % k.tiles, by = local / k.tiles;
+    switch (k.log_n2) {
+        case 2: inv_cols_body<0, 2, 128>(k.inv, bx, by, sm); break;
+        case 3: inv_cols_body<0, 3, 128>(k.inv, bx, by, sm); break;
+        case 4: inv_cols_body<0, 4, 128>(k.inv, bx, by, sm); break;
+        case 5: inv_cols_body<0, 5, 128>(k.inv, bx, by, sm); break;
+        case 6: inv_cols_body<0, 6, 128>(k.inv, bx, by, sm); break;
+        case 7: inv_cols_body<0, 7, 128>(k.inv, bx, by, sm); break;
+        case 8: inv_cols_body<0, 8, 128>(k.inv, bx, by, sm); break;
+        default: inv_cols_body<0, 9, 128>(k.inv, bx, by, sm); break;
+    }
+}
+
+__global__ void __launch_bounds__(kCarryThreads) k_mixed_carry(const __grid_constant__ MixedArgs m) {
+    __shared__ uint32_t s_t;
+    if (threadIdx.x == 0) s_t = (uint32_t)(atomicAdd(m.ticket, 1ull) - m.ticket_base);
+    __syncthreads();
+    pdl_wait();
+    pdl_trigger();
+    if (s_t >= gridDim.x) {  // the ticket counter and the launch disagree: report, touch nothing
+        if (threadIdx.x == 0) atomicOr(m.err, 2u);
+        return;
+    }
+    const MixedClass& k = m.classes[mixed_class(m, 3, s_t)];
+    const uint32_t local = s_t - k.begin[3];
+    carry_block(k.fwd.descs[local / k.bpp], local % k.bpp, k.nchunks, kFmtLimb64, m.epoch, m.err);
+}
+
+bool mixed_class_ok(int log_n, bool square) {
+    const TransformShape sh = choose_shape_batch(log_n);
+    return shape_ok(sh, square) && prime_set_for(log_n) == 0 && sh.log_n2 <= 9 && sh.log_n1 <= 9;
+}
+
+int mixed_fill(MixedClass* classes, int nclasses, const MixedClassSpec* spec, int slot, const NttConsts& c,
+               MixedSizes* sizes) {
+    if (nclasses > kMaxMixedClasses) return -1;
+    uint32_t at[4] = {0, 0, 0, 0};
+    size_t sm_fwd = 0, sm_mid = 0, sm_inv = 0;
+    for (int i = 0; i < nclasses; ++i) {
+        const MixedClassSpec& sp = spec[i];
+        if (!mixed_class_ok(sp.log_n, sp.square)) return -1;
+        const TransformShape sh = choose_shape_batch(sp.log_n);
+        MixedClass& k = classes[i];
+        k = MixedClass{};
+        const int nops = sp.square ? 1 : 2;
+        k.fwd.descs = sp.descs;
+        k.fwd.nops = nops;
+        k.fwd.log_n = sp.log_n;
+        k.fwd.log_n1 = sh.log_n1;
+        k.fwd.slot = slot;
+        k.mid.descs = sp.descs;
+        k.mid.log_n = sp.log_n;
+        k.mid.log_n2 = sh.log_n2;
+        k.mid.slot = slot;
+        set_scale(c, sp.log_n, k.mid.scale_w, k.mid.scale_wp);
+        k.inv.descs = sp.descs;
+        k.inv.log_n = sp.log_n;
+        k.inv.log_n1 = sh.log_n1;
+        k.inv.slot = slot;
+        k.tiles = (1u << sh.log_n1) / kCols;
+        k.rows = 1u << sh.log_n2;
+        k.count = sp.count;
+        k.log_n1 = sh.log_n1;
+        k.log_n2 = sh.log_n2;
+        k.square = sp.square ? 1 : 0;
+        k.nchunks = (uint32_t)(((size_t)1 << sp.log_n) / kCols);
+        k.bpp = carry_blocks(k.nchunks);
+        const uint32_t rpc = kMixedMidThreads / (uint32_t)mid_threads(sh.log_n1);
+        const size_t row_bytes = (smem_mid_rows(sh.log_n1, sp.square) + 15) & ~(size_t)15;
+        k.mid_words = (uint32_t)(row_bytes / 4);
+        for (int pass = 0; pass < 4; ++pass) k.begin[pass] = at[pass];
+        at[0] += k.tiles * kNumPrimes * nops * sp.count;
+        at[1] += k.rows * kNumPrimes * sp.count / rpc;
+        at[2] += k.tiles * sp.count;
+        at[3] += k.bpp * sp.count;
+        sm_fwd = std::max(sm_fwd, smem_fwd_cols(sh.log_n2));
+        sm_mid = std::max(sm_mid, rpc * row_bytes);
+        sm_inv = std::max(sm_inv, smem_inv_cols(sh.log_n2));
+    }
+    for (int pass = 0; pass < 4; ++pass) sizes->blocks[pass] = at[pass];
+    sizes->smem[0] = sm_fwd;
+    sizes->smem[1] = sm_mid;
+    sizes->smem[2] = sm_inv;
+    sizes->smem[3] = 0;
+    return 0;
+}
+
+cudaError_t launch_ntt_mixed(const MixedArgs& m, const MixedSizes& sz, cudaStream_t st) {
+    if (m.nclasses < 1) return cudaErrorInvalidValue;
+    allow_smem(k_mixed_fwd, sz.smem[0]);
+    cudaError_t e = launch_k(k_mixed_fwd, dim3(sz.blocks[0]), dim3(256), sz.smem[0], st, m);
+    if (e != cudaSuccess) return e;
+    const size_t sm_mid = std::max(sz.smem[1], m.nschool ? sizeof(SbSmem) : (size_t)0);
+    allow_smem(k_mixed_mid, sm_mid);
+    e = launch_k(k_mixed_mid, dim3(sz.blocks[1] + m.nschool), dim3(kMixedMidThreads), sm_mid, st, m);
+    if (e != cudaSuccess) return e;
+    const size_t sm_inv = std::max(sz.smem[2], m.nkara ? sizeof(KaSmem) : (size_t)0);
+    allow_smem(k_mixed_inv, sm_inv);
+    e = launch_k(k_mixed_inv, dim3(sz.blocks[2] + m.nkara), dim3(kNumPrimes * 128), sm_inv, st, m);
+    if (e != cudaSuccess) return e;
+    return launch_k(k_mixed_carry, dim3(sz.blocks[3]), dim3(kCarryThreads), 0, st, m);
 }
 
 const char* const kNttKernelNames[kNttLaunches] = {"k_fwd_cols", "k_mid_rows", "k_inv_cols",
