@@ -127,12 +127,13 @@ struct MixedArgs {
     uint64_t ticket_base;
     uint64_t epoch;
     uint32_t* err;
-    // small products of the same batch, one CTA each, ahead of the row
-    // pass's CTAs (schoolbook) and of the inverse pass's (Karatsuba)
+    // small products of the same batch, one CTA each, after the row pass's
+    // CTAs (schoolbook) and the inverse pass's (Karatsuba)
     const SchoolDesc* school;
     uint32_t nschool;
     const SchoolDesc* kara;
     uint32_t nkara;
+    uint32_t ntt_blocks[4];  // the NTT CTAs of each pass (small products follow them)
 };
 struct MixedClassSpec {
     const ProductDesc* descs;  // device descriptors of the class's products

@@ -1260,8 +1260,9 @@ cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t
 // computed from its place in the range.  The row pass packs 128 / T rows of T
 // threads into one 128-thread CTA.  The carry scan takes one ticket sequence
 // over all classes; a product's blocks hold consecutive tickets.  The small
-// products of the batch ride along as CTAs of their own ahead of the row pass
-// (schoolbook, 128 threads) and the inverse pass (Karatsuba, 384 threads),
+// products of the batch ride along as CTAs of their own after those of the
+// row pass (schoolbook, 128 threads) and the inverse pass (Karatsuba, 384
+// threads), filling the passes' last waves,
 // with their shared memory carved from the launch's dynamic buffer; they wait
 // on nothing.  Classes qualify when they use the lazy prime set, column tiles
 // of at most 2^9 rows and rows of at most 2^9 points (mixed_class_ok), which
@@ -1269,10 +1270,12 @@ cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t
 
 constexpr int kMixedMidThreads = 128;
 // Register budgets of the mixed launches (each holds every length's body):
-// 6 forward CTAs of 256 threads per SM (40 registers), 7 row CTAs of 128
-// threads (72 registers, what a 2^9-point row takes on its own).
+// 7 forward CTAs of 256 threads per SM (32 registers, some spilled; measured
+// on the 4096-product batch: 10.71 ms against 10.88 ms at 40 registers and 6
+// CTAs), 7 row CTAs of 128 threads (72 registers, what a 2^9-point row takes
+// on its own; 6 CTAs at 80 registers measured 10.87 ms).
 #ifndef BGPU_MIXED_FWD_MINB
-#define BGPU_MIXED_FWD_MINB 6
+#define BGPU_MIXED_FWD_MINB 7
 #endif
 #ifndef BGPU_MIXED_MID_MINB
 #define BGPU_MIXED_MID_MINB 7
@@ -1329,11 +1332,11 @@ static_assert(kSbThreads == kMixedMidThreads, "schoolbook CTAs ride in the mixed
 __global__ void __launch_bounds__(kMixedMidThreads, BGPU_MIXED_MID_MINB)
     k_mixed_mid(const __grid_constant__ MixedArgs m) {
     extern __shared__ __align__(16) uint32_t sm[];
-    if (blockIdx.x < m.nschool) {  // a schoolbook product: no wait on the column pass
-        schoolbook_body(m.school[blockIdx.x], *reinterpret_cast<SbSmem*>(sm));
+    if (blockIdx.x >= m.ntt_blocks[1]) {  // a schoolbook product: no wait on the column pass
+        schoolbook_body(m.school[blockIdx.x - m.ntt_blocks[1]], *reinterpret_cast<SbSmem*>(sm));
         return;
     }
-    const uint32_t b = blockIdx.x - m.nschool;
+    const uint32_t b = blockIdx.x;
     const MixedClass& k = m.classes[mixed_class(m, 1, b)];
     const uint32_t local = b - k.begin[1];
     if (k.square)
@@ -1346,11 +1349,11 @@ static_assert(kKaThreads == kNumPrimes * 128, "Karatsuba CTAs ride in the mixed 
 
 __global__ void __launch_bounds__(kNumPrimes * 128) k_mixed_inv(const __grid_constant__ MixedArgs m) {
     extern __shared__ __align__(16) uint32_t sm[];
-    if (blockIdx.x < m.nkara) {  // a Karatsuba product: no wait on the row pass
-        karatsuba_body(m.kara[blockIdx.x], *reinterpret_cast<KaSmem*>(sm));
+    if (blockIdx.x >= m.ntt_blocks[2]) {  // a Karatsuba product: no wait on the row pass
+        karatsuba_body(m.kara[blockIdx.x - m.ntt_blocks[2]], *reinterpret_cast<KaSmem*>(sm));
         return;
     }
-    const uint32_t b = blockIdx.x - m.nkara;
+    const uint32_t b = blockIdx.x;
     const MixedClass& k = m.classes[mixed_class(m, 2, b)];
     const uint32_t local = b - k.begin[2];
     const uint32_t bx = local % k.tiles, by = local / k.tiles;
@@ -1440,8 +1443,10 @@ int mixed_fill(MixedClass* classes, int nclasses, const MixedClassSpec* spec, in
     return 0;
 }
 
-cudaError_t launch_ntt_mixed(const MixedArgs& m, const MixedSizes& sz, cudaStream_t st) {
-    if (m.nclasses < 1) return cudaErrorInvalidValue;
+cudaError_t launch_ntt_mixed(const MixedArgs& m_in, const MixedSizes& sz, cudaStream_t st) {
+    if (m_in.nclasses < 1) return cudaErrorInvalidValue;
+    MixedArgs m = m_in;
+    for (int pass = 0; pass < 4; ++pass) m.ntt_blocks[pass] = sz.blocks[pass];
     allow_smem(k_mixed_fwd, sz.smem[0]);
     cudaError_t e = launch_k(k_mixed_fwd, dim3(sz.blocks[0]), dim3(256), sz.smem[0], st, m);
     if (e != cudaSuccess) return e;
