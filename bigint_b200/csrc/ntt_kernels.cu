@@ -369,7 +369,7 @@ __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx,
 }
 
 template <int PS, int L2, int T>
-__global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const __grid_constant__ FwdColsArgs a) {
+__global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const FwdColsArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     fwd_cols_body<PS, L2, T>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm);
 }
@@ -572,7 +572,7 @@ __device__ __forceinline__ void mid_rows_body(const MidRowsArgs& a, uint32_t slo
 }
 
 template <int PS, int L1, int T, bool SQR>
-__global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const __grid_constant__ MidRowsArgs a) {
+__global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const MidRowsArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     mid_rows_body<PS, L1, T, SQR>(a, blockIdx.x, blockIdx.y, sm);
 }
@@ -705,7 +705,7 @@ __device__ __forceinline__ void inv_cols_body(const InvColsArgs& a, uint32_t bx,
 }
 
 template <int PS, int L2, int TP>
-__global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const __grid_constant__ InvColsArgs a) {
+__global__ void __launch_bounds__(kNumPrimes * TP) k_inv_cols(const InvColsArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     inv_cols_body<PS, L2, TP>(a, blockIdx.x, blockIdx.y, sm);
 }
@@ -1287,7 +1287,7 @@ __device__ __forceinline__ int mixed_class(const MixedArgs& m, int pass, uint32_
     return c;
 }
 
-__global__ void __launch_bounds__(256, BGPU_MIXED_FWD_MINB) k_mixed_fwd(const __grid_constant__ MixedArgs m) {
+__global__ void __launch_bounds__(256, BGPU_MIXED_FWD_MINB) k_mixed_fwd(const MixedArgs m) {
     extern __shared__ __align__(16) uint32_t sm[];
     const MixedClass& k = m.classes[mixed_class(m, 0, blockIdx.x)];
     const uint32_t local = blockIdx.x - k.begin[0];
@@ -1330,7 +1330,7 @@ __device__ __forceinline__ void mixed_mid_len(const MixedClass& k, uint32_t loca
 static_assert(kSbThreads == kMixedMidThreads, "schoolbook CTAs ride in the mixed row pass");
 
 __global__ void __launch_bounds__(kMixedMidThreads, BGPU_MIXED_MID_MINB)
-    k_mixed_mid(const __grid_constant__ MixedArgs m) {
+    k_mixed_mid(const MixedArgs m) {
     extern __shared__ __align__(16) uint32_t sm[];
     if (blockIdx.x >= m.ntt_blocks[1]) {  // a schoolbook product: no wait on the column pass
         schoolbook_body(m.school[blockIdx.x - m.ntt_blocks[1]], *reinterpret_cast<SbSmem*>(sm));
@@ -1347,7 +1347,7 @@ __global__ void __launch_bounds__(kMixedMidThreads, BGPU_MIXED_MID_MINB)
 
 static_assert(kKaThreads == kNumPrimes * 128, "Karatsuba CTAs ride in the mixed inverse pass");
 
-__global__ void __launch_bounds__(kNumPrimes * 128) k_mixed_inv(const __grid_constant__ MixedArgs m) {
+__global__ void __launch_bounds__(kNumPrimes * 128) k_mixed_inv(const MixedArgs m) {
     extern __shared__ __align__(16) uint32_t sm[];
     if (blockIdx.x >= m.ntt_blocks[2]) {  // a Karatsuba product: no wait on the row pass
         karatsuba_body(m.kara[blockIdx.x - m.ntt_blocks[2]], *reinterpret_cast<KaSmem*>(sm));
@@ -1369,7 +1369,7 @@ __global__ void __launch_bounds__(kNumPrimes * 128) k_mixed_inv(const __grid_con
     }
 }
 
-__global__ void __launch_bounds__(kCarryThreads) k_mixed_carry(const __grid_constant__ MixedArgs m) {
+__global__ void __launch_bounds__(kCarryThreads) k_mixed_carry(const MixedArgs m) {
     __shared__ uint32_t s_t;
     if (threadIdx.x == 0) s_t = (uint32_t)(atomicAdd(m.ticket, 1ull) - m.ticket_base);
     __syncthreads();
