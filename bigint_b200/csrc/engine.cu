@@ -742,7 +742,16 @@ int mul_u64_many_locked(const bgpu_host_product* p, size_t count, uint32_t flags
             if (e == cudaSuccess) e = cudaEventRecord(g.ev_comp[k], st);
         }
         if (e == cudaSuccess) e = cudaStreamWaitEvent(g.d2h, g.ev_comp[k], 0);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(q.out, dout, nout * 8, cudaMemcpyDeviceToHost, g.d2h);
+        // The product goes back in pieces the size of the larger operand's
+        // upload.  With copies of equal size in flight both ways the copy
+        // engines share the link evenly; one 4 MiB download against 2 MiB
+        // uploads left the uploads at 31 GB/s (measured at 2^24-bit
+        // products: 137 us per product, 122 us with two 2 MiB pieces;
+        // smaller pieces were slower again).
+        const size_t piece = std::max<size_t>(std::max(m.na, m.nb), 4096) * 8;
+        for (size_t off = 0; e == cudaSuccess && off < nout * 8; off += piece)
+            e = cudaMemcpyAsync(reinterpret_cast<char*>(q.out) + off, reinterpret_cast<const char*>(dout) + off,
+                                std::min(piece, nout * 8 - off), cudaMemcpyDeviceToHost, g.d2h);
         if (e == cudaSuccess) e = cudaEventRecord(g.ev_out[k], g.d2h);
         if (e != cudaSuccess) return cuda_status(e);
     }
