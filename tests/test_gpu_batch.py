@@ -75,3 +75,53 @@ def test_batch_rejects_bad_descriptor(bb):
     with pytest.raises(bb.BigIntGPUError) as e:
         bb.BatchPlan([(0, 4, 0, 4, 0)])
     assert e.value.code == -1
+
+
+def _run_plan_and_check(bb, port, torch, A, B, square_idx=()):
+    dA, dB = _to_dev(torch, A), _to_dev(torch, B)
+    for i in square_idx:
+        dB[i] = dA[i]
+    outs = [torch.full((a.size + (a.size if i in square_idx else b.size),), -1, dtype=torch.int64,
+                       device="cuda") for i, (a, b) in enumerate(zip(A, B))]
+    prods = [(dA[i].data_ptr(), A[i].size, dB[i].data_ptr(), A[i].size if i in square_idx else B[i].size,
+              outs[i].data_ptr()) for i in range(len(A))]
+    plan = bb.BatchPlan(prods)
+    launches = plan.launches
+    for _ in range(2):
+        plan.run(0)
+        bb.device_status(0)
+    plan.close()
+    for i in range(len(A)):
+        got = outs[i].cpu().numpy().view(np.uint64)
+        want = port.mul(A[i]) if i in square_idx else port.mul(A[i], B[i])
+        assert np.array_equal(got[: want.size], want) and not got[want.size:].any(), i
+    return launches
+
+
+def test_batch_one_launch_per_pass_with_small_products(bb, port):
+    """Every length qualifies for the mixed-length launches: four kernels in
+    all, the schoolbook and Karatsuba products riding in the row and inverse
+    passes, squares among them; run twice (state reset between runs)."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 42)
+    A, B = _make_batch(torch, rng, 200, 6, 17, ones_every=13)
+    A[3] = A[2]
+    assert _run_plan_and_check(bb, port, torch, A, B, square_idx=(3,)) == 4
+
+
+def test_batch_with_a_long_class_runs_per_class(bb, port):
+    """A transform too long for the mixed-length launches (2^20 points) sends
+    the batch back to one set of launches per class on graph branches."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 43)
+    A, B = _make_batch(torch, rng, 40, 8, 14)
+    A.append(rand_limbs(rng, 1 << 18))
+    B.append(rand_limbs(rng, 1 << 18))
+    assert _run_plan_and_check(bb, port, torch, A, B) > 4
+
+
+def test_batch_of_small_products_only(bb, port):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 44)
+    A, B = _make_batch(torch, rng, 100, 6, 13)
+    _run_plan_and_check(bb, port, torch, A, B)
