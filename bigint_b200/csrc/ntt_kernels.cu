@@ -778,7 +778,7 @@ cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t 
 // tickets of one launch (their look-back waits only on earlier blocks).
 __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid, uint32_t nchunks, int out_fmt,
                                             uint64_t epoch, uint32_t* err) {
-    __shared__ uint32_t s_cin;
+    __shared__ uint32_t s_cin, s_win_g, s_win_p;
     __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
     const uint64_t* chunks = pd.chunks;
     const uint64_t* spill = pd.spill;
@@ -801,6 +801,34 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
             S[i][0] = S[i][1] = S[i][2] = S[i][3] = 0;
         }
         sp[i] = (cc >= 1 && cc - 1 < nchunks) ? spill[cc - 1] : 0;
+    }
+    // Warp 0 also reads the 32 chunks below the block (all real chunks: the
+    // block starts at or below the last one) and records their (G, P): the
+    // carry into the block is the G of the highest of them that does not
+    // propagate, found without waiting on any other block.
+    if (warp == 0) {
+        const int64_t j = (int64_t)bid * kCarryChunksPerBlock - 32 + lane;
+        uint32_t g = 0, pbit = 0;  // below chunk 0: no carry, nothing propagates
+        if (j >= 0) {
+            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)j * 4);
+            const ulonglong2 u = src[0], v = src[1];
+            const uint64_t s0 = j >= 1 ? spill[j - 1] : 0;
+            const uint64_t t0 = u.x + s0;
+            uint32_t cy = t0 < s0;
+            const uint64_t t1 = u.y + cy;
+            cy = cy & (t1 == 0);
+            const uint64_t t2 = v.x + cy;
+            cy = cy & (t2 == 0);
+            const uint64_t t3 = v.y + cy;
+            cy = cy & (t3 == 0);
+            g = cy;
+            pbit = (!cy) && ((t0 & t1 & t2 & t3) == ~0ull);
+        }
+        const uint32_t wg = __ballot_sync(0xffffffffu, g), wp = __ballot_sync(0xffffffffu, pbit);
+        if (lane == 0) {
+            s_win_g = wg;
+            s_win_p = wp;
+        }
     }
     // per-chunk (G, P) and per-segment ballots
     uint32_t gm[kCarryPer], bm[kCarryPer];
@@ -844,9 +872,13 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
         uint32_t cin = 0;
         cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> self(
             *reinterpret_cast<unsigned long long*>(flags + bid));
+        const uint32_t stop = ~s_win_p;  // window chunks that do not propagate a carry
         if (bid == 0) {
             self.store(make_flag(epoch, 2, bG, 0), cuda::memory_order_release);
-        } else {
+        } else if (stop) {
+            cin = (s_win_g >> (31 - __clz(stop))) & 1u;  // the highest one's carry out
+            self.store(make_flag(epoch, 2, bG | (bP & cin), 0), cuda::memory_order_release);
+        } else {  // 32 propagating chunks: the decoupled look-back on the blocks' flags
             self.store(make_flag(epoch, 1, bG, bP), cuda::memory_order_release);
             int k = (int)bid - 1;
             while (true) {
