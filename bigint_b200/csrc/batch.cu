@@ -278,6 +278,7 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
             destroy_plan(p);
             return BGPU_ERR_INVALID_ARG;
         }
+        for (auto& k : mc) k.inv.err = hooks.err;
         p->mixed_begin.resize(mc.size());
         for (size_t i = 0; i < mc.size(); ++i)
             for (int pass = 0; pass < 4; ++pass) p->mixed_begin[i][pass] = mc[i].begin[pass];

@@ -101,6 +101,7 @@ struct InvColsArgs {
     const ProductDesc* descs;  // y (A's planes after the middle pass), chunks, spill
     ProductDesc one;
     int log_n, log_n1, slot;
+    uint32_t* err;  // sticky device error word (a bounded wait that gave up), or nullptr
 };
 
 // A mixed-length batch (all its NTT classes in one launch per pass): one
