@@ -603,11 +603,7 @@ __device__ __forceinline__ void crt3(const NttConsts& c, uint32_t r0, uint32_t r
 #define BGPU_INV_UNROLL 4
 #endif
 
-constexpr int kInvUnroll = BGPU_INV_UNROLL;
-#ifndef BGPU_INV_TMA
-#define BGPU_INV_TMA 0
-#endif
-constexpr uint32_t kInvWaitLimit = 1u << 22;  // bounded mbarrier polls of the bulk-copy variant  // groups of the first (global-memory) round in flight per thread
+constexpr int kInvUnroll = BGPU_INV_UNROLL;  // groups of the first (global-memory) round in flight per thread
 
 // The inverse column pass of one CTA: tile bx of product by.  Three thread
 // groups of TP threads, one per prime, transform their prime's column tile
