@@ -163,7 +163,7 @@ int set_split(int log_n, int log_n2);  // 0 on success; log_n2 == 0 restores the
 int set_batch_split(int log_n, int log_n2);
 bool shape_supported(int log_n, bool square);
 bool shape_supported_batch(int log_n, bool square);
-size_t smem_fwd_cols(int log_n2);
+size_t smem_fwd_cols(int log_n2, int cols);
 size_t smem_mid_rows(int log_n1, bool square);
 size_t smem_inv_cols(int log_n2);
 

@@ -45,6 +45,11 @@ __host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
 }
 
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
+#ifndef BGPU_FWD_COLS
+#define BGPU_FWD_COLS 8
+#endif
+constexpr int kFwdCols = BGPU_FWD_COLS;      // columns per forward-pass tile
+constexpr int kFwdThreads = 32 * kFwdCols;   // its threads (the same work per thread)
 
 __constant__ NttConsts c_consts[kConstSlots];
 
@@ -214,7 +219,7 @@ __device__ __forceinline__ uint32_t load_digit32_fmt(const OperandDesc& in, uint
 // first stage (a, 0) -> (a, a w) is one multiply per pair.  With a single
 // round the inter-pass twiddle and the global store follow; otherwise the
 // elements go to the shared tile.
-template <int PS, int L2, int T, bool LIMB, bool HALF>
+template <int PS, int L2, int T, int FC, bool LIMB, bool HALF>
 __device__ __forceinline__ void fwd_round0(const FwdColsArgs& a, const OperandDesc& in, const NttConsts& c,
                                            int q, uint32_t c0, uint32_t* y, const uint2* sS, uint32_t* sm) {
     constexpr bool LAZY = PS == 0;
@@ -222,7 +227,7 @@ __device__ __forceinline__ void fwd_round0(const FwdColsArgs& a, const OperandDe
     constexpr int NR = P2::nr;
     constexpr int RL = P2::r(NR - 1);
     constexpr int SROW = (1 << RL) + 1;
-    using Gr = Group<L2, kCols, 0>;
+    using Gr = Group<L2, FC, 0>;
     constexpr int R = Gr::R;
     constexpr int D = 1 << (R - 1);
     constexpr int NL = HALF ? D : (1 << R);  // elements read from the operand
@@ -285,14 +290,14 @@ __device__ __forceinline__ void fwd_round0(const FwdColsArgs& a, const OperandDe
 // 0.4 us shorter than with the 40 registers the compiler picks on its own
 // (6 CTAs per SM).  Other heights keep the compiler's choice.
 __host__ __device__ constexpr int fwd_min_blocks(int l2, int threads) {
-    return (l2 == 9 && threads == 256) ? 8 : 1;
+    return l2 == 9 ? 2048 / threads : 1;
 }
 
 // The forward column pass of one CTA: tile bx, prime by, operand and product
 // bz (block coordinates passed in, so a mixed-length launch can run it too).
-template <int PS, int L2, int T>
+template <int PS, int L2, int T, int FC = kCols>
 __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx, uint32_t by, uint32_t bz,
-                                              uint32_t* sm) {  // sm: [2^L2][kCols] + column powers
+                                              uint32_t* sm) {  // sm: [2^L2][FC] + column powers
     constexpr bool LAZY = PS == 0;
     using P2 = Plan<L2>;
     constexpr int NR = P2::nr;
@@ -302,7 +307,7 @@ __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx,
     const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
     const uint2* tw = c.stage[q][0];
     const OperandDesc in = opi == 0 ? pd.op[0] : pd.op[1];
-    const uint32_t c0 = bx * kCols;
+    const uint32_t c0 = bx * FC;
     const size_t nn = (size_t)1 << a.log_n;
     uint32_t* y = pd.y + ((size_t)opi * kNumPrimes + q) * nn;
 
@@ -314,8 +319,8 @@ __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx,
     // banks (an unpadded 2^RL-entry row puts all of them in one bank).
     constexpr int RL = P2::r(NR - 1);
     constexpr int SROW = (1 << RL) + 1;
-    uint2* sS = reinterpret_cast<uint2*>(sm + (kCols << L2));
-    for (int t = threadIdx.x; t < (kCols << RL); t += T) {
+    uint2* sS = reinterpret_cast<uint2*>(sm + (FC << L2));
+    for (int t = threadIdx.x; t < (FC << RL); t += T) {
         const uint32_t col = (uint32_t)t >> RL, m = (uint32_t)t & ((1u << RL) - 1u);
         const uint32_t e = (((c0 + col) * m) << (L2 - RL)) & (uint32_t)(nn - 1);
         const uint32_t w = inter_twiddle(c, q, 0, e, a.log_n, p);
@@ -330,20 +335,20 @@ __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx,
     // the launch, so each combination is its own copy of the round.
     if (in.fmt == kFmtLimb64) {
         if (2 * (size_t)in.nd32 <= nn)
-            fwd_round0<PS, L2, T, true, true>(a, in, c, q, c0, y, sS, sm);
+            fwd_round0<PS, L2, T, FC, true, true>(a, in, c, q, c0, y, sS, sm);
         else
-            fwd_round0<PS, L2, T, true, false>(a, in, c, q, c0, y, sS, sm);
+            fwd_round0<PS, L2, T, FC, true, false>(a, in, c, q, c0, y, sS, sm);
     } else {
         if (2 * (size_t)in.nd32 <= nn)
-            fwd_round0<PS, L2, T, false, true>(a, in, c, q, c0, y, sS, sm);
+            fwd_round0<PS, L2, T, FC, false, true>(a, in, c, q, c0, y, sS, sm);
         else
-            fwd_round0<PS, L2, T, false, false>(a, in, c, q, c0, y, sS, sm);
+            fwd_round0<PS, L2, T, FC, false, false>(a, in, c, q, c0, y, sS, sm);
     }
     if constexpr (NR > 1) {
         __syncthreads();
-        dif_rounds<LAZY, L2, kCols, T, 1, NR - 2>(sm, tw, p, threadIdx.x);
+        dif_rounds<LAZY, L2, FC, T, 1, NR - 2>(sm, tw, p, threadIdx.x);
         // Last round: butterflies, inter-pass twiddle, store to global.
-        using Gr = Group<L2, kCols, NR - 1>;
+        using Gr = Group<L2, FC, NR - 1>;
         constexpr int R = Gr::R;
 #pragma unroll 2
         for (int g = threadIdx.x; g < Gr::G; g += T) {
@@ -371,7 +376,7 @@ __device__ __forceinline__ void fwd_cols_body(const FwdColsArgs& a, uint32_t bx,
 template <int PS, int L2, int T>
 __global__ void __launch_bounds__(T, fwd_min_blocks(L2, T)) k_fwd_cols(const FwdColsArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
-    fwd_cols_body<PS, L2, T>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm);
+    fwd_cols_body<PS, L2, T, kFwdCols>(a, blockIdx.x, blockIdx.y, blockIdx.z, sm);
 }
 
 // ---- kernel 2: middle row pass ----------------------------------------------
@@ -1056,7 +1061,7 @@ static bool shape_ok(const TransformShape& s, bool square) {
 bool shape_supported(int log_n, bool square) { return shape_ok(choose_shape(log_n), square); }
 bool shape_supported_batch(int log_n, bool square) { return shape_ok(choose_shape_batch(log_n), square); }
 
-size_t smem_fwd_cols(int l2) { return ((size_t)kCols * 4 << l2) + kCols * 17 * sizeof(uint2); }
+size_t smem_fwd_cols(int l2, int cols) { return ((size_t)cols * 4 << l2) + cols * 17 * sizeof(uint2); }
 size_t smem_mid_rows(int l1, bool square) {
     return (square || l1 >= 15 ? 1 : 2) * ((size_t)4 << l1) + 16 * sizeof(uint2);
 }
@@ -1071,12 +1076,14 @@ static cudaError_t launch_outer(const FwdColsArgs* f, const InvColsArgs* inv, ui
 #ifndef BGPU_INV_TP
 #define BGPU_INV_TP 128
 #endif
-    constexpr int T = 256, TP = BGPU_INV_TP;
+    constexpr int TP = BGPU_INV_TP;
     if (f) {
-        auto k = k_fwd_cols<PS, L2, T>;
-        const size_t sm = smem_fwd_cols(L2);
+        // `tiles` counts 8-column tiles; the forward pass's tiles are kFwdCols wide
+        auto k = k_fwd_cols<PS, L2, kFwdThreads>;
+        const size_t sm = smem_fwd_cols(L2, kFwdCols);
         allow_smem(k, sm);
-        return launch_k(k, dim3(tiles, kNumPrimes, f->nops * count), dim3(T), sm, st, *f);
+        return launch_k(k, dim3(tiles * (kCols / kFwdCols), kNumPrimes, f->nops * count), dim3(kFwdThreads), sm,
+                        st, *f);
     }
     auto k = k_inv_cols<PS, L2, TP>;
     const size_t sm = smem_inv_cols(L2);
@@ -1464,7 +1471,7 @@ int mixed_fill(MixedClass* classes, int nclasses, const MixedClassSpec* spec, in
         at[1] += k.rows * kNumPrimes * sp.count / rpc;
         at[2] += k.tiles * sp.count;
         at[3] += k.bpp * sp.count;
-        sm_fwd = std::max(sm_fwd, smem_fwd_cols(sh.log_n2));
+        sm_fwd = std::max(sm_fwd, smem_fwd_cols(sh.log_n2, kCols));
         sm_mid = std::max(sm_mid, rpc * row_bytes);
         sm_inv = std::max(sm_inv, smem_inv_cols(sh.log_n2));
     }
