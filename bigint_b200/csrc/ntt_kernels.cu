@@ -45,11 +45,10 @@ __host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
 }
 
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
-#ifndef BGPU_FWD_COLS
-#define BGPU_FWD_COLS 8
-#endif
-constexpr int kFwdCols = BGPU_FWD_COLS;      // columns per forward-pass tile
-constexpr int kFwdThreads = 32 * kFwdCols;   // its threads (the same work per thread)
+// The forward pass's tiles and threads (measured against 4-column tiles of
+// 128 or 64 threads and 8-column tiles of 128 threads: all slower).
+constexpr int kFwdCols = 8;
+constexpr int kFwdThreads = 256;
 
 __constant__ NttConsts c_consts[kConstSlots];
 
