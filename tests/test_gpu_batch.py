@@ -125,3 +125,38 @@ def test_batch_of_small_products_only(bb, port):
     rng = np.random.default_rng(SEED + 44)
     A, B = _make_batch(torch, rng, 100, 6, 13)
     _run_plan_and_check(bb, port, torch, A, B)
+
+
+def test_batch_more_products_than_one_class_launch_slice(bb, port):
+    """20000 products of several lengths in the mixed launches (the per-class
+    launches slice classes above 16384 products; the mixed ones take every
+    CTA in one grid); a sample checked against the oracle, every product by
+    its residue."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 45)
+    n = 20000
+    na = rng.integers(1, 1500, n)  # schoolbook, Karatsuba and four transform lengths
+    nb = rng.integers(1, 1500, n)
+    big = rng.integers(0, 2**64, int(na.sum() + nb.sum()), dtype=np.uint64, endpoint=False)
+    offs_a = np.concatenate([[0], np.cumsum(na)[:-1]])
+    offs_b = np.concatenate([[0], np.cumsum(nb)[:-1]]) + na.sum()
+    outn = na + nb
+    offs_o = np.concatenate([[0], np.cumsum(outn)[:-1]])
+    dbig = torch.from_numpy(big.view(np.int64)).cuda()
+    dout = torch.full((int(outn.sum()),), -1, dtype=torch.int64, device="cuda")
+    bi, bo = dbig.data_ptr(), dout.data_ptr()
+    plan = bb.BatchPlan([(bi + 8 * int(offs_a[i]), int(na[i]), bi + 8 * int(offs_b[i]), int(nb[i]),
+                          bo + 8 * int(offs_o[i])) for i in range(n)])
+    assert plan.launches == 4
+    plan.run(0)
+    bb.device_status(0)
+    plan.close()
+    host = dout.cpu().numpy().view(np.uint64)
+    M = (1 << 61) - 1
+    for i in range(n):
+        a = big[offs_a[i]:offs_a[i] + na[i]]
+        b = big[offs_b[i]:offs_b[i] + nb[i]]
+        c = host[offs_o[i]:offs_o[i] + outn[i]]
+        assert port.mod_m61(a) * port.mod_m61(b) % M == port.mod_m61(c), i
+        if i % 997 == 0:
+            assert np.array_equal(np.trim_zeros(c, "b"), port.mul(a, b)), i
