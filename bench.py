@@ -498,7 +498,8 @@ def plain_2p20_form(bb, torch, device, port, cpu: bool = True):
 def sweep_form(bb, torch, device, port):
     """Config "NTT size sweep": squares at 2^16..2^30 bits, uniform and all-ones
     limbs, plus the 1:8 and 1:64 unbalanced pairs, and two sizes beyond the
-    largest transform (2^31 x 2^31 bits, a 2^32-bit square: block products);
+    largest transform (2^31 x 2^31 bits, a 2^32-bit square: spectral sums of
+    block products);
     device-resident products back to back on one stream (operands smaller
     than L2 stay cached there)."""
     stream = torch.cuda.Stream(device)
@@ -514,7 +515,8 @@ def sweep_form(bb, torch, device, port):
         ref.init_thread_pool(ref_pool_threads())
     cases = [(1 << b, 1 << b, "square") for b in range(16, 31, 2)]
     cases += [(1 << 24, 1 << 21, "1:8"), (1 << 20, 1 << 14, "1:64")]
-    # beyond the largest transform (2^31 product bits): blocks of 2^30-bit NTT products
+    # beyond the largest transform (2^31 product bits): 2^30-bit blocks, each
+    # transformed once, output blocks formed as spectral sums
     cases += [(1 << 31, 1 << 31, "1:1"), (1 << 32, 1 << 32, "square")]
     for abits, bbits, kind in cases:
         na, nb = abits // 64, bbits // 64

@@ -286,12 +286,120 @@ bool beyond_transform(size_t na, size_t nb) {
     return ceil_log2(2 * (uint64_t)(na + nb) - 1) > transform_cap_log();
 }
 
+// Largest number of block products one spectral sum may hold: a block has at
+// most 2S 32-bit digits, so a block product's coefficients are below
+// 2S (2^32 - 1)^2, and the sum's must stay below the product of the three
+// primes for the CRT to return them exactly.  2 for the default 2^24-limb
+// blocks (2^90 against 2^90.47).
+int spectral_terms(int ps, uint64_t S) {
+    const PrimeSetInfo& s = kPrimeSets[ps];
+    const unsigned __int128 m = (unsigned __int128)s.p[0] * s.p[1] * s.p[2];
+    const unsigned __int128 per = (unsigned __int128)0xFFFFFFFFu * 0xFFFFFFFFu * (2 * S);
+    const unsigned __int128 t = (m - 1) / per;
+    return (int)(t < (unsigned __int128)kMaxSpecTerms ? t : kMaxSpecTerms);
+}
+
+// The spectral form of a product beyond the largest transform:
+//   A * B = sum_k 2^(64 S k) C_k,  C_k = sum_{i+j=k} A_i B_j,
+// with every block's transform computed once (its spectrum, 3 N residues)
+// and each C_k formed in the transform domain as sums of at most `tmax`
+// pointwise products.  Each sum is inverse-transformed once (row DIT,
+// inverse column pass with CRT) and carried straight into dout's window of
+// 2S + 1 limbs at offset S k, together with what that window already holds
+// (the chunk merge before the carry scan).  Output blocks go in increasing
+// k, so above limb (k+1)S + 1 dout is still zero when C_k's first sum
+// arrives, and every partial sum of the product that ends with (part of)
+// C_k is below 2^(64 (kS + 2S + 1)): nothing carries out of the window.  A
+// square's off-diagonal pairs (i < j) are summed once and doubled in the
+// merge, its diagonal squares summed on their own.  The pairwise form
+// multiplies every block pair as a whole product: 3 transforms per pair
+// against about 1 here.
+int huge_spectral(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, uint64_t* dout, bool square,
+                  int tmax, cudaStream_t st) {
+    const uint64_t S = g.huge_block, L = na + nb;
+    const int ln = transform_cap_log(), ps = prime_set_for(ln);
+    const size_t nn = (size_t)1 << ln;
+    const uint64_t nA = (na + S - 1) / S, nB = square ? nA : (nb + S - 1) / S;
+    const size_t nspec = nA + (square ? 0 : nB);
+    const size_t spec_bytes = align256((size_t)kNumPrimes * nn * 4);
+    int rc = ensure(&g.d_huge, &g.huge_bytes, nspec * spec_bytes);
+    if (rc != BGPU_OK) return rc;
+    char* base = static_cast<char*>(g.d_huge);
+    auto spec = [&](uint64_t i) { return reinterpret_cast<uint32_t*>(base + i * spec_bytes); };
+    ProductScratch s{};
+    rc = prepare_scratch(ln, true, &s);  // 3 residue planes: the sums' row pass output
+    if (rc != BGPU_OK) return rc;
+    const int slot = kSlotEngine + ps;
+    cudaError_t e = cudaMemsetAsync(dout, 0, L * 8, st);
+    for (uint64_t i = 0; e == cudaSuccess && i < nspec; ++i) {
+        const bool from_a = i < nA;
+        const uint64_t off = (from_a ? i : i - nA) * S;
+        const uint64_t len = std::min<uint64_t>(S, (from_a ? na : nb) - off);
+        const OperandDesc od{(from_a ? da : db) + off, (uint32_t)len, (uint32_t)(2 * len), kFmtLimb64};
+        e = launch_ntt_spectrum(slot, g.consts[ps], od, ln, spec(i), st);
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    // (i, j) pairs of output block k in sums of at most tmax; `first`: the
+    // window holds only C_(k-1)'s top S + 1 limbs so far (nothing when k = 0)
+    auto run_sums = [&](const std::vector<std::pair<uint64_t, uint64_t>>& pairs, uint64_t k, bool twice,
+                        bool& first) {
+        const uint64_t off = k * S, win = std::min<uint64_t>(2 * S + 1, L - off);
+        for (size_t g0 = 0; g0 < pairs.size(); g0 += (size_t)tmax) {
+            const int n = (int)std::min<size_t>((size_t)tmax, pairs.size() - g0);
+            const uint32_t* sa[kMaxSpecTerms];
+            const uint32_t* sb[kMaxSpecTerms];
+            for (int t = 0; t < n; ++t) {
+                sa[t] = spec(pairs[g0 + t].first);
+                sb[t] = spec(square ? pairs[g0 + t].second : nA + pairs[g0 + t].second);
+            }
+            const uint64_t nadd = first ? (k == 0 ? 0 : std::min<uint64_t>(S + 1, win)) : win;
+            first = false;
+            CarryLaunch cl;
+            cl.ticket_base = g.ticket_base;
+            cl.epoch = ++g.epoch;
+            g.ticket_base += carry_blocks((uint32_t)(nn / 8));
+            const cudaError_t e2 = launch_ntt_spectral_sum(slot, g.consts[ps], sa, sb, n, twice, ln, s, dout + off,
+                                                           win, nadd ? dout + off : nullptr, nadd, cl, st);
+            if (e2 != cudaSuccess) return e2;
+        }
+        return cudaSuccess;
+    };
+    std::vector<std::pair<uint64_t, uint64_t>> once, twice;
+    for (uint64_t k = 0; e == cudaSuccess && k + 1 < nA + nB; ++k) {
+        once.clear();
+        twice.clear();
+        for (uint64_t i = k >= nB ? k - (nB - 1) : 0; i <= k && i < nA; ++i) {
+            const uint64_t j = k - i;
+            if (!square)
+                once.emplace_back(i, j);
+            else if (i < j)
+                twice.emplace_back(i, j);
+            else if (i == j)
+                once.emplace_back(i, j);
+        }
+        bool first = true;
+        e = run_sums(once, k, false, first);
+        if (e == cudaSuccess) e = run_sums(twice, k, true, first);
+    }
+    g.ntt_log_n = -1;  // no forward pass overlaps the carry scans that end this product
+    return cuda_status(e);
+}
+
 // Product beyond the largest transform (huge.cu): both operands in blocks of
-// kHugeBlockLimbs limbs, every block pair one NTT product, each added into
-// dout (na + nb limbs) at its offset with a carry scan over the rest.  A
-// square computes each off-diagonal block pair once and adds it twice.
+// g.huge_block limbs (2^24: 2^30 bits) added into dout (na + nb limbs) at
+// their offsets with a carry scan over the rest.  The spectral form
+// (huge_spectral) when its row kernels exist for the block's transform and its
+// spectra fit in device memory; otherwise every block pair is one NTT
+// product, a square computing each off-diagonal pair once and adding it
+// twice.
 int huge_product(const uint64_t* da, size_t na, const uint64_t* db, size_t nb, uint64_t* dout, bool square,
                  cudaStream_t st) {
+    const int ln = transform_cap_log();
+    const int tmax = spectral_terms(prime_set_for(ln), g.huge_block);
+    if (tmax >= 1 && spectral_supported(ln)) {
+        const int rc = huge_spectral(da, na, db, nb, dout, square, tmax, st);
+        if (rc != BGPU_ERR_OOM) return rc;
+    }
     const uint64_t S = g.huge_block, L = na + nb;
     const size_t acc = align256((size_t)accumulate_blocks(L) * 4);
     int rc = ensure(&g.d_huge, &g.huge_bytes, 2 * S * 8 + 2 * acc);

@@ -104,6 +104,20 @@ struct InvColsArgs {
     uint32_t* err;  // sticky device error word (a bounded wait that gave up), or nullptr
 };
 
+// Spectral sums (products beyond the largest transform): the row-pass launch
+// that finishes an operand block's forward transform in place (y = its
+// spectrum), or the one that forms sum_t sa[t] (.) sb[t] over nterms pairs
+// of block spectra and runs the row DIT into y (3 planes each).
+constexpr int kMaxSpecTerms = 4;
+struct SpecArgs {
+    const uint32_t* sa[kMaxSpecTerms];
+    const uint32_t* sb[kMaxSpecTerms];
+    int nterms;
+    uint32_t* y;
+    int log_n, log_n2, slot;
+    uint32_t scale_w[kNumPrimes], scale_wp[kNumPrimes];  // N^-1 * 2^32 mod p (Montgomery form)
+};
+
 // A mixed-length batch (all its NTT classes in one launch per pass): one
 // class of products of equal transform length and squaring flag, with its
 // CTA range in each pass's launch (begin[3] is its first carry ticket).
@@ -225,6 +239,27 @@ cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t 
 cudaError_t launch_ntt_batch(int slot, const NttConsts& host, const ProductDesc* descs, int count,
                              bool square, int log_n, int out_fmt, const CarryLaunch& cl,
                              cudaStream_t stream);
+
+// Spectral sums of block products (2 launches per operand block, 3 or 4 per
+// sum): spectral_supported(log_n) tells whether the row-pass kernels exist
+// for the tuned split of 2^log_n points.  launch_ntt_spectrum writes the
+// forward transform of operand `a` (3 planes of 2^log_n residues, in the row
+// pass's element order) to `spec`; launch_ntt_spectral_sum multiplies nterms
+// pairs of such spectra pointwise, sums them, and inverse-transforms the sum
+// through the row DIT and the inverse column pass with CRT; then the sum
+// (twice the sum when `twice`) plus the nadd u64 limbs at `add` (nullptr:
+// none) is carried into `out_cap` u64 limbs at `out`, which may be the
+// limbs at `add` (the doubling is exact limb arithmetic after the CRT).  The
+// caller keeps every coefficient of the sum below the product of the three
+// primes, and the total below 2^(64 out_cap).
+bool spectral_supported(int log_n);
+cudaError_t launch_ntt_spectrum(int slot, const NttConsts& host, const OperandDesc& a, int log_n,
+                                uint32_t* spec, cudaStream_t stream);
+cudaError_t launch_ntt_spectral_sum(int slot, const NttConsts& host, const uint32_t* const* sa,
+                                    const uint32_t* const* sb, int nterms, bool twice, int log_n,
+                                    const ProductScratch& s, uint64_t* out, size_t out_cap,
+                                    const uint64_t* add, size_t nadd, const CarryLaunch& cl,
+                                    cudaStream_t stream);
 
 // ---- FP64 complex-FFT form ----
 constexpr int kFftMaxLogN = 26;     // largest FFT transform (2^26 complex points)

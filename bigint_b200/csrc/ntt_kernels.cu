@@ -479,6 +479,45 @@ __device__ __forceinline__ void mid_dif_row(const uint32_t* row, uint32_t* s, co
     dif_rounds<LAZY, L1, 1, T, 1, P1::nr - 2>(s, twf, p, tid);
 }
 
+// The last DIT round's groups hold n1 = q + (j << LO0); the inverse
+// inter-pass twiddle omega_N^-(k2 n1) = B(q) * T^j with the row-constant
+// powers sT[j] = omega_N^-(k2 j << LO0), written here for one row.
+template <int L1, int T>
+__device__ __forceinline__ void row_inv_powers(const NttConsts& c, int q, uint32_t k2, int log_n, size_t nn,
+                                               uint32_t p, uint32_t pinv, uint2* sT, int tid) {
+    using P1 = Plan<L1>;
+    constexpr int R0 = P1::r(0), LO0 = P1::lo(0);
+    for (int t = tid; t < (1 << R0); t += T) {
+        const uint32_t w = inter_twiddle(c, q, 1, ((k2 * (uint32_t)t) << LO0) & (uint32_t)(nn - 1), log_n, p);
+        sT[t] = make_uint2(w, w * pinv);
+    }
+}
+
+// Round 0 of a row's DIT (its top bits) from shared memory `s`; each group
+// times its inverse inter-pass twiddle and the scale N^-1 * 2^32 (sw, swp),
+// stored to the row in global memory.
+template <bool LAZY, int L1, int T>
+__device__ __forceinline__ void row_dit_store(const NttConsts& c, int q, uint32_t k2, int log_n, size_t nn,
+                                              uint32_t sw, uint32_t swp, const uint32_t* s, const uint2* sT,
+                                              const uint2* twi, uint32_t p, uint32_t pinv, uint32_t* row,
+                                              int tid) {
+    using Gr = Group<L1, 1, 0>;
+    constexpr int R = Gr::R;
+#pragma unroll 2
+    for (int g = tid; g < Gr::G; g += T) {
+        const Gr gr(g);
+        uint32_t x[1 << R];
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) x[j] = s[gr.at(j)];
+        dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+        const uint32_t bw =
+            mont_mul_pre(inter_twiddle(c, q, 1, (k2 * gr.base) & (uint32_t)(nn - 1), log_n, p), sw, swp, p);
+        const uint32_t bwp = bw * pinv;
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) row[gr.idx(j)] = mul2<LAZY>(x[j], sT[j], bw, bwp, p);
+    }
+}
+
 // The row pass of one row: row slot `slot`, prime and product from `by`
 // (prime + 3 * product), run by T threads on the shared slice `sm`; every
 // thread of the CTA takes the same barriers, so a CTA may hold several rows
@@ -509,7 +548,11 @@ __device__ __forceinline__ void mid_rows_body(const MidRowsArgs& a, uint32_t slo
 
     // The last DIT round's groups hold n1 = q + (j << LO0); the inverse
     // inter-pass twiddle omega_N^-(k2 n1) = B(q) * T^j with the row-constant
-    // powers sT[j] = omega_N^-(k2 j << LO0).
+    // powers sT[j] = omega_N^-(k2 j << LO0).  (row_inv_powers and
+    // row_dit_store do the same steps for the spectral row passes; they are
+    // written out here because routing this body through them changed the
+    // register allocation, and the spills, of the mixed-length row launch
+    // that inlines it.)
     constexpr int R0 = P1::r(0), LO0 = P1::lo(0);
     uint2* sT = reinterpret_cast<uint2*>(sm + ((SQR || ONE ? 1u : 2u) << L1));
     for (int t = tid; t < (1 << R0); t += T) {
@@ -579,6 +622,109 @@ template <int PS, int L1, int T, bool SQR>
 __global__ void __launch_bounds__(T, mid_min_blocks(L1, T)) k_mid_rows(const MidRowsArgs a) {
     extern __shared__ __align__(16) uint32_t sm[];
     mid_rows_body<PS, L1, T, SQR>(a, blockIdx.x, blockIdx.y, sm);
+}
+
+// ---- spectral sums: the row pass split at the pointwise product ----------------
+//
+// k_rows_dif finishes an operand block's forward transform: the row DIF of
+// row blockIdx.x, prime blockIdx.y, stored back in place with element i at
+// row[i] (the order the one-buffer row pass parks A's transform in).
+// k_rows_mac forms, per row, sum_t sa[t] (.) sb[t] over the launch's pairs of
+// such spectra (Montgomery products, so the sum carries 2^-32, which the scale
+// in the last round cancels) and runs the row DIT with the inverse
+// inter-pass twiddle into y, where the inverse column pass reads it.
+
+template <int PS, int L1, int T>
+__global__ void __launch_bounds__(T) k_rows_dif(const SpecArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];  // one row
+    constexpr bool LAZY = PS == 0;
+    constexpr int NR = Plan<L1>::nr;
+    static_assert(NR > 1, "the spectral row passes need several rounds");
+    const NttConsts& c = c_consts[a.slot];
+    const int q = (int)blockIdx.y;
+    const uint32_t p = c.pr[q].p;
+    const uint2* twf = c.stage[q][0];
+    uint32_t* row = a.y + (size_t)q * ((size_t)1 << a.log_n) + ((size_t)blockIdx.x << L1);
+    pdl_wait();
+    mid_dif_row<LAZY, L1, T, false>(row, sm, twf, p);
+    smem_round<LAZY, L1, 1, T, NR - 1, false>(sm, twf, p, threadIdx.x);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < (1u << L1); i += T) row[i] = sm[sidx<1>(i, 0)];
+    pdl_trigger();
+}
+
+// NT > 0: exactly NT terms, every term's loads of a group issued before its
+// products; NT == 0: any count up to kMaxSpecTerms, one term at a time.
+template <int PS, int L1, int T, int NT>
+__global__ void __launch_bounds__(T) k_rows_mac(const SpecArgs a) {
+    extern __shared__ __align__(16) uint32_t sm[];  // one row + the row's inverse powers
+    constexpr bool LAZY = PS == 0;
+    constexpr int NR = Plan<L1>::nr;
+    static_assert(NR > 1, "the spectral row passes need several rounds");
+    const NttConsts& c = c_consts[a.slot];
+    const int q = (int)blockIdx.y;
+    const uint32_t p = c.pr[q].p, pinv = c.pr[q].pinv;
+    const uint2* twi = c.stage[q][1];
+    const size_t nn = (size_t)1 << a.log_n;
+    const size_t off = (size_t)q * nn + ((size_t)blockIdx.x << L1);
+    const uint32_t k2 = bitrev(blockIdx.x, a.log_n2);
+    const uint32_t sw = q == 0 ? a.scale_w[0] : (q == 1 ? a.scale_w[1] : a.scale_w[2]);
+    const uint32_t swp = q == 0 ? a.scale_wp[0] : (q == 1 ? a.scale_wp[1] : a.scale_wp[2]);
+    uint2* sT = reinterpret_cast<uint2*>(sm + (1u << L1));
+    row_inv_powers<L1, T>(c, q, k2, a.log_n, nn, p, pinv, sT, threadIdx.x);
+    __syncthreads();
+    pdl_wait();
+    {  // the sum of products, then the first DIT round (the last DIF round's groups)
+        using Gr = Group<L1, 1, NR - 1>;
+        constexpr int R = Gr::R;
+#pragma unroll 2
+        for (int g = threadIdx.x; g < Gr::G; g += T) {
+            const Gr gr(g);
+            uint32_t x[1 << R];
+            if constexpr (NT > 0) {
+                // the last round's groups are 2^R consecutive elements from
+                // a multiple of 2^R (its LO is 0): 16-byte loads
+                static_assert(Gr::LO == 0 && R >= 2, "vector loads need whole 4-element runs");
+                uint32_t va[NT][1 << R], vb[NT][1 << R];
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    const uint4* pa = reinterpret_cast<const uint4*>(a.sa[t] + off + gr.base);
+                    const uint4* pb = reinterpret_cast<const uint4*>(a.sb[t] + off + gr.base);
+#pragma unroll
+                    for (int v = 0; v < (1 << R) / 4; ++v) {
+                        const uint4 wa = pa[v], wb = pb[v];
+                        va[t][4 * v] = wa.x, va[t][4 * v + 1] = wa.y, va[t][4 * v + 2] = wa.z, va[t][4 * v + 3] = wa.w;
+                        vb[t][4 * v] = wb.x, vb[t][4 * v + 1] = wb.y, vb[t][4 * v + 2] = wb.z, vb[t][4 * v + 3] = wb.w;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) {
+                    x[j] = pointwise<LAZY>(va[0][j], vb[0][j], p, pinv);
+#pragma unroll
+                    for (int t = 1; t < NT; ++t) x[j] = mod_add(x[j], pointwise<LAZY>(va[t][j], vb[t][j], p, pinv), p);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < (1 << R); ++j) x[j] = 0;
+#pragma unroll
+                for (int t = 0; t < kMaxSpecTerms; ++t) {  // constant indices into the parameters
+                    if (t >= a.nterms) break;
+                    const uint32_t* ra = a.sa[t] + off;
+                    const uint32_t* rb = a.sb[t] + off;
+#pragma unroll
+                    for (int j = 0; j < (1 << R); ++j)
+                        x[j] = mod_add(x[j], pointwise<LAZY>(ra[gr.idx(j)], rb[gr.idx(j)], p, pinv), p);
+                }
+            }
+            dit_regs<LAZY, R, Gr::HI, Gr::LO>(x, gr.base_low, twi, p);
+#pragma unroll
+            for (int j = 0; j < (1 << R); ++j) sm[gr.at(j)] = x[j];
+        }
+    }
+    __syncthreads();
+    dit_rounds<LAZY, L1, 1, T, NR - 2, 1>(sm, twi, p, threadIdx.x);
+    row_dit_store<LAZY, L1, T>(c, q, k2, a.log_n, nn, sw, swp, sm, sT, twi, p, pinv, a.y + off, threadIdx.x);
+    pdl_trigger();
 }
 
 // ---- kernel 3: inverse column pass + CRT + chunk sums -------------------------
@@ -1002,6 +1148,58 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     carry_block(product(a.descs, a.one, s_bid / a.bpp), s_bid % a.bpp, a.nchunks, a.out_fmt, a.epoch, a.err);
 }
 
+// Before the carry scan of a spectral sum that lands in a window of the
+// result already holding earlier sums: chunk c's value (4 limbs + 2^256 *
+// spill[c]) becomes twice itself when `twice` (a square's off-diagonal
+// pairs), plus limbs 4c..4c+3 of the window; the top limb past the chunks
+// (the carry scan's extra chunk, which is spill[nchunks-1]) takes window
+// limb 4 nchunks.  A chunk's overflow above 256 bits goes into its spill, so
+// the scan still sees chunk + spill below 2^257.  Spills stay below 2^61:
+// the coefficients are below 2^91, a chunk's top one shifted by 224 bits.
+struct ChunkMerge {
+    const uint64_t* add;  // window limbs to add, or nullptr
+    uint64_t nadd;
+    int twice;
+    uint64_t* chunks;  // the product's chunk sums and spills (set by the launcher)
+    uint64_t* spill;
+    uint32_t nchunks;
+};
+
+__global__ void __launch_bounds__(256) k_chunks_merge(const ChunkMerge m) {
+    pdl_wait();
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nchunks = m.nchunks;
+    if (c < nchunks) {
+        ulonglong2* p = reinterpret_cast<ulonglong2*>(m.chunks + (size_t)c * 4);
+        const ulonglong2 u = p[0], v = p[1];
+        uint64_t s[4] = {u.x, u.y, v.x, v.y};
+        uint64_t sp = m.spill[c];
+        if (m.twice) {
+            sp = (sp << 1) | (s[3] >> 63);
+            s[3] = (s[3] << 1) | (s[2] >> 63);
+            s[2] = (s[2] << 1) | (s[1] >> 63);
+            s[1] = (s[1] << 1) | (s[0] >> 63);
+            s[0] <<= 1;
+        }
+        const uint64_t base = (uint64_t)c * 4;
+        uint64_t cy = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint64_t w = base + k < m.nadd ? m.add[base + k] : 0ull;
+            const uint64_t t = s[k] + w;
+            const uint64_t r = t + cy;
+            cy = (uint64_t)(t < w) | (uint64_t)(r < t);
+            s[k] = r;
+        }
+        sp += cy;
+        if (c == nchunks - 1 && m.nadd > base + 4) sp += m.add[base + 4];
+        p[0] = make_ulonglong2(s[0], s[1]);
+        p[1] = make_ulonglong2(s[2], s[3]);
+        m.spill[c] = sp;
+    }
+    pdl_trigger();
+}
+
 // ---- host launchers -------------------------------------------------------------
 
 // Column length per transform length, as set by the tuner (0 = default
@@ -1147,6 +1345,71 @@ static cudaError_t dispatch_mid(int l1, const MidRowsArgs& m, bool square, uint3
     }
 }
 
+// Row lengths of the spectral row passes: several rounds (2^5 points and up);
+// the lazy set's transforms (up to 2^23 points) have rows of at most 2^14,
+// the strict set's (2^24 to 2^26 points, columns of at most 2^11) at least 2^13.
+static bool spec_rows_built(int ps, int l1) { return ps == 0 ? (l1 >= 5 && l1 <= 14) : (l1 >= 13 && l1 <= 15); }
+
+// Threads of the spectral row passes: rows of 2^13 points and more fill one
+// or two CTAs per SM (their shared rows take 32-128 KB), so these run 512
+// threads, twice the row pass's, for more global loads in flight.
+static constexpr int spec_threads(int l1) { return l1 >= 13 ? 512 : mid_threads(l1); }
+
+template <int PS, int L1, int NT>
+static cudaError_t launch_spec_mac(const SpecArgs& s, uint32_t rows, cudaStream_t st) {
+    constexpr int T = spec_threads(L1);
+    auto k = k_rows_mac<PS, L1, T, NT>;
+    const size_t sm = ((size_t)4 << L1) + 16 * sizeof(uint2);
+    allow_smem(k, sm);
+    return launch_k(k, dim3(rows, kNumPrimes), dim3(T), sm, st, s);
+}
+
+template <int PS, int L1>
+static cudaError_t launch_spec_rows(const SpecArgs& s, bool mac, uint32_t rows, cudaStream_t st) {
+    constexpr int T = spec_threads(L1);
+    const dim3 grid(rows, kNumPrimes);
+    if (mac) {
+        // the strict set's transforms are the large blocks, whose sums hold
+        // one or two products; other counts and the small blocks' sums take
+        // the general loop
+        if constexpr (PS == 1) {
+            if (s.nterms == 1) return launch_spec_mac<PS, L1, 1>(s, rows, st);
+            if (s.nterms == 2) return launch_spec_mac<PS, L1, 2>(s, rows, st);
+        }
+        return launch_spec_mac<PS, L1, 0>(s, rows, st);
+    }
+    auto k = k_rows_dif<PS, L1, T>;
+    const size_t sm = (size_t)4 << L1;
+    allow_smem(k, sm);
+    return launch_k(k, grid, dim3(T), sm, st, s);
+}
+
+template <int PS>
+static cudaError_t dispatch_spec_rows(int l1, const SpecArgs& s, bool mac, uint32_t rows, cudaStream_t st) {
+    if constexpr (PS == 0) {
+        switch (l1) {
+            case 5: return launch_spec_rows<0, 5>(s, mac, rows, st);
+            case 6: return launch_spec_rows<0, 6>(s, mac, rows, st);
+            case 7: return launch_spec_rows<0, 7>(s, mac, rows, st);
+            case 8: return launch_spec_rows<0, 8>(s, mac, rows, st);
+            case 9: return launch_spec_rows<0, 9>(s, mac, rows, st);
+            case 10: return launch_spec_rows<0, 10>(s, mac, rows, st);
+            case 11: return launch_spec_rows<0, 11>(s, mac, rows, st);
+            case 12: return launch_spec_rows<0, 12>(s, mac, rows, st);
+            case 13: return launch_spec_rows<0, 13>(s, mac, rows, st);
+            case 14: return launch_spec_rows<0, 14>(s, mac, rows, st);
+            default: return cudaErrorInvalidValue;
+        }
+    } else {
+        switch (l1) {
+            case 13: return launch_spec_rows<1, 13>(s, mac, rows, st);
+            case 14: return launch_spec_rows<1, 14>(s, mac, rows, st);
+            case 15: return launch_spec_rows<1, 15>(s, mac, rows, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+}
+
 uint32_t carry_blocks(uint32_t nchunks) {
     return (nchunks + 1 + kCarryChunksPerBlock - 1) / kCarryChunksPerBlock;
 }
@@ -1169,6 +1432,11 @@ static void set_scale(const NttConsts& c, int log_n, uint32_t* w, uint32_t* wp) 
 }
 
 // The four launches of `count` products (descs on the device, or `one`).
+static cudaError_t launch_inverse_carry(int slot, int ps, const ProductDesc* descs, const ProductDesc& one,
+                                        int count, const TransformShape& sh, int out_fmt,
+                                        const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev,
+                                        const ChunkMerge* merge = nullptr);
+
 static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDesc* descs,
                                    const ProductDesc& one, int count, bool square,
                                    const TransformShape& sh, int out_fmt, const CarryLaunch& cl,
@@ -1176,7 +1444,6 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
     const int log_n = sh.log_n;
     if (!shape_ok(sh, square) || log_n > c.log_max || count < 1) return cudaErrorInvalidValue;
     const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
-    const size_t nn = (size_t)1 << log_n;
     const uint32_t tiles = (1u << sh.log_n1) / kCols;
     if (ev) cudaEventRecord(ev[0], st);
 
@@ -1204,7 +1471,19 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
                 : dispatch_mid<1>(sh.log_n1, m, square, 1u << sh.log_n2, count, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[2], st);
+    return launch_inverse_carry(slot, ps, descs, one, count, sh, out_fmt, cl, st, ev);
+}
 
+// The inverse column pass (with CRT and chunk sums) and the carry scan of
+// `count` products whose row pass has run; `merge` (one product only) runs
+// k_chunks_merge between them.
+static cudaError_t launch_inverse_carry(int slot, int ps, const ProductDesc* descs, const ProductDesc& one,
+                                        int count, const TransformShape& sh, int out_fmt,
+                                        const CarryLaunch& cl, cudaStream_t st, cudaEvent_t* ev,
+                                        const ChunkMerge* merge) {
+    const int log_n = sh.log_n;
+    const size_t nn = (size_t)1 << log_n;
+    const uint32_t tiles = (1u << sh.log_n1) / kCols;
     InvColsArgs iv{};
     iv.descs = descs;
     iv.one = one;
@@ -1212,10 +1491,18 @@ static cudaError_t launch_ntt_core(int slot, const NttConsts& c, const ProductDe
     iv.log_n1 = sh.log_n1;
     iv.slot = slot;
     iv.err = cl.err;
-    e = ps == 0 ? dispatch_outer<0>(sh.log_n2, nullptr, &iv, tiles, count, st)
+    cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, nullptr, &iv, tiles, count, st)
                 : dispatch_outer<1>(sh.log_n2, nullptr, &iv, tiles, count, st);
     if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[3], st);
+    if (merge) {
+        ChunkMerge mg = *merge;
+        mg.chunks = one.chunks;
+        mg.spill = one.spill;
+        mg.nchunks = (uint32_t)(nn / kCols);
+        e = launch_k(k_chunks_merge, dim3((mg.nchunks + 255) / 256), dim3(256), 0, st, mg);
+        if (e != cudaSuccess) return e;
+    }
 
     CarryArgs ca{};
     ca.descs = descs;
@@ -1269,6 +1556,78 @@ cudaError_t launch_ntt_batch(int slot, const NttConsts& c, const ProductDesc* de
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+bool spectral_supported(int log_n) {
+    const TransformShape sh = choose_shape(log_n);
+    return shape_ok(sh, false) && spec_rows_built(prime_set_for(log_n), sh.log_n1);
+}
+
+cudaError_t launch_ntt_spectrum(int slot, const NttConsts& c, const OperandDesc& a, int log_n, uint32_t* spec,
+                                cudaStream_t st) {
+    const TransformShape sh = choose_shape(log_n);
+    const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
+    if (!spectral_supported(log_n) || log_n > c.log_max || ps != prime_set_for(log_n))
+        return cudaErrorInvalidValue;
+    ProductDesc one{};
+    one.op[0] = one.op[1] = a;
+    one.y = spec;
+    FwdColsArgs f{};
+    f.one = one;
+    f.nops = 1;
+    f.log_n = log_n;
+    f.log_n1 = sh.log_n1;
+    f.slot = slot;
+    const uint32_t tiles = (1u << sh.log_n1) / kCols;
+    cudaError_t e = ps == 0 ? dispatch_outer<0>(sh.log_n2, &f, nullptr, tiles, 1, st)
+                            : dispatch_outer<1>(sh.log_n2, &f, nullptr, tiles, 1, st);
+    if (e != cudaSuccess) return e;
+    SpecArgs s{};
+    s.y = spec;
+    s.log_n = log_n;
+    s.log_n2 = sh.log_n2;
+    s.slot = slot;
+    return ps == 0 ? dispatch_spec_rows<0>(sh.log_n1, s, false, 1u << sh.log_n2, st)
+                   : dispatch_spec_rows<1>(sh.log_n1, s, false, 1u << sh.log_n2, st);
+}
+
+cudaError_t launch_ntt_spectral_sum(int slot, const NttConsts& c, const uint32_t* const* sa,
+                                    const uint32_t* const* sb, int nterms, bool twice, int log_n,
+                                    const ProductScratch& scr, uint64_t* out, size_t out_cap,
+                                    const uint64_t* add, size_t nadd, const CarryLaunch& cl,
+                                    cudaStream_t st) {
+    const TransformShape sh = choose_shape(log_n);
+    const int ps = c.log_max == kPrimeSets[0].log_max ? 0 : 1;
+    if (!spectral_supported(log_n) || log_n > c.log_max || ps != prime_set_for(log_n) || nterms < 1 ||
+        nterms > kMaxSpecTerms)
+        return cudaErrorInvalidValue;
+    SpecArgs s{};
+    for (int t = 0; t < nterms; ++t) {
+        s.sa[t] = sa[t];
+        s.sb[t] = sb[t];
+    }
+    s.nterms = nterms;
+    s.y = scr.y;
+    s.log_n = log_n;
+    s.log_n2 = sh.log_n2;
+    s.slot = slot;
+    set_scale(c, log_n, s.scale_w, s.scale_wp);
+    cudaError_t e = ps == 0 ? dispatch_spec_rows<0>(sh.log_n1, s, true, 1u << sh.log_n2, st)
+                            : dispatch_spec_rows<1>(sh.log_n1, s, true, 1u << sh.log_n2, st);
+    if (e != cudaSuccess) return e;
+    ProductDesc one{};
+    one.y = scr.y;
+    one.chunks = scr.chunks;
+    one.spill = scr.spill;
+    one.flags = scr.flags;
+    one.out = out;
+    one.out_cap = out_cap;
+    CarryLaunch c2 = cl;
+    c2.ticket = scr.ticket;
+    c2.err = scr.err;
+    const ChunkMerge merge{add, add ? (uint64_t)nadd : 0ull, twice ? 1 : 0, nullptr, nullptr, 0};
+    return launch_inverse_carry(slot, ps, nullptr, one, 1, sh, kFmtLimb64, c2, st, nullptr,
+                                (add || twice) ? &merge : nullptr);
 }
 
 cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t nchunks, void* out,

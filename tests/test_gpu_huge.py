@@ -1,13 +1,18 @@
 """Products beyond the largest transform (2^26 points, 2^31 product bits).
 
 The reference switches to Schoenhage-Strassen there (src/mul/ssa.cpp:383);
-the engine cuts both operands into 2^30-bit blocks, multiplies every block
-pair on the NTT and adds the block products into the result with a device
-carry scan.  At these sizes the CPU oracle takes minutes, so the checks are
-size-independent: the residue identity mod 2^61-1, the low limb, operand
-order, and the all-ones closed form, whose carries cross every block
-boundary.  The block path itself is also run with small blocks (the
-bgpu_set_block_limbs test hook) and compared limb-exact with the oracle."""
+the engine cuts both operands into 2^30-bit blocks, transforms every block
+once, forms each output block's sum of block products in the transform
+domain (at most as many products per sum as the CRT modulus allows: two at
+this block size), inverse-transforms each sum and adds it into the result
+with a device carry scan.  At these sizes the CPU oracle takes minutes, so
+the checks are size-independent: the residue identity mod 2^61-1, the low
+limb, operand order, and the all-ones closed form, whose carries cross every
+block boundary and whose coefficients are the largest the bound admits.  The
+block path is also run with small blocks (the bgpu_set_block_limbs test hook)
+and compared limb-exact with the oracle, with 2^22-limb blocks on the strict
+prime set against one whole transform, and with rows too short for the
+spectral row passes, where every block pair is one NTT product."""
 from __future__ import annotations
 
 import numpy as np
@@ -28,7 +33,8 @@ def check_product(port, a, b, c):
 
 
 def test_general_2p31_product(bb, port):
-    """2^31 x 2^31 bits: four block products."""
+    """2^31 x 2^31 bits: two blocks each, three spectral sums (the middle one
+    of two block products)."""
     rng = np.random.default_rng(SEED + 500)
     n = 2 * BLOCK
     a, b = rand_limbs(rng, n), rand_limbs(rng, n)
@@ -138,9 +144,11 @@ def small_blocks(bb):
 @pytest.mark.parametrize("na,nb", [(4096, 4096), (3000, 5000), (1025, 9000), (1 << 13, 1 << 13),
                                    (10000, 1500), (2049, 2049)])
 def test_block_path_small_blocks_vs_oracle(bb, port, small_blocks, na, nb):
-    """Blocks of 2^10 limbs: every product above 2^12 points runs as block
-    products plus carry-scan accumulation; ragged last blocks, unbalanced
-    block counts and squares, limb-exact against the oracle."""
+    """Blocks of 2^10 limbs: every product above 2^12 points runs as spectral
+    sums of block products (up to four per sum at this block size, so the
+    8 x 8-block case splits its longest sums) plus carry-scan accumulation;
+    ragged last blocks, unbalanced block counts and squares, limb-exact
+    against the oracle."""
     rng = np.random.default_rng(SEED + 300 + na + 3 * nb)
     a, b = rand_limbs(rng, na), rand_limbs(rng, nb)
     assert np.array_equal(bb.ntt_mul(a, b), port.mul(a, b))
@@ -165,6 +173,44 @@ def test_block_path_small_blocks_all_ones_and_device_entry(bb, port, small_block
     rng = np.random.default_rng(SEED + 310)
     da_, db_ = rand_digits(rng, 9000), rand_digits(rng, 7000)
     assert np.array_equal(bb.mul_digits(da_, db_), port.mul_digits(da_, db_))
+
+
+def test_spectral_strict_primes_vs_one_transform(bb, port):
+    """2^22-limb blocks: 2^24-point block spectra on the strict prime set
+    (rows of 2^13 points), for a product and a square that also fit one
+    2^26-point transform; both ways agree limb for limb."""
+    rng = np.random.default_rng(SEED + 506)
+    blk = 1 << 22
+    a, b = rand_limbs(rng, 3 * blk + 5), rand_limbs(rng, 2 * blk + 7)
+    want, want_sq = bb.ntt_mul(a, b), bb.ntt_mul(a)
+    bb.set_block_limbs(blk)
+    try:
+        got, got_sq = bb.ntt_mul(a, b), bb.ntt_mul(a)
+        got_ba = bb.ntt_mul(b, a)
+    finally:
+        bb.set_block_limbs(0)
+    check_product(port, a, b, got)
+    assert np.array_equal(got, want)
+    assert np.array_equal(got_ba, want)
+    assert np.array_equal(got_sq, want_sq)
+
+
+def test_pairwise_block_path_vs_oracle(bb, port):
+    """64-limb blocks on a 2^8-point transform split into rows of 2^4 points,
+    too short for the spectral row passes: every block pair is one NTT
+    product added at its offset; limb-exact against the oracle."""
+    rng = np.random.default_rng(SEED + 507)
+    old = bb.get_split(8)
+    bb.set_block_limbs(64)
+    bb.set_split(8, 4)
+    try:
+        a, b = rand_limbs(rng, 700), rand_limbs(rng, 300)
+        got, sq = bb.ntt_mul(a, b), bb.ntt_mul(a)
+    finally:
+        bb.set_split(8, old)
+        bb.set_block_limbs(0)
+    assert np.array_equal(got, port.mul(a, b))
+    assert np.array_equal(sq, port.mul(a))
 
 
 def test_block_limbs_hook_rejects_bad_sizes(bb):
