@@ -1,16 +1,18 @@
-// Products beyond the largest transform.
+// Limb accumulation: out[0, L) += add[0, nadd) with full carry propagation.
 //
-// The three-prime NTT stops at 2^26 points (2^31 product bits).  The
-// reference goes on with Schoenhage-Strassen (src/mul/ssa.cpp:383, chosen by
-// _mul above its NTT capacity, include/bigint/mul.h:199-205).  Here both
-// operands are cut into blocks of kHugeBlockLimbs limbs (2^30 bits); every
-// pair of blocks is one 2^26-point NTT product (3.9 ms for a 2^30-bit square
-// on a B200), and each block product is added into the result at its limb
-// offset by a carry scan over the rest of the result:
+// Used by the pairwise fallback for products beyond the largest transform
+// (the three-prime NTT stops at 2^26 points, 2^31 product bits; the reference
+// goes on with Schoenhage-Strassen, src/mul/ssa.cpp:383, chosen by _mul above
+// its NTT capacity, include/bigint/mul.h:199-205): there every pair of
+// operand blocks is one NTT product, added into the result at its limb offset
+// by a carry scan over the rest of the result,
 //   A * B = sum_{i,j} (A_i * B_j) * 2^(64 S (i + j)).
-// The accumulation is three launches per block product -- per-block
-// (generate, propagate) aggregates, one block scanning them, every block
-// applying its carry-in -- with no inter-block waits.
+// (The default form for those sizes, the spectral sums in engine.cu, carries
+// each sum into its window of the result and needs no accumulation.)  Also
+// used by the decimal conversions (their power tables and level sums).  Three launches per
+// accumulation -- per-block (generate, propagate) aggregates, one block
+// scanning them, every block applying its carry-in -- with no inter-block
+// waits.
 #include <cuda_runtime.h>
 
 #include <cstdint>
