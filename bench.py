@@ -43,7 +43,23 @@ if ROOT not in sys.path:
 SEED = 0x9E3779B97F4A7C15
 CONFIG_INDEX = 1  # the plain-NTT size sweep's 2^24-bit point
 OPERAND_BITS = 1 << 24
-L2_BYTES = 126 << 20  # B200 L2; inputs of all operand pairs together exceed it
+L2_BYTES_B200 = 126 << 20  # B200's L2, when no device answers
+
+
+def l2_bytes() -> int:
+    """The device's L2 size (cudaDevAttrL2CacheSize, through torch's device
+    properties), or B200's 126 MB without a device: the timed inputs of all
+    operand pairs together must exceed it."""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            n = int(getattr(torch.cuda.get_device_properties(torch.cuda.current_device()), "L2_cache_size", 0))
+            if n > 0:
+                return n
+    except Exception:
+        pass
+    return L2_BYTES_B200
 
 
 def make_operands(bits: int = OPERAND_BITS, seed: int = SEED + CONFIG_INDEX, pairs: int = 1):
@@ -62,7 +78,7 @@ def make_operands(bits: int = OPERAND_BITS, seed: int = SEED + CONFIG_INDEX, pai
 def pairs_beyond_l2(bits: int) -> int:
     """Distinct operand pairs whose inputs together are twice the L2 cache."""
     per_pair = 2 * bits // 8
-    return max(2, -(-2 * L2_BYTES // per_pair))
+    return max(2, -(-2 * l2_bytes() // per_pair))
 
 
 def host_cores() -> int:
