@@ -1302,6 +1302,27 @@ def run_gpu_arm(args) -> None:
     bb.device_status(sptr)
     seq_ms = reduce_max(statistics.median(seq_win), world, device)
 
+    # Diagnostic of the host launches: the same K products enqueued behind a
+    # bounded GPU sleep (torch.cuda._sleep, four times their host issue time),
+    # so every launch is queued before the first product starts.  When the
+    # timed windows' launches are hidden, both give the same time per product.
+    sleep_cycles = int(min(2e9, 4 * max(issue) * 2.0e9))
+
+    def prequeued_window(first_step):
+        torch.cuda.synchronize(device)
+        with torch.cuda.stream(stream):
+            torch.cuda._sleep(sleep_cycles)
+            t0.record(stream)
+            for i in range(args.steps):
+                step(first_step + i)
+            t1.record(stream)
+        torch.cuda.synchronize(device)
+        return t0.elapsed_time(t1)
+
+    preq_win = [prequeued_window(args.warmup + w * args.steps) for w in range(5)]
+    bb.device_status(sptr)
+    preq_ms = reduce_max(statistics.median(preq_win), world, device)
+
     # Roofline pass: the same K products again with CUDA events recorded on
     # the launching stream between the kernels of every product (kept out of
     # the timed region above because an event between two kernels stops the
@@ -1437,7 +1458,11 @@ def run_gpu_arm(args) -> None:
                                   "max": max(win_ms), "count": nwin},
                    "host_issue_us_per_product": statistics.median(issue) / args.steps * 1e6,
                    "host_issue_note": "host time to enqueue one product (4 launches through the C-ABI); "
-                                      "below the device time per product, the launches are hidden"},
+                                      "below the device time per product, the launches are hidden",
+                   "prequeued_us_per_product": preq_ms / args.steps * 1e3,
+                   "prequeued_note": "the same K products with every launch queued before the first one "
+                                     "starts (behind a GPU sleep), median of 5 windows: equal to ms_per_step "
+                                     "when the timed windows' host launches are hidden"},
         "sequential": {"ms_per_step": seq_ms / args.steps, "value": world * args.steps / (seq_ms * 1e-3),
                        "note": "the same products without BGPU_INDEPENDENT, each after the previous "
                                f"(median of {len(seq_win)} windows)"},
