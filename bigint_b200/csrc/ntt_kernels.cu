@@ -1155,7 +1155,9 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
 // (the carry scan's extra chunk, which is spill[nchunks-1]) takes window
 // limb 4 nchunks.  A chunk's overflow above 256 bits goes into its spill, so
 // the scan still sees chunk + spill below 2^257.  Spills stay below 2^61:
-// the coefficients are below 2^91, a chunk's top one shifted by 224 bits.
+// the coefficients are below 2^91, a chunk's top one shifted by 224 bits, and
+// the window's top limb is 0 before its first sum and after it below the
+// number of block products carried there.
 struct ChunkMerge {
     const uint64_t* add;  // window limbs to add, or nullptr
     uint64_t nadd;
