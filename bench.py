@@ -1074,6 +1074,19 @@ def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5, ref_
     bb.device_status(sp)
     launches = plan.launches
     plan.close()
+    # the same batch with every NTT class on its own launches (parallel graph
+    # branches): the alternative form, timed and compared beside the default
+    plan_pc = bb.BatchPlan(prods, flags=bb.BGPU_BATCH_PER_CLASS)
+    dout.zero_()
+    for _ in range(2):
+        plan_pc.run(sp)
+    bb.device_status(sp)
+    ms_pc = _event_ms(torch, stream, lambda i: plan_pc.run(sp), runs)
+    bb.device_status(sp)
+    launches_pc = plan_pc.launches
+    plan_pc.close()
+    if not np.array_equal(dout.cpu().numpy().view(np.uint64), host):
+        raise SystemExit("bench batched: the per-class launch sets differ from the default plan")
     verified = "residue mod 2^61-1 and identical to one plain NTT call, every product"
     from oracle.pyoracle import Reference, have_reference
 
@@ -1091,6 +1104,10 @@ def batched_form(bb, torch, device, port, nprod: int = 4096, runs: int = 5, ref_
             "batched": {"ms_per_batch": ms_batch, "products_per_s": nprod / (ms_batch * 1e-3),
                         "launches_per_batch": launches, "graph_launches": 1,
                         "plan_build_s": t_plan},
+            "per_class_launch_sets": {"ms_per_batch": ms_pc, "products_per_s": nprod / (ms_pc * 1e-3),
+                                      "launches_per_batch": launches_pc, "speedup": ms_single / ms_pc,
+                                      "note": "BGPU_BATCH_PER_CLASS: every NTT class its own four "
+                                              "launches on parallel graph branches; same outputs"},
             "one_plain_ntt_launch_per_product": {"ms": ms_single,
                                                  "products_per_s": nprod / (ms_single * 1e-3),
                                                  "launches": 4 * nprod},

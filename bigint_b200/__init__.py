@@ -33,6 +33,7 @@ from __future__ import annotations
 from ._lib import (  # noqa: F401
     BGPU_FFT_AVERAGE_BOUND,
     BGPU_INDEPENDENT,
+    BGPU_BATCH_PER_CLASS,
     BGPU_METHOD_AUTO,
     BGPU_METHOD_FFT,
     BGPU_METHOD_KARATSUBA,

@@ -19,6 +19,7 @@ BGPU_METHOD_FFT = 3
 BGPU_METHOD_KARATSUBA = 4
 BGPU_FFT_AVERAGE_BOUND = 0x10
 BGPU_INDEPENDENT = 0x20  # mul_device: operands not written by work in flight on the stream
+BGPU_BATCH_PER_CLASS = 0x40  # BatchPlan: every NTT class its own launches on parallel graph branches
 BGPU_TUNE_SCHOOLBOOK_MAX_LIMBS = 1
 BGPU_TUNE_BATCH_SCHOOLBOOK_MAX_LIMBS = 2
 BGPU_TUNE_FFT_MIN_LIMBS = 3

@@ -164,7 +164,6 @@ int batch_record(bgpu_batch_plan_s* p, cudaStream_t st, const EngineHooks& hooks
 
 int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, int device,
                       const EngineHooks& hooks, bgpu_batch_plan_s** out) {
-    (void)flags;
     auto* p = new (std::nothrow) bgpu_batch_plan_s();
     if (!p) return BGPU_ERR_OOM;
     p->device = device;
@@ -222,14 +221,16 @@ int batch_plan_create(const bgpu_product* prods, size_t count, uint32_t flags, i
         scratch += c.members.size() * ntt_scratch_bytes(c.log_n, c.square);
     }
     // The mixed-length launches take every class when each qualifies and
-    // there are several lengths; a single length runs its own per-length
+    // there are several lengths, unless the caller asks for per-class launch
+    // sets (BGPU_BATCH_PER_CLASS); a single length runs its own per-length
     // kernels (tuned for it, without the mixed launches' register budget):
     // a uniform batch of the decimal conversions' levels ran 5.6 -> 9.0 ms
     // per 1.26 M-digit print through the mixed launches.
 #ifndef BGPU_MIXED_BATCH
 #define BGPU_MIXED_BATCH 1
 #endif
-    p->mixed = BGPU_MIXED_BATCH && p->classes.size() >= 2 && p->classes.size() <= (size_t)kMaxMixedClasses;
+    p->mixed = BGPU_MIXED_BATCH && !(flags & BGPU_BATCH_PER_CLASS) && p->classes.size() >= 2 &&
+               p->classes.size() <= (size_t)kMaxMixedClasses;
     for (auto& c : p->classes) p->mixed = p->mixed && mixed_class_ok(c.log_n, c.square);
     const size_t mixed_off = al256(n_desc * sizeof(ProductDesc));
     const size_t school_off = mixed_off + al256((p->mixed ? p->classes.size() : 0) * sizeof(MixedClass));

@@ -77,7 +77,7 @@ def test_batch_rejects_bad_descriptor(bb):
     assert e.value.code == -1
 
 
-def _run_plan_and_check(bb, port, torch, A, B, square_idx=()):
+def _run_plan_and_check(bb, port, torch, A, B, square_idx=(), flags=0):
     dA, dB = _to_dev(torch, A), _to_dev(torch, B)
     for i in square_idx:
         dB[i] = dA[i]
@@ -85,7 +85,7 @@ def _run_plan_and_check(bb, port, torch, A, B, square_idx=()):
                        device="cuda") for i, (a, b) in enumerate(zip(A, B))]
     prods = [(dA[i].data_ptr(), A[i].size, dB[i].data_ptr(), A[i].size if i in square_idx else B[i].size,
               outs[i].data_ptr()) for i in range(len(A))]
-    plan = bb.BatchPlan(prods)
+    plan = bb.BatchPlan(prods, flags=flags)
     launches = plan.launches
     for _ in range(2):
         plan.run(0)
@@ -107,6 +107,17 @@ def test_batch_one_launch_per_pass_with_small_products(bb, port):
     A, B = _make_batch(torch, rng, 200, 6, 17, ones_every=13)
     A[3] = A[2]
     assert _run_plan_and_check(bb, port, torch, A, B, square_idx=(3,)) == 4
+
+
+def test_batch_per_class_flag(bb, port):
+    """BGPU_BATCH_PER_CLASS: the same kind of batch as the mixed-launch test,
+    every class on its own four launches (graph branches), same results."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(SEED + 42)
+    A, B = _make_batch(torch, rng, 200, 6, 17, ones_every=13)
+    A[3] = A[2]
+    launches = _run_plan_and_check(bb, port, torch, A, B, square_idx=(3,), flags=bb.BGPU_BATCH_PER_CLASS)
+    assert launches > 4
 
 
 def test_batch_with_a_long_class_runs_per_class(bb, port):
