@@ -219,7 +219,7 @@ int prepare_scratch(int log_n, bool square, ProductScratch* s) {
     const size_t y_bytes = align256((square ? 1 : 2) * (size_t)kNumPrimes * nn * 4);
     const size_t ch_bytes = align256(nn / 2 * 8);
     const size_t sp_bytes = align256(nn / 8 * 8);
-    const size_t fl_bytes = align256((size_t)carry_blocks((uint32_t)(nn / 8)) * 8);
+    const size_t fl_bytes = align256((size_t)carry_blocks_narrow((uint32_t)(nn / 8)) * 8);  // either shape
     int rc = ensure(&g.d_scratch, &g.scratch_bytes, y_bytes + ch_bytes + sp_bytes + fl_bytes);
     if (rc != BGPU_OK) return rc;
     char* b = static_cast<char*>(g.d_scratch);
@@ -254,10 +254,12 @@ int multiply_device(const OperandDesc& a, const OperandDesc& b, bool square, voi
     // only an identical layout keeps this forward pass's planes clear of the
     // previous product's carry data while that scan still runs.
     cl.overlap_prev = overlap_prev && st == g.ntt_stream && ln == g.ntt_log_n && square == g.ntt_square;
+    cl.narrow = !cl.overlap_prev;
     g.ntt_stream = st;
     g.ntt_log_n = ln;
     g.ntt_square = square;
-    g.ticket_base += carry_blocks((uint32_t)(((size_t)1 << ln) / 8));
+    const uint32_t nch = (uint32_t)(((size_t)1 << ln) / 8);
+    g.ticket_base += cl.narrow ? carry_blocks_narrow(nch) : carry_blocks(nch);
     cudaEvent_t* ev = nullptr;
     if (g.kernel_timing) {
         ev = g.kev.data() + (g.kev_count % kTimingRing) * (kNttLaunches + 1);

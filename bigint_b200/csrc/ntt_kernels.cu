@@ -926,22 +926,24 @@ cudaError_t launch_wait_selftest(const uint64_t* flag, uint64_t epoch, uint32_t 
 // Block `bid` of one product's carry scan over `nchunks` chunks, writing the
 // output in `out_fmt`; blocks of the same product must hold increasing
 // tickets of one launch (their look-back waits only on earlier blocks).
+template <int TH, int PER>
 __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid, uint32_t nchunks, int out_fmt,
                                             uint64_t epoch, uint32_t* err) {
+    constexpr uint32_t CPB = (uint32_t)(TH * PER);  // chunks per block
     __shared__ uint32_t s_cin, s_win_g, s_win_p;
-    __shared__ uint32_t s_wg[kCarryThreads / 32], s_wp[kCarryThreads / 32];
+    __shared__ uint32_t s_wg[TH / 32], s_wp[TH / 32];
     const uint64_t* chunks = pd.chunks;
     const uint64_t* spill = pd.spill;
     uint64_t* flags = pd.flags;
     const size_t out_cap = pd.out_cap;
     const uint32_t ntot = nchunks + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t wbase = (bid * kCarryThreads + (uint32_t)warp * 32) * kCarryPer;
+    const uint32_t wbase = (bid * TH + (uint32_t)warp * 32) * PER;
 
     // every load first: chunk words and the spill of the chunk before
-    uint64_t S[kCarryPer][4], sp[kCarryPer];
+    uint64_t S[PER][4], sp[PER];
 #pragma unroll
-    for (int i = 0; i < kCarryPer; ++i) {
+    for (int i = 0; i < PER; ++i) {
         const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
         if (cc < nchunks) {
             const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)cc * 4);
@@ -957,7 +959,7 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
     // carry into the block is the G of the highest of them that does not
     // propagate, found without waiting on any other block.
     if (warp == 0) {
-        const int64_t j = (int64_t)bid * kCarryChunksPerBlock - 32 + lane;
+        const int64_t j = (int64_t)bid * CPB - 32 + lane;
         uint32_t g = 0, pbit = 0;  // below chunk 0: no carry, nothing propagates
         if (j >= 0) {
             const ulonglong2* src = reinterpret_cast<const ulonglong2*>(chunks + (size_t)j * 4);
@@ -981,10 +983,10 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
         }
     }
     // per-chunk (G, P) and per-segment ballots
-    uint32_t gm[kCarryPer], bm[kCarryPer];
+    uint32_t gm[PER], bm[PER];
     uint32_t G = 0, P = 1;  // warp aggregate over its segments
 #pragma unroll
-    for (int i = 0; i < kCarryPer; ++i) {
+    for (int i = 0; i < PER; ++i) {
         const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
         uint32_t g = 0, pbit = 1;  // chunks past the end pass carries through untouched
         if (cc < ntot) {
@@ -1015,7 +1017,7 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t bG = 0, bP = 1;
-        for (int w = 0; w < kCarryThreads / 32; ++w) {
+        for (int w = 0; w < TH / 32; ++w) {
             bG = s_wg[w] | (s_wp[w] & bG);
             bP = bP & s_wp[w];
         }
@@ -1057,9 +1059,9 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
     __syncthreads();
     uint32_t cw = s_cin;  // carry into this warp's first segment
     for (int w = 0; w < warp; ++w) cw = s_wg[w] | (s_wp[w] & cw);
-    uint32_t cout[kCarryPer];  // carry out of each of this lane's chunks
+    uint32_t cout[PER];  // carry out of each of this lane's chunks
 #pragma unroll
-    for (int i = 0; i < kCarryPer; ++i) {
+    for (int i = 0; i < PER; ++i) {
         const uint64_t sum = (uint64_t)gm[i] + bm[i] + cw;
         const uint32_t carries = (uint32_t)sum ^ gm[i] ^ bm[i];
         const uint32_t cin = (carries >> lane) & 1u;
@@ -1078,7 +1080,7 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
         uint64_t* o = static_cast<uint64_t*>(pd.out);
         const bool vec = (reinterpret_cast<uintptr_t>(o) & 15u) == 0;  // 16-byte stores when aligned
 #pragma unroll
-        for (int i = 0; i < kCarryPer; ++i) {
+        for (int i = 0; i < PER; ++i) {
             const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
             if (cc >= ntot) continue;
             const size_t base = (size_t)cc * 4;
@@ -1102,7 +1104,7 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
         uint32_t* o = static_cast<uint32_t*>(pd.out);
         const uint64_t mask = (1u << 28) - 1u;
 #pragma unroll
-        for (int i = 0; i < kCarryPer; ++i) {
+        for (int i = 0; i < PER; ++i) {
             const uint32_t cc = wbase + (uint32_t)i * 32 + lane;
             if (cc >= ntot) continue;
             uint64_t nl = (cc + 1 < nchunks) ? chunks[(size_t)(cc + 1) * 4] : 0;
@@ -1131,7 +1133,8 @@ __device__ __forceinline__ void carry_block(const ProductDesc& pd, uint32_t bid,
     }
 }
 
-__global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
+template <int TH, int PER>
+__global__ void __launch_bounds__(TH) k_carry(const CarryArgs a) {
     __shared__ uint32_t s_bid;
     if (threadIdx.x == 0) s_bid = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticket_base);
     __syncthreads();
@@ -1145,7 +1148,8 @@ __global__ void __launch_bounds__(kCarryThreads) k_carry(const CarryArgs a) {
     }
     // tickets enumerate (product, block) in order, so a block's predecessor
     // within its product always holds a smaller ticket
-    carry_block(product(a.descs, a.one, s_bid / a.bpp), s_bid % a.bpp, a.nchunks, a.out_fmt, a.epoch, a.err);
+    carry_block<TH, PER>(product(a.descs, a.one, s_bid / a.bpp), s_bid % a.bpp, a.nchunks, a.out_fmt, a.epoch,
+                         a.err);
 }
 
 // Before the carry scan of a spectral sum that lands in a window of the
@@ -1416,6 +1420,11 @@ uint32_t carry_blocks(uint32_t nchunks) {
     return (nchunks + 1 + kCarryChunksPerBlock - 1) / kCarryChunksPerBlock;
 }
 
+uint32_t carry_blocks_narrow(uint32_t nchunks) {
+    constexpr uint32_t cpb = (uint32_t)(kCarryNarrowThreads * kCarryNarrowPer);
+    return (nchunks + 1 + cpb - 1) / cpb;
+}
+
 static uint32_t mont_of(uint64_t v, uint32_t p) { return (uint32_t)((v % p << 32) % p); }
 
 // The row pass's scale per prime: the pointwise Montgomery product leaves a
@@ -1510,13 +1519,19 @@ static cudaError_t launch_inverse_carry(int slot, int ps, const ProductDesc* des
     ca.descs = descs;
     ca.one = one;
     ca.nchunks = (uint32_t)(nn / kCols);
-    ca.bpp = carry_blocks(ca.nchunks);
     ca.out_fmt = out_fmt;
     ca.ticket = cl.ticket;
     ca.ticket_base = cl.ticket_base;
     ca.epoch = cl.epoch;
     ca.err = cl.err;
-    e = launch_k(k_carry, dim3(ca.bpp * count), dim3(kCarryThreads), 0, st, ca);
+    if (cl.narrow && count == 1) {
+        ca.bpp = carry_blocks_narrow(ca.nchunks);
+        e = launch_k(k_carry<kCarryNarrowThreads, kCarryNarrowPer>, dim3(ca.bpp), dim3(kCarryNarrowThreads), 0, st,
+                     ca);
+    } else {
+        ca.bpp = carry_blocks(ca.nchunks);
+        e = launch_k(k_carry<kCarryThreads, kCarryPer>, dim3(ca.bpp * count), dim3(kCarryThreads), 0, st, ca);
+    }
     if (ev) cudaEventRecord(ev[4], st);
     return e;
 }
@@ -1648,7 +1663,7 @@ cudaError_t launch_carry(const uint64_t* chunks, const uint64_t* spill, uint32_t
     ca.ticket_base = cl.ticket_base;
     ca.epoch = cl.epoch;
     ca.err = s.err;
-    return launch_k(k_carry, dim3(ca.bpp), dim3(kCarryThreads), 0, st, ca);
+    return launch_k(k_carry<kCarryThreads, kCarryPer>, dim3(ca.bpp), dim3(kCarryThreads), 0, st, ca);
 }
 
 // ---- mixed-length batches: one launch per pass for every class -------------
@@ -1781,7 +1796,8 @@ __global__ void __launch_bounds__(kCarryThreads) k_mixed_carry(const MixedArgs m
     }
     const MixedClass& k = m.classes[mixed_class(m, 3, s_t)];
     const uint32_t local = s_t - k.begin[3];
-    carry_block(k.fwd.descs[local / k.bpp], local % k.bpp, k.nchunks, kFmtLimb64, m.epoch, m.err);
+    carry_block<kCarryThreads, kCarryPer>(k.fwd.descs[local / k.bpp], local % k.bpp, k.nchunks, kFmtLimb64, m.epoch,
+                                          m.err);
 }
 
 bool mixed_class_ok(int log_n, bool square) {
