@@ -391,10 +391,11 @@ cudaError_t launch_extent(const uint32_t* d, uint32_t n, uint32_t from0, uint32_
 cudaError_t launch_shift_digits(const uint32_t* v, uint32_t n, uint32_t s, bool left, uint32_t* out,
                                 cudaStream_t st);
 
-// Products beyond the largest transform (huge.cu): out[0..L) += add[0..nadd)
-// (nadd <= L) with the carry carried through all of out; agg and cin hold
-// accumulate_blocks(L) words each.  kHugeBlockLimbs is the operand block of
-// the block decomposition: two blocks make the largest general NTT product.
+// Limb accumulation (huge.cu): out[0..L) += add[0..nadd) (nadd <= L) with the
+// carry carried through all of out; agg and cin hold accumulate_blocks(L)
+// words each (the pairwise block products' fallback and the decimal
+// conversions).  kHugeBlockLimbs is the operand block of products beyond the
+// largest transform: a pair of blocks fills the largest NTT transform.
 constexpr uint64_t kHugeBlockLimbs = (uint64_t)1 << 24;
 // Limbs per leaf of the decimal printer: one thread prints a leaf by repeated
 // division by 10^9, its work growing with the square of the leaf.
