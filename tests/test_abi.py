@@ -139,3 +139,28 @@ def test_point_positions_beyond_the_bound_rejected_on_host(lib):
         assert lib.bgpu_bigfloat_to_decimal(pd, 4, bad, 0, 0, buf, 16, C.byref(n)) == -4
         assert lib.bgpu_reciprocal_digits(pd, 4, bad, 0, 0, pd, 4, C.byref(n), C.byref(pp),
                                           C.byref(neg)) == -4
+
+
+def header_constants() -> dict[str, int]:
+    """Every `#define BGPU_NAME <integer>[u]` of include/*.h."""
+    out = {}
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        for name, val in re.findall(r"^#define\s+(BGPU_\w+)\s+(-?(?:0x[0-9A-Fa-f]+|\d+))u?\b", open(h).read(),
+                                    flags=re.M):
+            out[name] = int(val, 0)
+    return out
+
+
+def test_python_constants_match_the_header(lib):
+    """The Python binding's flag, method, status and tuning constants are the
+    header's values (the binding passes them straight through the C-ABI)."""
+    import bigint_b200._lib as L
+
+    consts = header_constants()
+    for must in ("BGPU_METHOD_NTT", "BGPU_INDEPENDENT", "BGPU_BATCH_PER_CLASS", "BGPU_FFT_AVERAGE_BOUND",
+                 "BGPU_ERR_CAPACITY", "BGPU_NOALLOC_MAX_LIMBS"):
+        assert must in consts, must
+    shared = [n for n in consts if hasattr(L, n)]
+    assert "BGPU_BATCH_PER_CLASS" in shared and "BGPU_INDEPENDENT" in shared
+    for n in shared:
+        assert getattr(L, n) == consts[n], n
