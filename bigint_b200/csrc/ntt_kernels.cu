@@ -32,13 +32,15 @@
 
 namespace bgpu {
 
-// Row-pass CTAs of rows up to 2^11 points are capped at 48 registers a thread
-// (1280 threads' worth per SM): the pass then fits one more CTA per SM, which
-// shortens the hand-over from the column pass under programmatic dependent
-// launch (measured at 2^20 points: the isolated kernel time is unchanged, the
-// product 7 us shorter).  Longer rows need more registers and keep the default.
+// Row-pass CTAs of rows of 2^10 and 2^11 points are held to 1024 threads'
+// worth per SM (64 registers a thread, eight 128-thread CTAs at 2^11), where
+// the compiler on its own takes more registers and fewer CTAs.  Measured at
+// 2^20 points (2^24 x 2^24 bits), per product back to back: 61.98 us against
+// 62.16 at 1152 threads' worth (56 registers), 63.42 at 1280 (48) and 62.87
+// at 896 (72); at 2^19 points 38.97 against 38.7, 39.6 and 38.8.  Longer rows
+// need more registers and keep the default.
 #ifndef BGPU_MID_THREADS_PER_SM
-#define BGPU_MID_THREADS_PER_SM 1280
+#define BGPU_MID_THREADS_PER_SM 1024
 #endif
 __host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
     return (l1 <= 11 && threads >= 64) ? BGPU_MID_THREADS_PER_SM / threads : 1;
