@@ -32,18 +32,24 @@
 
 namespace bgpu {
 
-// Row-pass CTAs of rows of 2^10 and 2^11 points are held to 1024 threads'
-// worth per SM (64 registers a thread, eight 128-thread CTAs at 2^11), where
-// the compiler on its own takes more registers and fewer CTAs.  Measured at
-// 2^20 points (2^24 x 2^24 bits), per product back to back: 61.98 us against
-// 62.16 at 1152 threads' worth (56 registers), 63.42 at 1280 (48) and 62.87
-// at 896 (72); at 2^19 points 38.97 against 38.7, 39.6 and 38.8.  Longer rows
-// need more registers and keep the default.
+// Row-pass CTAs are held to a register budget below what the compiler takes
+// on its own, so that more of them share an SM: rows of 2^10 to 2^12 points at
+// 1024 threads' worth per SM (64 registers a thread: sixteen, eight or four
+// CTAs), rows of 2^13 points at three 256-thread CTAs (80 registers; their two
+// shared row buffers leave room for no more).  Measured per product back to
+// back, each against the compiler's own choice or the earlier cap:
+//   2^20 points (2^24 x 2^24 bits, rows of 2^11): 61.98 us against 62.16 at
+//     1152 threads' worth (56 registers), 63.42 at 1280 (48), 62.87 at 896;
+//   2^19 points (rows of 2^10): 38.97 against 39.6 at 1280;
+//   2^21 points (rows of 2^12): 119.2 against 126.4 (95 registers, two CTAs),
+//     122.3 at three CTAs, 121.4 at five;
+//   2^22 points (rows of 2^13): 239.7 against 254.8 (88 registers, two CTAs).
+// Longer rows keep the compiler's choice.
 #ifndef BGPU_MID_THREADS_PER_SM
 #define BGPU_MID_THREADS_PER_SM 1024
 #endif
 __host__ __device__ constexpr int mid_min_blocks(int l1, int threads) {
-    return (l1 <= 11 && threads >= 64) ? BGPU_MID_THREADS_PER_SM / threads : 1;
+    return threads < 64 ? 1 : (l1 <= 12 ? BGPU_MID_THREADS_PER_SM / threads : (l1 == 13 ? 768 / threads : 1));
 }
 
 constexpr int kCols = 8;  // columns per outer tile == 32-bit digits per carry chunk
