@@ -295,9 +295,14 @@ __device__ __forceinline__ void fwd_round0(const FwdColsArgs& a, const OperandDe
 // Column tiles of 2^9 rows run 8 CTAs of 256 threads per SM (32 registers a
 // thread, a few bytes spilled): measured at 2^20 points, the product is
 // 0.4 us shorter than with the 40 registers the compiler picks on its own
-// (6 CTAs per SM).  Other heights keep the compiler's choice.
+// (6 CTAs per SM).  Tiles of 2^10 rows run 4 CTAs (64 registers, no spills)
+// where the compiler took 124 registers for 2: at 2^23 points (2^27 x 2^27
+// bits) 502.8 -> 476.0 us per product (3 CTAs at 80 registers: 486.4).
+// Tiles of 2^11 rows keep the compiler's choice (3 CTAs at 80 registers,
+// all their shared memory allows, measured no faster: 1126.3 against
+// 1125.6 us at 2^24 points); so do the shorter ones.
 __host__ __device__ constexpr int fwd_min_blocks(int l2, int threads) {
-    return l2 == 9 ? 2048 / threads : 1;
+    return l2 == 9 ? 2048 / threads : (l2 == 10 ? 1024 / threads : 1);
 }
 
 // The forward column pass of one CTA: tile bx, prime by, operand and product
